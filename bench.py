@@ -1,0 +1,358 @@
+"""Benchmark: converged solves/s of the SIMPLE + FAS multigrid V-cycle on B200.
+
+Workload (default, N=1): the obstacle-flow configuration — 256 x 256 cells, ngrid 5,
+red-black Gauss-Seidel, a seeded staggered lattice of blocks on a 16 x 16 base grid
+(porosity 0.75), both Reynolds numbers 10 and 100 solved together.  A step is one
+converged solve of those cases from the initial guess through the public API:
+reset (device init + rest_geom) and V-cycles until each case reaches the V-cycle
+fixed point (per-cycle relative change of u, v, sc and mean-free p below FP_TOL) or
+the reference's own mass-error test fires.  FP64 throughout, bit-identical to the
+reference's arithmetic.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload c1|c0|c2]
+
+Multi-GPU: one process per GPU (torchrun); every rank solves its own copy of the
+workload (independent cases, no data-path collective: weak scaling); time is the max
+over ranks of device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "multigrid-fvm_b200"))
+
+FP_TOL = 0.0            # stop rule of a solve: the reference's own (mass error or nvcycle)
+# V-cycles each workload case needs to converge (FP_TOL, FP64).  The FP64 engine is
+# bit-identical to the reference per cycle, so these counts are the reference's own;
+# the CPU arm uses them to turn its timed sample of cycles into solves/s.  Re-derived
+# by every GPU run of this script (reported as cycles_per_solve).
+CYCLES_TO_CONVERGE = {"c1": [2000, 2000], "c0": [2000], "c2": None}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# --------------------------------------------------------------- workloads
+def workload(name):
+    from mgfvm import configs
+    if name == "c1":
+        return configs.c1_pair(seed=1), "obstacle flow 256x256 ngrid 5 RBGS Re {10,100} (2 cases)"
+    if name == "c0":
+        return [configs.c0(1)], "channel 64x64 ngrid 3 Jacobi Re 100"
+    if name == "c2":
+        return configs.c2(64, seed=2), "64 mixed-size obstacle cases 64/128/256, coarsest 8x8"
+    raise SystemExit(f"unknown workload {name}")
+
+
+def cell_sweeps_per_cycle(cfg):
+    """(3 nswpm + nswpp) x sum over levels of visits x interior cells (visits: 1 for
+    the finest and coarsest level, 2 otherwise)."""
+    tot = 0
+    for ig in range(cfg.ngrid):
+        cells = (cfg.nfx >> ig) * (cfg.nfy >> ig)
+        visits = 1 if ig in (0, cfg.ngrid - 1) else 2
+        tot += visits * cells
+    return (3 * cfg.nswpm + cfg.nswpp) * tot
+
+
+# --------------------------------------------------------------- clocks
+class ClockSampler:
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(REPO, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                p = [x.strip() for x in line.split(",")]
+                if len(p) >= 9:
+                    rows.append(p)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# --------------------------------------------------------------- CPU side
+def _ref_worker(args):
+    """One process: time `ncyc` V-cycles of one case with the reference build (or the
+    oracle port when the reference build is absent)."""
+    cfg_dict, ncyc, warm = args
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    sys.path.insert(0, os.path.join(REPO, "multigrid-fvm_b200"))
+    import oracle
+    from mgfvm.inputs import CaseConfig
+    cfg = CaseConfig(**cfg_dict)
+    if oracle.ref_available():
+        r = oracle.RefCase(cfg)
+        r.time_cycles(warm)
+        return "reference", r.time_cycles(ncyc) / ncyc
+    o = oracle.OracleCase(cfg)
+    o.cycle(warm)
+    t = time.perf_counter()
+    o.cycle(ncyc)
+    return "port", (time.perf_counter() - t) / ncyc
+
+
+def cpu_sample(cases, cycles_to_converge, ncyc, procs):
+    """solves/s of the CPU implementation on `procs` host processes (one case each,
+    round-robin over the workload's cases), from the mean time per V-cycle."""
+    import dataclasses
+    import multiprocessing as mp
+    jobs = [(dataclasses.asdict(cases[k % len(cases)]), ncyc, 2) for k in range(procs)]
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_ref_worker, jobs)
+    wall = time.perf_counter() - t0
+    kind = res[0][0]
+    # mean time of one solve of the workload's cases on one core
+    per_case = []
+    for k, (_, tcyc) in enumerate(res):
+        per_case.append(tcyc * cycles_to_converge[k % len(cases)])
+    t_solve_one_core = float(np.mean(per_case))
+    return procs / t_solve_one_core, kind, wall, float(np.mean([r[1] for r in res]))
+
+
+def run_reference_arm(a, rank, world):
+    if rank != 0:
+        return
+    cases, desc = workload(a.workload)
+    ctc = CYCLES_TO_CONVERGE[a.workload]
+    if ctc is None:
+        print(json.dumps({"impl": "reference", "unavailable": f"no converged cycle counts for {a.workload}"}))
+        return
+    procs = max(1, min(os.cpu_count() or 1, 64))
+    ncyc = {"c1": 8, "c0": 200}.get(a.workload, 8)
+    vals = []
+    for s in range(a.warmup + a.steps):
+        v, kind, wall, tcyc = cpu_sample(cases, ctc, ncyc, procs)
+        if s >= a.warmup:
+            vals.append(v)
+    value = float(np.mean(vals))
+    sample = (f"{ncyc} V-cycles per process after 2 warm-up cycles, {procs} processes (one case each, "
+              f"round-robin over the workload's cases); solves/s = processes / (mean time per V-cycle x "
+              f"V-cycles to converge {ctc})")
+    line = {
+        "impl": "reference", "metric": "converged solves/s", "value": value, "unit": "solves/s",
+        "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": desc},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": procs, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# --------------------------------------------------------------- GPU side
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c1", choices=["c1", "c0", "c2"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-cycles", type=int, default=0,
+                    help="only run 3 warm-up V-cycles then this many V-cycles of the workload "
+                         "(for ncu launch lists) and exit")
+    a = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        run_reference_arm(a, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    from mgfvm import Solver
+    cases, desc = workload(a.workload)
+    n_cases = len(cases)
+    solver = Solver(cases, device=local, sync_every=64)
+    if a.profile_cycles:
+        solver.cycle(3)
+        n0 = solver.kernel_launches
+        solver.cycle(a.profile_cycles)
+        log(f"profile: {n0} launches before, {solver.kernel_launches - n0} in {a.profile_cycles} cycle(s), "
+            f"{solver.last_elapsed_ms:.3f} ms")
+        solver.close()
+        return
+    stream = torch.cuda.ExternalStream(solver.stream, device=torch.device("cuda", local))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def step():
+        solver.reset()
+        return solver.solve(max(c.nvcycle for c in cases), FP_TOL)
+
+    for _ in range(a.warmup):
+        cyc = step()
+    launches0 = solver.kernel_launches
+    cycles = []
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(a.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)          # L2 flush between steps (256 MiB write)
+            cycles.append(step())
+        e1.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    launches = solver.kernel_launches - launches0
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    total_solves = n_cases * a.steps * world
+    value = total_solves / (ms / 1e3)
+    cyc_arr = np.array(cycles)
+    cycles_per_solve = [int(x) for x in cyc_arr[-1]]
+    sweeps = sum(cell_sweeps_per_cycle(c) * int(n) for c, n in zip(cases, cycles_per_solve))
+    cell_sweeps_per_s = sweeps * a.steps * world / (ms / 1e3)
+
+    # ---- dominant kernel: one colour of the red-black p' sweep on level 0 (live)
+    import mgfvm
+    reps = 20
+    solver.time_op("smooth_pp", 0, 2)
+    kms, klaunch = solver.time_op("smooth_pp", 0, reps)
+    per_launch_ms = kms / klaunch
+    colour_cells = sum(((c.nfx * c.nfy) + 1) // 2 for c in cases)
+    algo_bytes = colour_cells * 64          # 6 coefficients + phi read + phi write, 8 B each
+    peaks = {}
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except Exception:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = algo_bytes / (per_launch_ms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": None,
+                "kernel": "k_gs (one colour of a red-black sweep, p' equation, level 0)",
+                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                "per_launch_us": round(per_launch_ms * 1e3, 3), "algorithmic_bytes_per_launch": algo_bytes}
+
+    # ---- end to end through the public API with host buffers
+    e2e = None
+    if rank == 0 or True:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        h2d = d2h = 0
+        for _ in range(max(1, a.steps)):
+            with Solver(cases, device=local) as s2:
+                s2.solve(max(c.nvcycle for c in cases), FP_TOL)
+                for k in range(n_cases):
+                    for f in ("u", "v", "p", "sc"):
+                        s2.field(k, 0, f)
+                b = s2.transfer_bytes
+            h2d += b[0]
+            d2h += b[1]
+        torch.cuda.synchronize()
+        t_e2e = time.perf_counter() - t0
+        e2e = {"value": n_cases * max(1, a.steps) * world / t_e2e, "unit": "solves/s",
+               "h2d_bytes_per_step": int(h2d / max(1, a.steps)), "d2h_bytes_per_step": int(d2h / max(1, a.steps))}
+        if world > 1:
+            t = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e["value"] = n_cases * max(1, a.steps) * world / float(t.item())
+
+    # ---- parity spot check at full size: 3 cycles against the CPU oracle
+    l2err = None
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        import oracle
+        with Solver(cases[:1], device=local) as s3:
+            o = oracle.OracleCase(cases[0])
+            s3.cycle(3)
+            o.cycle(3)
+            l2err = max(float(np.linalg.norm(s3.field(0, 0, f) - o.get(0, f)) /
+                              max(np.linalg.norm(o.get(0, f)), 1e-300)) for f in ("u", "v", "p", "sc"))
+        ctc = cycles_per_solve
+        v, kind, wall, tcyc = cpu_sample(cases, ctc, {"c1": 8, "c0": 200}.get(a.workload, 4),
+                                         max(1, min(os.cpu_count() or 1, 64)))
+        cpu = {"value": v, "unit": "solves/s", "cores": max(1, min(os.cpu_count() or 1, 64)), "kind": kind,
+               "sample": f"V-cycles timed per host process ({wall:.1f} s wall), one case per process, "
+                         f"extrapolated with the GPU's cycles-to-converge {ctc}"}
+
+    if rank == 0:
+        line = {
+            "metric": "converged solves/s", "value": round(value, 4), "unit": "solves/s", "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms / a.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded obstacle patterns)",
+            "config": {"workload": desc, "cases_per_gpu": n_cases,
+                       "stop_rule": "reference: mass error < convergence or nvcycle V-cycles",
+                       "nvcycle": [c.nvcycle for c in cases], "l2": "flushed between steps (256 MiB write)",
+                       "parallelism": f"independent cases, {world} rank(s)"},
+            "cycles_per_solve": cycles_per_solve,
+            "cell_sweeps_per_s": cell_sweeps_per_s,
+            "l2_rel_err_vs_oracle_3cycles": l2err,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line))
+    solver.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,284 @@
+/*
+ * mgfvm.h — C ABI of the B200 engine for the staggered-grid SIMPLE solver with a
+ * FAS multigrid V-cycle (akashu4295/Multigrid-FVM, Version-6-26-04.c).
+ *
+ * The reference is one C program whose state lives in globals (Version-6-26-04.c:27-39)
+ * and in one `struct SoA` per multigrid level (:42-54).  This header replaces that
+ * process-global interface with an opaque context that owns every level of every
+ * case on one GPU.  A single solve is a batch of one case.
+ *
+ * Conventions shared by every entry point:
+ *   - every function returns an int status (MGFVM_OK on success); the message of
+ *     the last failure on the calling thread is returned by mgfvm_last_error();
+ *     nothing in the library calls exit().  (The reference exits the process on
+ *     any parse or allocation error: :283-291, :106-114, :2369-2378.)
+ *   - arrays use the reference layout: level `ig` is npx x npy doubles with
+ *     npx = nfx/2^ig + 2, npy = nfy/2^ig + 2 (:408-411), row-major, ij = j*npx + i.
+ *   - host buffers passed in or out are plain host memory owned by the caller;
+ *     device memory is owned by the context, except for the raw-pointer kernel
+ *     entry points at the end of this file, which take caller-owned device memory.
+ *   - calls on one context are not thread-safe; use one context per host thread.
+ */
+#ifndef MGFVM_H
+#define MGFVM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MGFVM_ABI_VERSION 1
+
+/* ---------------------------------------------------------------- status */
+enum mgfvm_status {
+    MGFVM_OK = 0,
+    MGFVM_EINVAL = 1,       /* malformed InputData/pattern or bad argument        */
+    MGFVM_EIO = 2,          /* file missing or unreadable                         */
+    MGFVM_EOOB = 3,         /* obstacle/inlet/outlet index range leaves the grid  */
+    MGFVM_ENONFINITE = 4,   /* NaN or Inf in the mass-error history               */
+    MGFVM_ETIMEOUT = 5,     /* a bounded device-side wait gave up                 */
+    MGFVM_ECUDA = 6,        /* CUDA runtime error                                 */
+    MGFVM_ENOMEM = 7,       /* host or device allocation failed                   */
+    MGFVM_EUNSUPPORTED = 8  /* valid input this build does not handle             */
+};
+
+/* ---------------------------------------------------------------- fields */
+/* One id per array of `struct SoA` (Version-6-26-04.c:42-54). */
+enum mgfvm_field {
+    MGFVM_F_U = 0, MGFVM_F_V, MGFVM_F_P, MGFVM_F_PP, MGFVM_F_SC,
+    MGFVM_F_SU, MGFVM_F_RS, MGFVM_F_RESU, MGFVM_F_RESV, MGFVM_F_RESSC,
+    MGFVM_F_C,
+    MGFVM_F_AW, MGFVM_F_AE, MGFVM_F_AS, MGFVM_F_AN, MGFVM_F_AP,
+    MGFVM_F_APU, MGFVM_F_APV, MGFVM_F_SPU, MGFVM_F_SPV, MGFVM_F_SPSC,
+    MGFVM_F_CX, MGFVM_F_CY, MGFVM_F_AREAX, MGFVM_F_AREAY,
+    MGFVM_NFIELDS
+};
+
+/* ------------------------------------------------------ single-step ops */
+/* The per-level routines of one V-cycle, for parity tests and for callers that
+ * drive their own cycle (Version-6-26-04.c:195-249).  `level` is the level the
+ * routine acts on; RESTRICT acts on (level -> level+1), PROLONG on
+ * (level+1 -> level). */
+enum mgfvm_op {
+    MGFVM_OP_FLUXES = 0,      /* fluxes        :678-694                          */
+    MGFVM_OP_SOLVE_U,         /* solve_u       :696-703   coefu, umom, smoother   */
+    MGFVM_OP_SOLVE_V,         /* solve_v       :705-712                          */
+    MGFVM_OP_SOLVE_PP,        /* solve_pprime  :714-728   masserror..update       */
+    MGFVM_OP_PBOUND,          /* pbound        :1179-1210                        */
+    MGFVM_OP_OUTFLOW,         /* outflow       :1211-1228                        */
+    MGFVM_OP_SOLVE_SC,        /* solve_sc      :729-737                          */
+    MGFVM_OP_RESTRICT,        /* restv, fluxes(c), fluxes(f), restru, restrv, restrsc :211-220 */
+    MGFVM_OP_PROLONG,         /* prolu, prolv, prolp, prolsc :230-233           */
+    MGFVM_OP_SMOOTH_U,        /* the smoother alone on u with the current coefficients */
+    MGFVM_OP_SMOOTH_V,
+    MGFVM_OP_SMOOTH_PP,
+    MGFVM_OP_SMOOTH_SC,
+    MGFVM_NOPS
+};
+
+/* Linear smoothers (InputData isolve, :1231-1351). */
+enum { MGFVM_JACOBI = 1, MGFVM_GAUSS_SEIDEL = 2 };
+
+/* Arithmetic of the V-cycle. */
+enum mgfvm_precision {
+    MGFVM_PREC_FP64 = 0,   /* every array and every operation in FP64, as the reference */
+    MGFVM_PREC_MIXED = 1   /* FP32 smoothing/transfers, FP64 defect, norms and coarsest level */
+};
+
+#define MGFVM_MAX_PORTS 10   /* inlet/outlet arrays of the reference hold 10 (:29, :38) */
+
+/* ------------------------------------------------------------ one case */
+/* Everything InputData and pattern.txt hold, field for field (README.md:6-29,
+ * readInput Version-6-26-04.c:280-401, read_obstacle_data :2367-2400). */
+typedef struct mgfvm_config {
+    /* InputData line 1 */
+    int nfx, nfy, ngrid, ig_obs, ibeg_obs, ig_inlt, ig_outlt;
+    int nvcycle, nswpm, nswpp, isolve;
+    double omega, convergence;
+    /* line 2 */
+    double xl, yl, amuf, prsc, relxm, relxp;
+    /* line 3: 1 fixed value, 2 p' Dirichlet, 3 periodic, 4 outflow (x+ only) */
+    int ibc_xm, ibc_xp, ibc_ym, ibc_yp;
+    /* lines 4-7 */
+    double u_xm, v_xm, p_xm, sc_xm;
+    double u_xp, v_xp, p_xp, sc_xp;
+    double u_ym, v_ym, p_ym, sc_ym;
+    double u_yp, v_yp, p_yp, sc_yp;
+    /* line 8 */
+    double u_guess, v_guess, p_guess, sc_guess;
+    /* line 9 */
+    double sc_obs;
+    /* discrete inlets and outlets */
+    int ninlt;
+    int jfinlt[MGFVM_MAX_PORTS], jlinlt[MGFVM_MAX_PORTS];
+    double uinlt[MGFVM_MAX_PORTS], vinlt[MGFVM_MAX_PORTS], scinlt[MGFVM_MAX_PORTS];
+    int noutlt;
+    int jfoutlt[MGFVM_MAX_PORTS], jloutlt[MGFVM_MAX_PORTS];
+    double uoutlt[MGFVM_MAX_PORTS], voutlt[MGFVM_MAX_PORTS], scoutlt[MGFVM_MAX_PORTS];
+    /* pattern.txt: nobs rectangles {if, il, jf, jl} (1-based, on level ig_obs-1) */
+    int nobs;
+    int *obs;          /* 4*nobs ints; owned by whoever filled the struct */
+    /* body-force pressure gradients; declared but never read by the reference (:33) */
+    double dpdxm, dpdym;
+} mgfvm_config;
+
+/* Context options. */
+typedef struct mgfvm_options {
+    int device;        /* CUDA device ordinal                                        */
+    int precision;     /* enum mgfvm_precision                                       */
+    int tail_level;    /* first level run by the one-CTA-per-case coarse kernel;
+                          -1 = chosen by the tuner, >= ngrid = no coarse kernel      */
+    int use_graph;     /* replay V-cycles from a captured CUDA graph (1) or launch
+                          every kernel directly (0)                                   */
+    int sync_every;    /* cycles between host reads of the stop flags in mgfvm_solve */
+} mgfvm_options;
+
+typedef struct mgfvm_ctx mgfvm_ctx;
+
+/* ------------------------------------------------------ configuration */
+void mgfvm_config_default(mgfvm_config *cfg);
+void mgfvm_options_default(mgfvm_options *opt);
+
+/* Parse InputData and pattern.txt exactly as readInput/read_obstacle_data do
+ * (Version-6-26-04.c:280-401, :2367-2400; pattern.txt is read between lines 8
+ * and 9 of InputData, :357).  cfg->obs is allocated by the library; release it
+ * with mgfvm_config_release.  `verbose` != 0 prints the reference's echo lines
+ * to stdout. */
+int mgfvm_config_read(const char *inputdata_path, const char *pattern_path,
+                      mgfvm_config *cfg, int verbose);
+void mgfvm_config_release(mgfvm_config *cfg);
+
+/* Check a configuration against the grid: level sizes divisible by 2^(ngrid-1),
+ * every obstacle/inlet/outlet range inside the padded grid of every level it
+ * touches, supported boundary codes.  Returns MGFVM_EINVAL/MGFVM_EOOB/... */
+int mgfvm_config_validate(const mgfvm_config *cfg);
+
+/* ------------------------------------------------------------ context */
+/* Build the device state of `ncases` independent cases (AllocateMemorySoA :402-506,
+ * init :546-676, rest_geom :1391-1473) and upload it.  All cases must share
+ * isolve, nswpm and nswpp; grid sizes, ngrid, physics and obstacles may differ. */
+int mgfvm_create(const mgfvm_config *cases, int ncases, const mgfvm_options *opt,
+                 mgfvm_ctx **out);
+int mgfvm_destroy(mgfvm_ctx *ctx);
+
+/* Return every case to its initial state (init + rest_geom) and clear histories. */
+int mgfvm_reset(mgfvm_ctx *ctx);
+
+/* Per-face inlet profile: level-0 u at the x- boundary face of rows j = 1..n
+ * (n = nfy), applied after init and before rest_geom, so coarse levels take the
+ * face average of it (rest_geom :1440-1446).  Resets that case. */
+int mgfvm_set_inlet_profile(mgfvm_ctx *ctx, int icase, const double *u, int n);
+
+/* Run exactly `ncycles` V-cycles on every case (no stop test). */
+int mgfvm_cycle(mgfvm_ctx *ctx, int ncycles);
+
+/* Run V-cycles until every case has stopped or `max_cycles` have run.  A case stops
+ * after the cycle whose level-0 mass error is below its `convergence` (the
+ * reference test, :247-248), or whose fixed-point change is below `fp_tol`
+ * (fp_tol <= 0 disables that rule).  The fixed-point change of cycle k is
+ *   max over f in {u, v, sc, p - mean(p)} of ||f_k - f_{k-1}||_2 / ||f_k||_2
+ * over the level-0 interior.  cycles_out[c] (may be NULL) receives the number of
+ * cycles case c ran. */
+int mgfvm_solve(mgfvm_ctx *ctx, int max_cycles, double fp_tol, int *cycles_out);
+
+/* Per-cycle history of case `icase`: err[k] = level-0 sum |div| measured before the
+ * cycle's p' correction (convergence_data, :717-724); delta[k] = the fixed-point
+ * change defined above (0 for cycle 0 and when not tracked).  Either pointer may
+ * be NULL.  *n_out = cycles recorded (<= cap are copied). */
+int mgfvm_history(mgfvm_ctx *ctx, int icase, double *err, double *delta, int cap,
+                  int *n_out);
+
+/* --------------------------------------------------------- data access */
+int mgfvm_num_levels(mgfvm_ctx *ctx, int icase, int *ngrid);
+int mgfvm_level_dims(mgfvm_ctx *ctx, int icase, int level, int *npx, int *npy);
+/* Copy one array of one level of one case (npx*npy doubles) to or from the host. */
+int mgfvm_get_field(mgfvm_ctx *ctx, int icase, int level, int field, double *out);
+int mgfvm_set_field(mgfvm_ctx *ctx, int icase, int level, int field, const double *in);
+/* The cell tag of one level (1 fluid, 0 obstacle; init :617-641), npx*npy ints. */
+int mgfvm_get_tag(mgfvm_ctx *ctx, int icase, int level, int *out);
+/* Obstacle index ranges of one level after the level mapping of :468-478.  Levels
+ * at or above ig_obs hold the empty range {1, 0, 1, 0}.  out: 4*nobs ints
+ * {is, ie, js, je}. */
+int mgfvm_get_obstacle_ranges(mgfvm_ctx *ctx, int icase, int level, int *out);
+
+/* Run one single-step op (enum mgfvm_op) on `level` of every case. */
+int mgfvm_op(mgfvm_ctx *ctx, int op, int level);
+
+/* Number of kernels this context launched since creation (graph replays count
+ * each kernel node). */
+int mgfvm_kernel_launches(mgfvm_ctx *ctx, long long *out);
+
+/* Wall-clock of the last mgfvm_cycle/mgfvm_solve measured with CUDA events on the
+ * context stream, in milliseconds. */
+int mgfvm_last_elapsed_ms(mgfvm_ctx *ctx, double *ms);
+
+/* The CUDA stream the context launches on (a cudaStream_t). */
+int mgfvm_stream(mgfvm_ctx *ctx, void **stream);
+
+/* Time `reps` back-to-back runs of single-step op `op` on `level` of every case with
+ * CUDA events on the context stream (no host work between the events).
+ * *ms_total = elapsed milliseconds, *launches = kernels launched in that window. */
+int mgfvm_time_op(mgfvm_ctx *ctx, int op, int level, int reps, double *ms_total, int *launches);
+
+/* Bytes this context copied host->device and device->host since it was created. */
+int mgfvm_transfer_bytes(mgfvm_ctx *ctx, long long *h2d, long long *d2h);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *mgfvm_last_error(void);
+
+/* ------------------------------------------------- pattern generators */
+/* Seeded versions of the reference's interactive generators (which seed rand()
+ * with time(NULL)).  Host only; no GPU needed.
+ *
+ * Staggered lattice of 1x1 base blocks on an (n_base*scale)^2 sub-pixel grid:
+ * variant 1 inline, 2 staggered, >= 3 the (variant-2)-th random perturbation of the
+ * staggered lattice.  Replaces create_patterns_staggered.c:71-200.  grid: dim^2 ints. */
+int mgfvm_pattern_staggered(int n_base, int scale, int spacing_x, int spacing_y, int variant,
+                            unsigned long long seed, int *grid);
+/* Non-overlapping particles of side 3, 2, 1 at a target filled fraction; rects
+ * (may be NULL) receives {r1, r2, c1, c2} 1-based per particle, the reference's
+ * pattern-file rows.  Replaces create_patterns_random.c:18-181. */
+int mgfvm_pattern_random(int n_grid, double ratio, double pct1, double pct2, double pct3,
+                         unsigned long long seed, int *grid, int *rects, int max_rects,
+                         int *n_rects);
+/* One obstacle per occupied pixel {r+1, r+1, c+1, c+1} (create_patterns_staggered.c:47-54). */
+int mgfvm_pattern_pixels(const int *grid, int dim, int *obs, int max_obs, int *count);
+
+/* ------------------------------------- raw-pointer kernel entry points */
+/* These take caller-owned DEVICE pointers to one level laid out as above and
+ * launch on `stream` (a cudaStream_t, NULL = legacy default stream).  They are
+ * the drop-in replacements of the reference's per-level routines for callers
+ * that keep their own level storage. */
+
+/* Jacobi, `nsw` sweeps of phi <- (sum a_nb phi_nb + su) / (ap + 1e-30) over
+ * i in [1, nx-1], j in [1, ny-1], ping-ponging through `scratch` (npx*npy doubles,
+ * caller-owned); the result is left in phi.  Replaces solver(),
+ * Version-6-26-04.c:1231-1296 (which mallocs its scratch on every call). */
+int mgfvm_jacobi_f64(const double *aw, const double *ae, const double *as,
+                     const double *an, const double *ap, const double *su,
+                     double *phi, double *scratch, int npx, int npy, int nx, int ny,
+                     int nsw, void *stream);
+
+/* Red-black Gauss-Seidel, `nsw` sweeps of a red pass ((i+j) even) then a black
+ * pass, in place, phi <- (sum a_nb phi_nb + su) / ap.  Replaces solvergs(),
+ * Version-6-26-04.c:1297-1351. */
+int mgfvm_rbgs_f64(const double *aw, const double *ae, const double *as,
+                   const double *an, const double *ap, const double *su,
+                   double *phi, int npx, int npy, int nx, int ny, int nsw,
+                   void *stream);
+
+/* Mass residual: su = -div, pp = 0 on the interior and *err_out (device) =
+ * sum |div|, reduced in a fixed order through `partials` (caller-owned device
+ * scratch of mgfvm_masserror_scratch_doubles(npx, npy) doubles).  Replaces
+ * masserror(), Version-6-26-04.c:1096-1125. */
+int mgfvm_masserror_f64(const double *u, const double *v, const double *areax,
+                        const double *areay, double *su, double *pp, int npx,
+                        int npy, double *err_out, double *partials, void *stream);
+size_t mgfvm_masserror_scratch_doubles(int npx, int npy);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MGFVM_H */

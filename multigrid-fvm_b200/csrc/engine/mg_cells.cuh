@@ -1,0 +1,476 @@
+// mg_cells.cuh — the per-cell arithmetic of every V-cycle routine, shared by the
+// grid-wide kernels (one thread per cell, all cases of a batch in one launch) and
+// the coarse-level kernel (one CTA per case, all coarse levels in one launch).
+//
+// Every function restates one loop body of Version-6-26-04.c with the operations in
+// the reference's order; this file is compiled with --fmad=false so the FP64 results
+// are bit-identical to the reference built with gcc.  Where the reference runs a
+// second loop over boundary rows or obstacle cells after the main loop, the
+// function applies that loop's additions to the cell in the same order.
+#pragma once
+
+#include "mg_common.cuh"
+
+namespace mg {
+
+#define MGF(L, s) ((L).f[(s)])
+
+// max(|c|, D) +/- c: the hybrid upwind/central coefficient (:845-848)
+__device__ __forceinline__ double hyb_p(double c, double d) { return fmax(fabs(c), d) + c; }
+__device__ __forceinline__ double hyb_m(double c, double d) { return fmax(fabs(c), d) - c; }
+
+struct Coef { double aw, ae, as, an, ap; };
+
+// ------------------------------------------------------------------ fluxes
+// fluxes :678-694, domain i in [0, npx-2], j in [0, npy-2]
+__device__ __forceinline__ void cell_fluxes(const LevelDev &L, int q)
+{
+    MGF(L, S_CX)[q] = 0.5 * MGF(L, S_U)[q] * MGF(L, S_AREAX)[q];
+    MGF(L, S_CY)[q] = 0.5 * MGF(L, S_V)[q] * MGF(L, S_AREAY)[q];
+}
+
+// ------------------------------------------------------------ coefficients
+// coefu :815-860 at u face (i, j), i in [1, npx-3], j in [1, npy-2], including the
+// wall-shear rows j = npy-2 then j = 1 (:849-858; both use areay of row npy-2).
+__device__ __forceinline__ Coef coef_u(const LevelDev &L, int i, int j)
+{
+    const int nx = L.npx, q = j * nx + i, s = q - nx;
+    const double *cx = MGF(L, S_CX), *cy = MGF(L, S_CY);
+    double cxm = 0.5 * (cx[q] + cx[q - 1]);
+    double cxp = 0.5 * (cx[q] + cx[q + 1]);
+    double cym = 0.5 * (cy[s] + cy[s + 1]);
+    double cyp = 0.5 * (cy[q] + cy[q + 1]);
+    double dxm = L.amu * (MGF(L, S_AREAX)[q] / L.dx);
+    double dym = L.amu * (MGF(L, S_AREAY)[q] / L.dy);
+    Coef k;
+    k.aw = hyb_p(cxm, dxm);
+    k.ae = hyb_m(cxp, dxm);
+    k.as = hyb_p(cym, dym);
+    k.an = hyb_m(cyp, dym);
+    k.ap = k.aw + k.ae + k.as + k.an;
+    const int top = L.npy - 2;
+    if (j == top) {
+        double add = L.amu * (MGF(L, S_AREAY)[q] / L.dy);
+        k.an += add; k.ap += add;
+    }
+    if (j == 1) {
+        double add = L.amu * (MGF(L, S_AREAY)[top * nx + i] / L.dy);
+        k.as += add; k.ap += add;
+    }
+    return k;
+}
+
+// coefv :966-1016 at v face (i, j), i in [1, npx-2], j in [1, npy-3], including the
+// side-wall columns i = npx-2 then i = 1 (:1005-1015; both use areay of column npx-2).
+__device__ __forceinline__ Coef coef_v(const LevelDev &L, int i, int j)
+{
+    const int nx = L.npx, q = j * nx + i, n = q + nx, s = q - nx;
+    const double *cx = MGF(L, S_CX), *cy = MGF(L, S_CY);
+    double cxm = 0.5 * (cx[q - 1] + cx[n - 1]);
+    double cxp = 0.5 * (cx[q] + cx[n]);
+    double cym = 0.5 * (cy[q] + cy[s]);
+    double cyp = 0.5 * (cy[q] + cy[n]);
+    double dx_ = L.amu * (MGF(L, S_AREAX)[q] / L.dx);
+    double dy_ = L.amu * (MGF(L, S_AREAY)[q] / L.dy);
+    Coef k;
+    k.aw = hyb_p(cxm, dx_);
+    k.ae = hyb_m(cxp, dx_);
+    k.as = hyb_p(cym, dy_);
+    k.an = hyb_m(cyp, dy_);
+    k.ap = k.aw + k.ae + k.as + k.an;
+    const int rgt = nx - 2;
+    if (i == rgt) {
+        double add = L.amu * (MGF(L, S_AREAY)[q] / L.dy);
+        k.ae += add; k.ap += add;
+    }
+    if (i == 1) {
+        double add = L.amu * (MGF(L, S_AREAY)[j * nx + rgt] / L.dy);
+        k.aw += add; k.ap += add;
+    }
+    return k;
+}
+
+// coefsc :861-964 at cell (i, j) interior, then the obstacle-face additions this cell
+// receives from the host-only loop :939-963, in that loop's order (codes built by
+// mgfvm_build_obstacle_prog: 0 ae from the east cell, 1 aw from the west cell,
+// 2 an from the north cell, 3 as from the south cell; count in bits 28-31).
+__device__ __forceinline__ Coef coef_sc(const LevelDev &L, int i, int j)
+{
+    const int nx = L.npx, q = j * nx + i, s = q - nx;
+    const double *cx = MGF(L, S_CX), *cy = MGF(L, S_CY);
+    const double *ax = MGF(L, S_AREAX), *ay = MGF(L, S_AREAY);
+    const double amusc = L.amusc;
+    double dxm = amusc * (ax[q - 1] / L.dx);
+    double dym = amusc * (ay[s] / L.dy);
+    double dxp = amusc * (ax[q] / L.dx);
+    double dyp = amusc * (ay[q] / L.dy);
+    Coef k;
+    k.aw = hyb_p(cx[q - 1], dxm);
+    k.ae = hyb_m(cx[q], dxp);
+    k.as = hyb_p(cy[s], dym);
+    k.an = hyb_m(cy[q], dyp);
+    k.ap = k.aw + k.ae + k.as + k.an;
+    if (L.seq) {
+        unsigned code = L.seq[q];
+        int cnt = (int)(code >> 28);
+        for (int t = 0; t < cnt; ++t) {
+            int d = (int)((code >> (2 * t)) & 3u);
+            double add;
+            if (d == 0)      { add = amusc * (ax[q + 1] / L.dx);  k.ae += add; }
+            else if (d == 1) { add = amusc * (ax[q - 1] / L.dx);  k.aw += add; }
+            else if (d == 2) { add = amusc * (ay[q + nx] / L.dy); k.an += add; }
+            else             { add = amusc * (ay[q - nx] / L.dy); k.as += add; }
+            k.ap += add;
+        }
+    }
+    return k;
+}
+
+__device__ __forceinline__ void store_coef(const LevelDev &L, int q, const Coef &k)
+{
+    MGF(L, S_AW)[q] = k.aw; MGF(L, S_AE)[q] = k.ae;
+    MGF(L, S_AS)[q] = k.as; MGF(L, S_AN)[q] = k.an;
+    MGF(L, S_AP)[q] = k.ap;
+}
+
+// ---------------------------------------------------------- assembly ops
+// solve_u's assembly: coefu :815-860 then umom :741-767 at one u face
+__device__ __forceinline__ void cell_mom_u(const LevelDev &L, const CaseDev &C, int i, int j)
+{
+    const int q = j * L.npx + i;
+    Coef k = coef_u(L, i, j);
+    const double ax = MGF(L, S_AREAX)[q];
+    const double rm = C.relxm, rm1 = 1.0 - C.relxm;
+    double su = ax * (MGF(L, S_P)[q] - MGF(L, S_P)[q + 1]);
+    double ap = k.ap / rm;
+    su = su + rm1 * ap * MGF(L, S_U)[q] + MGF(L, S_RESU)[q] + C.dpdxm * ax * MGF(L, S_AREAY)[q];
+    ap = ap + MGF(L, S_SPU)[q];
+    k.ap = ap;
+    store_coef(L, q, k);
+    MGF(L, S_APU)[q] = ap;
+    MGF(L, S_SU)[q] = su;
+}
+
+// solve_v's assembly: coefv :966-1016 then vmom :769-793 at one v face
+__device__ __forceinline__ void cell_mom_v(const LevelDev &L, const CaseDev &C, int i, int j)
+{
+    const int q = j * L.npx + i;
+    Coef k = coef_v(L, i, j);
+    const double ay = MGF(L, S_AREAY)[q];
+    const double rm = C.relxm, rm1 = 1.0 - C.relxm;
+    double su = ay * (MGF(L, S_P)[q] - MGF(L, S_P)[q + L.npx]);
+    double ap = k.ap / rm;
+    su = su + rm1 * ap * MGF(L, S_V)[q] + MGF(L, S_RESV)[q] + C.dpdym * MGF(L, S_AREAX)[q] * ay;
+    ap = ap + MGF(L, S_SPV)[q];
+    k.ap = ap;
+    store_coef(L, q, k);
+    MGF(L, S_APV)[q] = ap;
+    MGF(L, S_SU)[q] = su;
+}
+
+// solve_pprime's assembly: masserror :1096-1125 then coefp :1018-1092 (with the
+// p' Dirichlet rows in the order x-, x+, y-, y+) at one interior cell; returns |div|.
+__device__ __forceinline__ double cell_mass_coefp(const LevelDev &L, const CaseDev &C, int i, int j)
+{
+    const int nx = L.npx, ny = L.npy, q = j * nx + i, s = q - nx;
+    const double *ax = MGF(L, S_AREAX), *ay = MGF(L, S_AREAY);
+    const double *u = MGF(L, S_U), *v = MGF(L, S_V);
+    const double *apu = MGF(L, S_APU), *apv = MGF(L, S_APV);
+    const double axq = ax[q], ayq = ay[q];
+    double div = axq * u[q] - axq * u[q - 1] + ayq * v[q] - ayq * v[s];
+    double su = -div;
+    MGF(L, S_PP)[q] = 0.0;
+    Coef k;
+    k.aw = ax[q - 1] * ax[q - 1] / apu[q - 1];
+    k.ae = axq * axq / apu[q];
+    k.as = ay[s] * ay[s] / apv[s];
+    k.an = ayq * ayq / apv[q];
+    k.ap = k.aw + k.ae + k.as + k.an + (double)(1 - L.tag[q]) * 1.0e30;
+    const double diag = 1.0e30;
+    if (C.ibc_xm == 2 && i == 1) { k.ap = k.ap + diag; su = 0.0; }
+    if (C.ibc_xp == 2 && i == nx - 2) { k.ap = k.ap + diag; su = 0.0; }
+    if (C.ibc_ym == 2 && j == 1) { k.ap = k.ap + diag; su = 0.0; }
+    if (C.ibc_yp == 2 && j == ny - 2) { k.ap = k.ap + diag; su = 0.0; }
+    store_coef(L, q, k);
+    MGF(L, S_SU)[q] = su;
+    return fabs(div);
+}
+
+// update :1127-1152 (the obstacle pressure copy :1153-1177 is a separate gather)
+__device__ __forceinline__ void cell_update(const LevelDev &L, const CaseDev &C, int q)
+{
+    double *u = MGF(L, S_U), *v = MGF(L, S_V), *p = MGF(L, S_P);
+    const double *pp = MGF(L, S_PP);
+    const double ppref = 0.0;
+    const double ppq = pp[q];
+    u[q] += MGF(L, S_AREAX)[q] * (ppq - pp[q + 1]) / MGF(L, S_APU)[q];
+    v[q] += MGF(L, S_AREAY)[q] * (ppq - pp[q + L.npx]) / MGF(L, S_APV)[q];
+    p[q] += C.relxp * (ppq - ppref);
+}
+
+// solve_sc's assembly: coefsc :861-964 (+ obstacle faces) then scalar :795-812
+__device__ __forceinline__ void cell_sc(const LevelDev &L, const CaseDev &C, int i, int j)
+{
+    const int q = j * L.npx + i;
+    Coef k = coef_sc(L, i, j);
+    const double spsc = MGF(L, S_SPSC)[q];
+    double su = spsc * C.sc_obs + MGF(L, S_RESSC)[q];
+    k.ap = k.ap + spsc;
+    store_coef(L, q, k);
+    MGF(L, S_SU)[q] = su;
+}
+
+// --------------------------------------------------------------- smoothers
+// one Jacobi point update, wj = 1 (solver :1259-1286)
+__device__ __forceinline__ void cell_jacobi(const LevelDev &L, const double *cur, double *nxt, int q)
+{
+    const int nx = L.npx;
+    const double wj = 1.0;
+    double nb = MGF(L, S_AW)[q] * cur[q - 1] + MGF(L, S_AE)[q] * cur[q + 1]
+              + MGF(L, S_AS)[q] * cur[q - nx] + MGF(L, S_AN)[q] * cur[q + nx];
+    double g = (nb + MGF(L, S_SU)[q]) / (MGF(L, S_AP)[q] + 1.0e-30);
+    nxt[q] = (1.0 - wj) * cur[q] + wj * g;
+}
+
+// one red-black Gauss-Seidel point update (solvergs :1308-1350)
+__device__ __forceinline__ void cell_gs(const LevelDev &L, double *phi, int q)
+{
+    const int nx = L.npx;
+    double nb = MGF(L, S_AW)[q] * phi[q - 1] + MGF(L, S_AE)[q] * phi[q + 1]
+              + MGF(L, S_AS)[q] * phi[q - nx] + MGF(L, S_AN)[q] * phi[q + nx];
+    phi[q] = (nb + MGF(L, S_SU)[q]) / MGF(L, S_AP)[q];
+}
+
+// ------------------------------------------------------------ restriction
+// restv :1354-1389 at coarse interior cell (ic, jc)
+__device__ __forceinline__ void cell_restv(const LevelDev &F, const LevelDev &K, int ic, int jc)
+{
+    const int nxf = F.npx, qc = jc * K.npx + ic, q = 2 * jc * nxf + 2 * ic, qw = q - 1, qs = q - nxf;
+    const double *uf = MGF(F, S_U), *vf = MGF(F, S_V), *pf = MGF(F, S_P), *sf = MGF(F, S_SC);
+    const double *axf = MGF(F, S_AREAX), *ayf = MGF(F, S_AREAY);
+    MGF(K, S_U)[qc] = (uf[q] * axf[q] + uf[qs] * axf[qs]) / (MGF(K, S_AREAX)[qc] + 1.0e-30);
+    MGF(K, S_V)[qc] = (vf[q] * ayf[q] + vf[qw] * ayf[qw]) / (MGF(K, S_AREAY)[qc] + 1.0e-30);
+    MGF(K, S_P)[qc] = 0.25 * (pf[q] + pf[qw] + pf[qs] + pf[qs - 1]);
+    MGF(K, S_SC)[qc] = 0.25 * (sf[q] + sf[qw] + sf[qs] + sf[qs - 1]);
+}
+
+// residual of the u equation at face (i, j) (restru :1494-1512 fine, :1528-1541 coarse)
+__device__ __forceinline__ double resid_u(const LevelDev &L, const CaseDev &C, int i, int j, bool fine)
+{
+    const int nx = L.npx, q = j * nx + i;
+    Coef k = coef_u(L, i, j);
+    const double *u = MGF(L, S_U), *p = MGF(L, S_P);
+    const double ax = MGF(L, S_AREAX)[q], ay = MGF(L, S_AREAY)[q];
+    double r = k.aw * u[q - 1] + k.ae * u[q + 1] + k.as * u[q - nx] + k.an * u[q + nx]
+             - k.ap * u[q] + ax * (p[q] - p[q + 1]);
+    if (fine) {
+        r = r + MGF(L, S_RESU)[q] + C.dpdxm * ax * ay;
+        if (ax == 0.0) r = 0.0;
+    } else {
+        r = r + C.dpdxm * ax * ay;
+    }
+    return r;
+}
+
+// residual of the v equation (restrv :1670-1688 fine, :1704-1718 coarse)
+__device__ __forceinline__ double resid_v(const LevelDev &L, const CaseDev &C, int i, int j, bool fine)
+{
+    const int nx = L.npx, q = j * nx + i;
+    Coef k = coef_v(L, i, j);
+    const double *v = MGF(L, S_V), *p = MGF(L, S_P);
+    const double ax = MGF(L, S_AREAX)[q], ay = MGF(L, S_AREAY)[q];
+    double r = k.aw * v[q - 1] + k.ae * v[q + 1] + k.as * v[q - nx] + k.an * v[q + nx]
+             - k.ap * v[q] + ay * (p[q] - p[q + nx]);
+    if (fine) {
+        r = r + MGF(L, S_RESV)[q] + C.dpdym * ax * ay;
+        if (ay == 0.0) r = 0.0;
+    } else {
+        r = r + C.dpdym * ax * ay;
+    }
+    return r;
+}
+
+// residual of the scalar equation (restrsc :1585-1600 fine, :1618-1630 coarse)
+__device__ __forceinline__ double resid_sc(const LevelDev &L, int i, int j, bool fine)
+{
+    const int nx = L.npx, q = j * nx + i;
+    Coef k = coef_sc(L, i, j);
+    const double *s = MGF(L, S_SC);
+    double r = k.aw * s[q - 1] + k.ae * s[q + 1] + k.as * s[q - nx] + k.an * s[q + nx] - k.ap * s[q];
+    if (fine) r = r + MGF(L, S_RESSC)[q];
+    return r;
+}
+
+// FAS defects of all three transported equations at coarse cell (ic, jc):
+// restru :1546-1563, restrv :1722-1738, restrsc :1634-1647, each fine residual
+// evaluated where the reference's restriction stencil reads it.
+__device__ __forceinline__ void cell_restrict(const LevelDev &F, const LevelDev &K, const CaseDev &C,
+                                              int ic, int jc)
+{
+    const int nxc = K.npx, nyc = K.npy, qc = jc * nxc + ic;
+    const int i = 2 * ic, j = 2 * jc;
+    if (ic <= nxc - 3) {
+        double r0 = resid_u(F, C, i, j, true), r1 = resid_u(F, C, i, j - 1, true);
+        double r2 = resid_u(F, C, i - 1, j, true), r3 = resid_u(F, C, i - 1, j - 1, true);
+        double r4 = resid_u(F, C, i + 1, j, true), r5 = resid_u(F, C, i + 1, j - 1, true);
+        double rc = resid_u(K, C, ic, jc, false);
+        MGF(K, S_RESU)[qc] = (r0 + r1) + 0.5 * (r2 + r3 + r4 + r5) - rc;
+    }
+    if (jc <= nyc - 3) {
+        double r0 = resid_v(F, C, i, j, true), r1 = resid_v(F, C, i - 1, j, true);
+        double r2 = resid_v(F, C, i, j - 1, true), r3 = resid_v(F, C, i - 1, j - 1, true);
+        double r4 = resid_v(F, C, i, j + 1, true), r5 = resid_v(F, C, i - 1, j + 1, true);
+        double rc = resid_v(K, C, ic, jc, false);
+        MGF(K, S_RESV)[qc] = (r0 + r1) + 0.5 * (r2 + r3 + r4 + r5) - rc;
+    }
+    {
+        double r0 = resid_sc(F, i, j, true), r1 = resid_sc(F, i, j - 1, true);
+        double r2 = resid_sc(F, i - 1, j, true), r3 = resid_sc(F, i - 1, j - 1, true);
+        double rc = resid_sc(K, ic, jc, false);
+        MGF(K, S_RESSC)[qc] = (r0 + r1 + r2 + r3) - rc;
+    }
+}
+
+// ---------------------------------------------------------- prolongation
+// coarse corrections c = x_c - R(x_f) at coarse interior cell (ic, jc):
+// prolu :1760-1777, prolv :1840-1856, prolp :1914-1928, prolsc :1981-1994
+__device__ __forceinline__ void cell_prol_corr(const LevelDev &F, const LevelDev &K, int ic, int jc)
+{
+    const int nxf = F.npx, nxc = K.npx, nyc = K.npy, qc = jc * nxc + ic;
+    const int q = 2 * jc * nxf + 2 * ic, qs = q - nxf;
+    if (ic <= nxc - 3) {
+        const double *u = MGF(F, S_U), *ax = MGF(F, S_AREAX);
+        double r = (u[q] * ax[q] + u[qs] * ax[qs]) / (MGF(K, S_AREAX)[qc] + 1.0E-30);
+        MGF(K, S_CU)[qc] = MGF(K, S_U)[qc] - r;
+    }
+    if (jc <= nyc - 3) {
+        const double *v = MGF(F, S_V), *ay = MGF(F, S_AREAY);
+        double r = (v[q] * ay[q] + v[q - 1] * ay[q - 1]) / (MGF(K, S_AREAY)[qc] + 1.0E-30);
+        MGF(K, S_CV)[qc] = MGF(K, S_V)[qc] - r;
+    }
+    {
+        const double *p = MGF(F, S_P);
+        double r = 0.25 * (p[q] + p[q - 1] + p[qs] + p[qs - 1]);
+        double c = MGF(K, S_P)[qc] - r;
+        if (MGF(F, S_SPU)[q] > 1.0e10) c = 0.0;
+        MGF(K, S_CP)[qc] = c;
+    }
+    {
+        const double *s = MGF(F, S_SC);
+        double r = 0.25 * (s[q] + s[q - 1] + s[qs] + s[qs - 1]);
+        MGF(K, S_C)[qc] = MGF(K, S_SC)[qc] - r;
+    }
+}
+
+// Fine-cell gather of the reference's scatter-add prolongation (same additions in
+// the same order as its sequential loops): fine interior cell (i, j).
+__device__ __forceinline__ void cell_prol_apply(const LevelDev &F, const LevelDev &K, int i, int j)
+{
+    const int nxf = F.npx, nyf = F.npy, nxc = K.npx, nyc = K.npy, q = j * nxf + i;
+    const double f1 = 3. / 4., f2 = 1. / 4.;
+    // u faces, i in [1, nxf-3]: prolu :1782-1814
+    if (i <= nxf - 3) {
+        const double *cu = MGF(K, S_CU);
+        const double *spu = MGF(F, S_SPU);
+        const bool up = (j & 1) == 0;                  // even row: corr1 of jc = j/2
+        const int jc = up ? j / 2 : (j + 1) / 2;       // odd row: corr2 of jc = (j+1)/2
+        const int dj = up ? nxc : -nxc;
+        double u = MGF(F, S_U)[q];
+        if ((i & 1) == 0) {
+            const int ic = i / 2, qc = jc * nxc + ic;
+            double corr = f1 * cu[qc] + f2 * cu[qc + dj];
+            if (spu[2 * jc * nxf + 2 * ic] > 1.0e10) corr = 0.0;
+            u += corr;
+        } else {
+            const int ia = (i - 1) / 2, ib = (i + 1) / 2;
+            if (ia >= 1) {
+                const int qc = jc * nxc + ia;
+                double corr = f1 * cu[qc] + f2 * cu[qc + dj];
+                if (spu[2 * jc * nxf + 2 * ia] > 1.0e10) corr = 0.0;
+                u += 0.5 * corr;
+            }
+            if (ib <= nxc - 3) {
+                const int qc = jc * nxc + ib;
+                double corr = f1 * cu[qc] + f2 * cu[qc + dj];
+                if (spu[2 * jc * nxf + 2 * ib] > 1.0e10) corr = 0.0;
+                u += 0.5 * corr;
+            }
+        }
+        MGF(F, S_U)[q] = u;
+    }
+    // v faces, j in [1, nyf-3]: prolv :1861-1888
+    if (j <= nyf - 3) {
+        const double *cv = MGF(K, S_CV);
+        const double *spv = MGF(F, S_SPV);
+        const bool right = (i & 1) == 0;               // even column: corr1 of ic = i/2
+        const int ic = right ? i / 2 : (i + 1) / 2;
+        const int di = right ? 1 : -1;
+        double v = MGF(F, S_V)[q];
+        if ((j & 1) == 0) {
+            const int jc = j / 2, qc = jc * nxc + ic;
+            double corr = f1 * cv[qc] + f2 * cv[qc + di];
+            if (spv[2 * jc * nxf + 2 * ic] > 1.0e10) corr = 0.0;
+            v += corr;
+        } else {
+            const int ja = (j - 1) / 2, jb = (j + 1) / 2;
+            if (ja >= 1) {
+                const int qc = ja * nxc + ic;
+                double corr = f1 * cv[qc] + f2 * cv[qc + di];
+                if (spv[2 * ja * nxf + 2 * ic] > 1.0e10) corr = 0.0;
+                v += 0.5 * corr;
+            }
+            if (jb <= nyc - 3) {
+                const int qc = jb * nxc + ic;
+                double corr = f1 * cv[qc] + f2 * cv[qc + di];
+                if (spv[2 * jb * nxf + 2 * ic] > 1.0e10) corr = 0.0;
+                v += 0.5 * corr;
+            }
+        }
+        MGF(F, S_V)[q] = v;
+    }
+    // p and sc cells: prolp :1933-1958, prolsc :1999-2025
+    {
+        const double g1 = 9. / 16., g2 = 3. / 16., g3 = 3. / 16., g4 = 1. / 16.;
+        const int ic = (i + 1) / 2, jc = (j + 1) / 2, qc = jc * nxc + ic;
+        const int di = (i & 1) == 0 ? 1 : -1;
+        const int dj = (j & 1) == 0 ? nxc : -nxc;
+        const double *cp = MGF(K, S_CP), *cs = MGF(K, S_C);
+        MGF(F, S_P)[q] += g1 * cp[qc] + g2 * cp[qc + di] + g3 * cp[qc + dj] + g4 * cp[qc + di + dj];
+        MGF(F, S_SC)[q] += g1 * cs[qc] + g2 * cs[qc + di] + g3 * cs[qc + dj] + g4 * cs[qc + di + dj];
+    }
+}
+
+// ---------------------------------------------------------- boundary lines
+// outflow :1211-1228, row j
+__device__ __forceinline__ void row_outflow(const LevelDev &L, int j)
+{
+    const int q = j * L.npx + L.npx - 1;
+    MGF(L, S_U)[q - 1] = MGF(L, S_U)[q - 2];
+    MGF(L, S_V)[q] = MGF(L, S_V)[q - 1];
+    MGF(L, S_P)[q] = MGF(L, S_P)[q - 1];
+    MGF(L, S_SC)[q] = MGF(L, S_SC)[q - 1];
+}
+
+// pbound x-periodic :1185-1195, row j in [1, npy-2]
+__device__ __forceinline__ void row_periodic_x(const LevelDev &L, int j)
+{
+    double *u = MGF(L, S_U), *v = MGF(L, S_V);
+    const int q = j * L.npx, q1 = q + L.npx - 3;
+    u[q] = u[q1]; u[q1 + 1] = u[q + 1];
+    v[q] = v[q1]; v[q1 + 1] = v[q + 1];
+}
+
+// pbound y-periodic :1197-1208; sequential: later iterations read cells earlier
+// iterations wrote (the reference's flat offset i + npy - 3), so one thread runs it.
+__device__ __forceinline__ void line_periodic_y(const LevelDev &L)
+{
+    double *u = MGF(L, S_U), *v = MGF(L, S_V);
+    const int nx = L.npx, ny = L.npy;
+    for (int i = 1; i < nx - 1; ++i) {
+        const int q = i, q1 = q + ny - 3;
+        u[q] = u[q1]; u[q1 + nx] = u[q + nx];
+        v[q] = v[q1]; v[q1 + nx] = v[q + nx];
+    }
+}
+
+}  // namespace mg

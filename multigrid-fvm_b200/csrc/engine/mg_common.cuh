@@ -1,0 +1,109 @@
+// mg_common.cuh — device-side data layout of the engine.
+//
+// HBM layout: one pool allocation per context.  Every (case, level) owns NSLOTS
+// FP64 arrays of npx*npy in the reference's row-major order (ij = j*npx + i,
+// Version-6-26-04.c:554), each aligned to 256 B, plus an int tag array and an
+// optional per-cell obstacle-code array.  Slots 0..24 are the arrays of the
+// reference's struct SoA (:42-54) in the order of enum mgfvm_field; the rest are
+// engine buffers: the Jacobi ping-pong array, one prolongation correction per
+// variable (the reference shares one `c`, :1745-2028), and the level-0 state of
+// the previous cycle for the fixed-point test.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "mgfvm.h"
+
+namespace mg {
+
+enum Slot {
+    S_U = MGFVM_F_U, S_V = MGFVM_F_V, S_P = MGFVM_F_P, S_PP = MGFVM_F_PP, S_SC = MGFVM_F_SC,
+    S_SU = MGFVM_F_SU, S_RS = MGFVM_F_RS, S_RESU = MGFVM_F_RESU, S_RESV = MGFVM_F_RESV,
+    S_RESSC = MGFVM_F_RESSC, S_C = MGFVM_F_C,     // S_C: the scalar correction (prolsc's c)
+    S_AW = MGFVM_F_AW, S_AE = MGFVM_F_AE, S_AS = MGFVM_F_AS, S_AN = MGFVM_F_AN,
+    S_AP = MGFVM_F_AP, S_APU = MGFVM_F_APU, S_APV = MGFVM_F_APV, S_SPU = MGFVM_F_SPU,
+    S_SPV = MGFVM_F_SPV, S_SPSC = MGFVM_F_SPSC, S_CX = MGFVM_F_CX, S_CY = MGFVM_F_CY,
+    S_AREAX = MGFVM_F_AREAX, S_AREAY = MGFVM_F_AREAY,
+    S_TMP = MGFVM_NFIELDS,   // Jacobi ping-pong buffer
+    S_CU, S_CV, S_CP,        // u, v, p prolongation corrections
+    NSLOTS_LEVEL,
+    S_PREV_U = NSLOTS_LEVEL, S_PREV_V, S_PREV_P, S_PREV_SC,   // level 0 only
+    NSLOTS
+};
+
+constexpr int MAXLEV = 16;
+constexpr int RED_STRIDE = 16;   // doubles per block in the reduction partials
+
+// One multigrid level of one case.
+struct LevelDev {
+    int npx, npy;
+    int ncopy;          // pressure-copy program length (update's obstacle loop)
+    int hazard;         // the copy program reads a cell it also writes
+    double dx, dy;
+    double amu;         // viscosity on this level (amuf, :419)
+    double amusc;       // scalar diffusivity amuf/prsc (:867)
+    double *f[NSLOTS];
+    int *tag;
+    const unsigned *seq;  // per-cell obstacle-face addition codes, or nullptr
+    const int *pdst;
+    const int *psrc;
+    double *pbuf;
+};
+
+// Stop-rule and status flags of one case.
+enum CaseStatus { CASE_RUNNING = 0, CASE_CONVERGED_REF = 1, CASE_CONVERGED_FP = 2,
+                  CASE_NONFINITE = 4 };
+
+struct CaseDev {
+    // physics and boundary codes shared by every level (Version-6-26-04.c:30-35)
+    double relxm, relxp, sc_obs, dpdxm, dpdym, convergence;
+    int ibc_xm, ibc_xp, ibc_ym, ibc_yp;
+    int ngrid;
+    int tail;           // first level run by the one-CTA coarse kernel (== ngrid: none)
+    int done;           // stop rule fired; every kernel skips this case
+    int status;         // enum CaseStatus bits
+    int ncyc;           // cycles recorded in the history
+    int hist_cap;
+    int have_prev;      // level-0 state of a previous cycle is in S_PREV_*
+    int stop_enabled;   // evaluate the stop rule at the end of every cycle
+    double fp_tol;
+    double last_err;    // level-0 sum|div| of the current cycle
+    double shift_d, shift_p;  // last cycle's mean p change and mean p (shifted sums)
+    double *hist_err, *hist_delta;
+    double *partials;   // RED_STRIDE doubles per block, reduction scratch
+    unsigned *counters; // [0] mass error, [1] end of cycle
+    LevelDev lv[MAXLEV];
+};
+
+// ---------------------------------------------------------------- modes
+// Which cases a launch at level `ig` touches.  Transfers are launched at their fine
+// level; M_*_C launches act on the coarse level of a transfer whose fine level is ig-1.
+enum Mode {
+    M_OP = 0,       // single-step op on level ig
+    M_OP_PAIR,      // single-step transfer between ig and ig+1
+    M_OP_C,         // coarse side (ig) of a single-step transfer from ig-1
+    M_DOWN,         // down-leg SIMPLE step on a grid-run level
+    M_RESTRICT,     // restriction ig -> ig+1 from a grid-run level
+    M_RESTRICT_C,   // coarse side (ig) of M_RESTRICT at ig-1
+    M_PROLONG,      // prolongation ig+1 -> ig into a grid-run level
+    M_UP            // up-leg SIMPLE step on level ig after M_PROLONG
+};
+
+__device__ __forceinline__ bool case_active(const CaseDev &C, int ig, int mode)
+{
+    if (C.done) return false;
+    switch (mode) {
+    case M_OP: return ig < C.ngrid;
+    case M_OP_PAIR: return ig + 1 < C.ngrid;
+    case M_OP_C: return ig >= 1 && ig < C.ngrid;
+    case M_DOWN: return ig < C.tail;
+    case M_RESTRICT: return ig < C.tail && ig + 1 < C.ngrid;
+    case M_RESTRICT_C: return ig >= 1 && ig - 1 < C.tail && ig < C.ngrid;
+    case M_PROLONG:
+    case M_UP: return ig + 1 <= C.tail && ig + 1 < C.ngrid;
+    default: return false;
+    }
+}
+
+}  // namespace mg

@@ -1,0 +1,897 @@
+// mg_context.cu — the C ABI of include/mgfvm.h on top of the engine's kernels.
+//
+// A context owns every level of every case of a batch in one device pool, builds
+// the launch schedule of one V-cycle (Version-6-26-04.c:195-249) once, captures it
+// in a CUDA graph and replays that graph; the stop rule is evaluated on the device
+// at the end of every cycle, so the host only polls per-case flags every
+// `sync_every` cycles and a converged case costs nothing but early-exiting blocks.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "mg_init.cuh"
+#include "mg_kernels.cuh"
+#include "mgfvm_host.h"
+
+using namespace mg;
+
+#define CK(call)                                                                                 \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess)                                                                   \
+            return mgfvm_fail(MGFVM_ECUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                              __FILE__, __LINE__);                                               \
+    } while (0)
+
+#define RC(call)                   \
+    do {                           \
+        int r_ = (call);           \
+        if (r_ != MGFVM_OK) return r_; \
+    } while (0)
+
+static const int TAIL_AUTO_CELLS = 70 * 70;   // levels at or below ~66x66 padded cells
+static const int HIST_INITIAL = 4096;
+
+struct mgfvm_ctx {
+    int device = 0;
+    mgfvm_options opt{};
+    int ncases = 0;
+    int maxng = 0;
+    Sched sched{};
+    std::vector<mgfvm_config> cfg;
+    std::vector<std::vector<int>> obs;
+    std::vector<std::vector<double>> profile;
+    std::vector<mgfvm_obstacle_prog> progs;   // ncases * MAXLEV
+    std::vector<CaseDev> hc;
+    std::vector<InitDev> hinit;
+    CaseDev *dc = nullptr;
+    InitDev *dinit = nullptr;
+    char *pool = nullptr;
+    double *hist = nullptr;
+    int hist_cap = 0;
+    double *dprofile = nullptr;
+    int *dobs = nullptr;
+    int *hflags = nullptr;                    // pinned readback of the per-case done flags
+    cudaStream_t stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    std::vector<Launch> cyc;
+    std::vector<int> maxcells;                // per level: max npx*npy over cases
+    long long launches = 0;
+    long long h2d = 0, d2h = 0;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    double last_ms = 0.0;
+};
+
+static inline int npx_of(const mgfvm_config &c, int ig) { return c.nfx / (1 << ig) + 2; }
+static inline int npy_of(const mgfvm_config &c, int ig) { return c.nfy / (1 << ig) + 2; }
+static inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+static inline int nblk(long long n) { return (int)std::max<long long>(1, (n + BLOCK - 1) / BLOCK); }
+
+// ------------------------------------------------------------------ schedule
+namespace {
+
+// Host mirror of case_active() in mg_common.cuh (without the per-case done flag).
+bool host_active(const CaseDev &C, int ig, int mode)
+{
+    switch (mode) {
+    case M_OP: return ig < C.ngrid;
+    case M_OP_PAIR: return ig + 1 < C.ngrid;
+    case M_OP_C: return ig >= 1 && ig < C.ngrid;
+    case M_DOWN: return ig < C.tail;
+    case M_RESTRICT: return ig < C.tail && ig + 1 < C.ngrid;
+    case M_RESTRICT_C: return ig >= 1 && ig - 1 < C.tail && ig < C.ngrid;
+    case M_PROLONG:
+    case M_UP: return ig + 1 <= C.tail && ig + 1 < C.ngrid;
+    default: return false;
+    }
+}
+
+struct Builder {
+    mgfvm_ctx *x;
+    std::vector<Launch> *out;
+
+    bool any(int ig, int mode) const
+    {
+        for (const CaseDev &C : x->hc)
+            if (host_active(C, ig, mode)) return true;
+        return false;
+    }
+    void add(int kernel, int ig, int mode, long long cells, int a0 = 0, int a1 = 0)
+    {
+        Launch L{};
+        L.kernel = kernel; L.ig = ig; L.mode = mode; L.a0 = a0; L.a1 = a1;
+        L.grid = dim3(nblk(cells), x->ncases);
+        L.block = BLOCK;
+        out->push_back(L);
+    }
+    long long cells(int ig) const { return ig < (int)x->maxcells.size() ? x->maxcells[ig] : 0; }
+    long long half_cells(int ig) const
+    {
+        long long m = 0;
+        for (const mgfvm_config &c : x->cfg)
+            if (ig < c.ngrid) m = std::max<long long>(m, (long long)(npx_of(c, ig) / 2 + 1) * npy_of(c, ig));
+        return m;
+    }
+    void smooth(int ig, int mode, int e)
+    {
+        const int nsw = e == 2 ? x->sched.nswpp : x->sched.nswpm;
+        if (x->sched.isolve == MGFVM_JACOBI) {
+            for (int it = 0; it < nsw; ++it) add(K_JACOBI, ig, mode, cells(ig), e, it);
+            if (nsw & 1) add(K_JACOBI_COPYBACK, ig, mode, cells(ig), e);
+        } else {
+            for (int it = 0; it < nsw; ++it)
+                for (int c = 0; c < 2; ++c) add(K_GS, ig, mode, half_cells(ig), e, c);
+        }
+    }
+    void pfix(int ig, int mode)
+    {
+        int maxcopy = 0, haz = 0;
+        for (int c = 0; c < x->ncases; ++c) {
+            if (!host_active(x->hc[c], ig, mode)) continue;
+            const mgfvm_obstacle_prog &P = x->progs[c * MAXLEV + ig];
+            maxcopy = std::max(maxcopy, P.ncopy);
+            haz |= P.hazard;
+        }
+        if (maxcopy == 0) return;
+        if (haz) { add(K_PFIX, ig, mode, maxcopy, 0); add(K_PFIX, ig, mode, maxcopy, 1); }
+        else add(K_PFIX, ig, mode, maxcopy, 2);
+    }
+    bool any_bc(int which) const
+    {
+        for (const CaseDev &C : x->hc) {
+            if (which == 0 && (C.ibc_xm == 3 || C.ibc_ym == 3)) return true;
+            if (which == 1 && C.ibc_xp == 4) return true;
+        }
+        return false;
+    }
+    void periodic(int ig, int mode)
+    {
+        if (!any_bc(0)) return;
+        Launch L{};
+        L.kernel = K_PERIODIC; L.ig = ig; L.mode = mode;
+        L.grid = dim3(1, x->ncases); L.block = BLOCK;
+        out->push_back(L);
+    }
+    void outflow(int ig, int mode)
+    {
+        if (!any_bc(1)) return;
+        long long m = 0;
+        for (const mgfvm_config &c : x->cfg) if (ig < c.ngrid) m = std::max<long long>(m, npy_of(c, ig));
+        add(K_OUTFLOW, ig, mode, m);
+    }
+    void solve_u(int ig, int mode) { add(K_MOM_U, ig, mode, cells(ig)); smooth(ig, mode, 0); }
+    void solve_v(int ig, int mode) { add(K_MOM_V, ig, mode, cells(ig)); smooth(ig, mode, 1); }
+    void solve_pp(int ig, int mode, bool reduce)
+    {
+        add(K_MASS_COEFP, ig, mode, cells(ig), reduce ? 1 : 0);
+        smooth(ig, mode, 2);
+        add(K_UPDATE, ig, mode, cells(ig));
+        pfix(ig, mode);
+    }
+    void solve_sc(int ig, int mode) { add(K_SC, ig, mode, cells(ig)); smooth(ig, mode, 3); }
+    // one SIMPLE step: down leg :201-207, up leg :235-244
+    void step(int ig, int mode, bool down, bool reduce)
+    {
+        add(K_FLUXES, ig, mode, cells(ig));
+        solve_u(ig, mode);
+        solve_v(ig, mode);
+        solve_pp(ig, mode, reduce);
+        periodic(ig, mode);
+        if (down) outflow(ig, mode);
+        solve_sc(ig, mode);
+        if (!down) outflow(ig, mode);
+    }
+    // :211-220
+    void restrict_(int ig, int mode_f, int mode_c)
+    {
+        add(K_RESTV, ig, mode_f, cells(ig + 1));
+        add(K_FLUXES, ig + 1, mode_c, cells(ig + 1));
+        add(K_FLUXES, ig, mode_f, cells(ig));
+        add(K_RESTRICT, ig, mode_f, cells(ig + 1));
+    }
+    // :230-233
+    void prolong(int ig, int mode)
+    {
+        add(K_PROL_CORR, ig, mode, cells(ig + 1));
+        add(K_PROL_APPLY, ig, mode, cells(ig));
+    }
+    void cycle()
+    {
+        for (int ig = 0; ig < x->maxng; ++ig) {
+            if (any(ig, M_DOWN)) step(ig, M_DOWN, true, ig == 0);
+            if (any(ig, M_RESTRICT)) restrict_(ig, M_RESTRICT, M_RESTRICT_C);
+        }
+        bool tail = false;
+        for (const CaseDev &C : x->hc) tail |= C.tail < C.ngrid;
+        if (tail) {
+            Launch L{};
+            L.kernel = K_TAIL; L.grid = dim3(x->ncases); L.block = TAIL_BLOCK;
+            out->push_back(L);
+        }
+        for (int ig = x->maxng - 1; ig > 0; --ig) {
+            if (!any(ig - 1, M_PROLONG)) continue;
+            prolong(ig - 1, M_PROLONG);
+            if (ig != 1) step(ig - 1, M_UP, false, false);
+        }
+        Launch L{};
+        L.kernel = K_ENDCYCLE;
+        long long n0 = 0;
+        for (const mgfvm_config &c : x->cfg)
+            n0 = std::max<long long>(n0, (long long)(npx_of(c, 0) - 2) * (npy_of(c, 0) - 2));
+        L.grid = dim3(nblk(n0), x->ncases);
+        L.block = BLOCK;
+        out->push_back(L);
+    }
+    void op(int op, int ig)
+    {
+        switch (op) {
+        case MGFVM_OP_FLUXES: add(K_FLUXES, ig, M_OP, cells(ig)); break;
+        case MGFVM_OP_SOLVE_U: solve_u(ig, M_OP); break;
+        case MGFVM_OP_SOLVE_V: solve_v(ig, M_OP); break;
+        case MGFVM_OP_SOLVE_PP: solve_pp(ig, M_OP, true); break;
+        case MGFVM_OP_PBOUND: periodic(ig, M_OP); break;
+        case MGFVM_OP_OUTFLOW: outflow(ig, M_OP); break;
+        case MGFVM_OP_SOLVE_SC: solve_sc(ig, M_OP); break;
+        case MGFVM_OP_RESTRICT: restrict_(ig, M_OP_PAIR, M_OP_C); break;
+        case MGFVM_OP_PROLONG: prolong(ig, M_OP_PAIR); break;
+        case MGFVM_OP_SMOOTH_U: smooth(ig, M_OP, 0); break;
+        case MGFVM_OP_SMOOTH_V: smooth(ig, M_OP, 1); break;
+        case MGFVM_OP_SMOOTH_PP: smooth(ig, M_OP, 2); break;
+        case MGFVM_OP_SMOOTH_SC: smooth(ig, M_OP, 3); break;
+        default: break;
+        }
+    }
+};
+
+int run_list(mgfvm_ctx *x, const std::vector<Launch> &v)
+{
+    for (const Launch &L : v) {
+        cudaError_t e = launch_one(L, x->dc, x->sched, x->stream);
+        if (e != cudaSuccess)
+            return mgfvm_fail(MGFVM_ECUDA, "kernel %d at level %d failed to launch: %s", L.kernel, L.ig,
+                              cudaGetErrorString(e));
+    }
+    x->launches += (long long)v.size();
+    return MGFVM_OK;
+}
+
+int pull(mgfvm_ctx *x)
+{
+    CK(cudaStreamSynchronize(x->stream));
+    CK(cudaMemcpy(x->hc.data(), x->dc, sizeof(CaseDev) * x->ncases, cudaMemcpyDeviceToHost));
+    x->d2h += (long long)sizeof(CaseDev) * x->ncases;
+    return MGFVM_OK;
+}
+
+int push(mgfvm_ctx *x)
+{
+    CK(cudaMemcpy(x->dc, x->hc.data(), sizeof(CaseDev) * x->ncases, cudaMemcpyHostToDevice));
+    x->h2d += (long long)sizeof(CaseDev) * x->ncases;
+    return MGFVM_OK;
+}
+
+int ensure_hist(mgfvm_ctx *x, int need)
+{
+    if (need <= x->hist_cap) return MGFVM_OK;
+    int cap = std::max(HIST_INITIAL, x->hist_cap);
+    while (cap < need) cap *= 2;
+    RC(pull(x));
+    double *h = nullptr;
+    CK(cudaMalloc(&h, sizeof(double) * 2 * (size_t)cap * x->ncases));
+    CK(cudaMemset(h, 0, sizeof(double) * 2 * (size_t)cap * x->ncases));
+    if (x->hist && x->hist_cap > 0)
+        CK(cudaMemcpy2D(h, sizeof(double) * cap, x->hist, sizeof(double) * x->hist_cap,
+                        sizeof(double) * x->hist_cap, 2 * (size_t)x->ncases, cudaMemcpyDeviceToDevice));
+    if (x->hist) cudaFree(x->hist);
+    x->hist = h;
+    x->hist_cap = cap;
+    for (int c = 0; c < x->ncases; ++c) {
+        x->hc[c].hist_err = h + (size_t)(2 * c) * cap;
+        x->hc[c].hist_delta = h + (size_t)(2 * c + 1) * cap;
+        x->hc[c].hist_cap = cap;
+    }
+    return push(x);
+}
+
+int build_graph(mgfvm_ctx *x)
+{
+    if (x->gexec) return MGFVM_OK;
+    CK(cudaStreamBeginCapture(x->stream, cudaStreamCaptureModeThreadLocal));
+    for (const Launch &L : x->cyc) {
+        cudaError_t e = launch_one(L, x->dc, x->sched, x->stream);
+        if (e != cudaSuccess) {
+            cudaGraph_t g;
+            cudaStreamEndCapture(x->stream, &g);
+            if (g) cudaGraphDestroy(g);
+            return mgfvm_fail(MGFVM_ECUDA, "graph capture: %s", cudaGetErrorString(e));
+        }
+    }
+    CK(cudaStreamEndCapture(x->stream, &x->graph));
+    CK(cudaGraphInstantiate(&x->gexec, x->graph, 0));
+    return MGFVM_OK;
+}
+
+int run_cycles(mgfvm_ctx *x, int n)
+{
+    if (x->opt.use_graph) {
+        RC(build_graph(x));
+        for (int k = 0; k < n; ++k) CK(cudaGraphLaunch(x->gexec, x->stream));
+        x->launches += (long long)n * (long long)x->cyc.size();
+    } else {
+        for (int k = 0; k < n; ++k) RC(run_list(x, x->cyc));
+    }
+    return MGFVM_OK;
+}
+
+int set_controls(mgfvm_ctx *x, int stop, double fp_tol)
+{
+    RC(pull(x));
+    for (CaseDev &C : x->hc) {
+        C.done = 0;
+        C.stop_enabled = stop;
+        C.fp_tol = fp_tol;
+    }
+    return push(x);
+}
+
+int init_state(mgfvm_ctx *x, int only_case)
+{
+    for (int c = 0; c < x->ncases; ++c) {
+        if (only_case >= 0 && c != only_case) continue;
+        CaseDev &C = x->hc[c];
+        C.done = 0; C.status = 0; C.ncyc = 0; C.have_prev = 0; C.stop_enabled = 0;
+        C.last_err = 0.0; C.shift_d = 0.0; C.shift_p = 0.0;
+    }
+    RC(push(x));
+    int max_obs = 0, max_npy = 0;
+    for (int c = 0; c < x->ncases; ++c) {
+        if (only_case >= 0 && c != only_case) continue;
+        max_obs = std::max(max_obs, x->cfg[c].nobs);
+        max_npy = std::max(max_npy, npy_of(x->cfg[c], 0));
+    }
+    CaseDev *dc = x->dc + (only_case >= 0 ? only_case : 0);
+    InitDev *di = x->dinit + (only_case >= 0 ? only_case : 0);
+    const int n = only_case >= 0 ? 1 : x->ncases;
+    cudaError_t e = launch_init(dc, di, n, x->maxng, x->maxcells.data(), max_obs, max_npy, x->stream);
+    if (e != cudaSuccess) return mgfvm_fail(MGFVM_ECUDA, "init kernels: %s", cudaGetErrorString(e));
+    x->launches += 3LL * x->maxng + 1 + (x->maxng - 1);
+    CK(cudaStreamSynchronize(x->stream));
+    return MGFVM_OK;
+}
+
+int upload_profiles(mgfvm_ctx *x)
+{
+    size_t tot = 0;
+    for (auto &p : x->profile) tot += p.size();
+    if (x->dprofile) { cudaFree(x->dprofile); x->dprofile = nullptr; }
+    if (tot) {
+        CK(cudaMalloc(&x->dprofile, sizeof(double) * tot));
+    }
+    size_t off = 0;
+    for (int c = 0; c < x->ncases; ++c) {
+        auto &p = x->profile[c];
+        x->hinit[c].profile = p.empty() ? nullptr : x->dprofile + off;
+        x->hinit[c].nprofile = (int)p.size();
+        if (!p.empty()) CK(cudaMemcpy(x->dprofile + off, p.data(), sizeof(double) * p.size(), cudaMemcpyHostToDevice));
+        x->h2d += (long long)(sizeof(double) * p.size());
+        off += p.size();
+    }
+    CK(cudaMemcpy(x->dinit, x->hinit.data(), sizeof(InitDev) * x->ncases, cudaMemcpyHostToDevice));
+    x->h2d += (long long)sizeof(InitDev) * x->ncases;
+    return MGFVM_OK;
+}
+
+void destroy_all(mgfvm_ctx *x)
+{
+    if (!x) return;
+    if (x->device >= 0) cudaSetDevice(x->device);
+    if (x->stream) cudaStreamSynchronize(x->stream);
+    if (x->gexec) cudaGraphExecDestroy(x->gexec);
+    if (x->graph) cudaGraphDestroy(x->graph);
+    if (x->pool) cudaFree(x->pool);
+    if (x->hist) cudaFree(x->hist);
+    if (x->dprofile) cudaFree(x->dprofile);
+    if (x->dobs) cudaFree(x->dobs);
+    if (x->dc) cudaFree(x->dc);
+    if (x->dinit) cudaFree(x->dinit);
+    if (x->hflags) cudaFreeHost(x->hflags);
+    if (x->e0) cudaEventDestroy(x->e0);
+    if (x->e1) cudaEventDestroy(x->e1);
+    if (x->stream) cudaStreamDestroy(x->stream);
+    for (auto &p : x->progs) mgfvm_free_obstacle_prog(&p);
+    delete x;
+}
+
+int check_ctx(mgfvm_ctx *x)
+{
+    if (!x) return mgfvm_fail(MGFVM_EINVAL, "null context");
+    CK(cudaSetDevice(x->device));
+    return MGFVM_OK;
+}
+
+int check_case_level(mgfvm_ctx *x, int icase, int level)
+{
+    if (icase < 0 || icase >= x->ncases) return mgfvm_fail(MGFVM_EINVAL, "case %d outside [0, %d)", icase, x->ncases);
+    if (level < 0 || level >= x->cfg[icase].ngrid)
+        return mgfvm_fail(MGFVM_EINVAL, "level %d outside [0, %d)", level, x->cfg[icase].ngrid);
+    return MGFVM_OK;
+}
+
+int create_impl(const mgfvm_config *cases, int ncases, const mgfvm_options *opt_in, mgfvm_ctx *x)
+{
+    mgfvm_options opt;
+    if (opt_in) opt = *opt_in; else mgfvm_options_default(&opt);
+    if (opt.sync_every < 1) opt.sync_every = 1;
+    if (opt.precision != MGFVM_PREC_FP64)
+        return mgfvm_fail(MGFVM_EUNSUPPORTED, "precision %d not available in this build", opt.precision);
+    x->opt = opt;
+    x->device = opt.device;
+    x->ncases = ncases;
+    for (int c = 0; c < ncases; ++c) RC(mgfvm_config_validate(&cases[c]));
+    for (int c = 1; c < ncases; ++c)
+        if (cases[c].isolve != cases[0].isolve || cases[c].nswpm != cases[0].nswpm ||
+            cases[c].nswpp != cases[0].nswpp)
+            return mgfvm_fail(MGFVM_EINVAL, "case %d: isolve/nswpm/nswpp differ from case 0; a batch "
+                                            "shares one smoothing schedule", c);
+    x->sched.isolve = cases[0].isolve;
+    x->sched.nswpm = cases[0].nswpm;
+    x->sched.nswpp = cases[0].nswpp;
+    x->cfg.assign(cases, cases + ncases);
+    x->obs.resize(ncases);
+    x->profile.resize(ncases);
+    for (int c = 0; c < ncases; ++c) {
+        x->obs[c].assign(cases[c].obs, cases[c].obs + 4 * (size_t)cases[c].nobs);
+        x->cfg[c].obs = x->obs[c].empty() ? nullptr : x->obs[c].data();
+        x->cfg[c].dpdxm = 0.0;   // never read by the reference (:33), so always 0 there
+        x->cfg[c].dpdym = 0.0;
+        x->maxng = std::max(x->maxng, cases[c].ngrid);
+    }
+    if (x->maxng > MAXLEV) return mgfvm_fail(MGFVM_EINVAL, "ngrid above %d", MAXLEV);
+    x->maxcells.assign(x->maxng, 0);
+    for (int c = 0; c < ncases; ++c)
+        for (int ig = 0; ig < x->cfg[c].ngrid; ++ig)
+            x->maxcells[ig] = std::max(x->maxcells[ig], npx_of(x->cfg[c], ig) * npy_of(x->cfg[c], ig));
+
+    // obstacle programs (host)
+    x->progs.assign((size_t)ncases * MAXLEV, mgfvm_obstacle_prog{});
+    for (int c = 0; c < ncases; ++c)
+        for (int ig = 0; ig < x->cfg[c].ngrid; ++ig)
+            RC(mgfvm_build_obstacle_prog(&x->cfg[c], ig, &x->progs[(size_t)c * MAXLEV + ig]));
+
+    CK(cudaSetDevice(x->device));
+    CK(cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&x->e0));
+    CK(cudaEventCreate(&x->e1));
+    CK(cudaMallocHost(&x->hflags, sizeof(int) * ncases));
+
+    // pool layout: pass 0 sizes, pass 1 assigns
+    x->hc.assign(ncases, CaseDev{});
+    std::vector<size_t> off_slots;
+    size_t off = 0;
+    auto take = [&](size_t bytes) { off = align_up(off, 256); size_t o = off; off += std::max<size_t>(bytes, 8); return o; };
+    struct Pend { int c, ig; size_t slot[NSLOTS]; size_t tag, seq, pdst, psrc, pbuf; };
+    std::vector<Pend> pend;
+    std::vector<size_t> part_off(ncases), cnt_off(ncases);
+    for (int c = 0; c < ncases; ++c) {
+        const mgfvm_config &g = x->cfg[c];
+        for (int ig = 0; ig < g.ngrid; ++ig) {
+            Pend p{};
+            p.c = c; p.ig = ig;
+            const size_t n = (size_t)npx_of(g, ig) * npy_of(g, ig);
+            const int ns = ig == 0 ? NSLOTS : NSLOTS_LEVEL;
+            for (int s = 0; s < NSLOTS; ++s) p.slot[s] = s < ns ? take(n * sizeof(double)) : (size_t)-1;
+            p.tag = take(n * sizeof(int));
+            const mgfvm_obstacle_prog &P = x->progs[(size_t)c * MAXLEV + ig];
+            p.seq = P.nseq ? take(n * sizeof(unsigned)) : (size_t)-1;
+            p.pdst = P.ncopy ? take(P.ncopy * sizeof(int)) : (size_t)-1;
+            p.psrc = P.ncopy ? take(P.ncopy * sizeof(int)) : (size_t)-1;
+            p.pbuf = P.ncopy ? take(P.ncopy * sizeof(double)) : (size_t)-1;
+            pend.push_back(p);
+        }
+        const long long n0 = (long long)(npx_of(g, 0) - 2) * (npy_of(g, 0) - 2);
+        part_off[c] = take((size_t)nblk(n0) * RED_STRIDE * sizeof(double));
+        cnt_off[c] = take(16 * sizeof(unsigned));
+    }
+    const size_t pool_bytes = align_up(off, 256);
+    cudaError_t me = cudaMalloc(&x->pool, pool_bytes);
+    if (me != cudaSuccess)
+        return mgfvm_fail(me == cudaErrorMemoryAllocation ? MGFVM_ENOMEM : MGFVM_ECUDA,
+                          "device pool of %zu bytes: %s", pool_bytes, cudaGetErrorString(me));
+    CK(cudaMemset(x->pool, 0, pool_bytes));
+
+    for (int c = 0; c < ncases; ++c) {
+        CaseDev &C = x->hc[c];
+        const mgfvm_config &g = x->cfg[c];
+        C.relxm = g.relxm; C.relxp = g.relxp; C.sc_obs = g.sc_obs;
+        C.dpdxm = g.dpdxm; C.dpdym = g.dpdym; C.convergence = g.convergence;
+        C.ibc_xm = g.ibc_xm; C.ibc_xp = g.ibc_xp; C.ibc_ym = g.ibc_ym; C.ibc_yp = g.ibc_yp;
+        C.ngrid = g.ngrid;
+        int tail = g.ngrid;
+        if (opt.tail_level >= 0) tail = std::min(opt.tail_level, g.ngrid);
+        else
+            for (int ig = 0; ig < g.ngrid; ++ig)
+                if (npx_of(g, ig) * npy_of(g, ig) <= TAIL_AUTO_CELLS) { tail = ig; break; }
+        C.tail = tail;
+        C.partials = (double *)(x->pool + part_off[c]);
+        C.counters = (unsigned *)(x->pool + cnt_off[c]);
+    }
+    for (const Pend &p : pend) {
+        CaseDev &C = x->hc[p.c];
+        LevelDev &L = C.lv[p.ig];
+        const mgfvm_config &g = x->cfg[p.c];
+        L.npx = npx_of(g, p.ig);
+        L.npy = npy_of(g, p.ig);
+        L.dx = g.xl / (L.npx - 2);       // AllocateMemorySoA :413-414
+        L.dy = g.yl / (L.npy - 2);
+        L.amu = g.amuf;
+        L.amusc = g.amuf / g.prsc;       // coefsc :867
+        for (int s = 0; s < NSLOTS; ++s) L.f[s] = p.slot[s] == (size_t)-1 ? nullptr : (double *)(x->pool + p.slot[s]);
+        L.tag = (int *)(x->pool + p.tag);
+        const mgfvm_obstacle_prog &P = x->progs[(size_t)p.c * MAXLEV + p.ig];
+        L.ncopy = P.ncopy;
+        L.hazard = P.hazard;
+        L.seq = nullptr; L.pdst = nullptr; L.psrc = nullptr; L.pbuf = nullptr;
+        if (P.nseq) {
+            const size_t n = (size_t)L.npx * L.npy;
+            std::vector<unsigned> dense(n, 0u);
+            for (int k = 0; k < P.nseq; ++k) dense[P.cells[k]] = P.codes[k];
+            unsigned *d = (unsigned *)(x->pool + p.seq);
+            CK(cudaMemcpy(d, dense.data(), n * sizeof(unsigned), cudaMemcpyHostToDevice));
+            x->h2d += (long long)(n * sizeof(unsigned));
+            L.seq = d;
+        }
+        if (P.ncopy) {
+            int *dd = (int *)(x->pool + p.pdst), *ds = (int *)(x->pool + p.psrc);
+            CK(cudaMemcpy(dd, P.dst, P.ncopy * sizeof(int), cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(ds, P.src, P.ncopy * sizeof(int), cudaMemcpyHostToDevice));
+            x->h2d += 2LL * P.ncopy * (long long)sizeof(int);
+            L.pdst = dd; L.psrc = ds;
+            L.pbuf = (double *)(x->pool + p.pbuf);
+        }
+    }
+
+    // init parameters
+    size_t nobs_tot = 0;
+    for (int c = 0; c < ncases; ++c) nobs_tot += x->obs[c].size();
+    if (nobs_tot) CK(cudaMalloc(&x->dobs, sizeof(int) * nobs_tot));
+    x->hinit.assign(ncases, InitDev{});
+    size_t ooff = 0;
+    for (int c = 0; c < ncases; ++c) {
+        const mgfvm_config &g = x->cfg[c];
+        InitDev &P = x->hinit[c];
+        P.guess[0] = g.u_guess; P.guess[1] = g.v_guess; P.guess[2] = g.p_guess; P.guess[3] = g.sc_guess;
+        const double bc[4][4] = {{g.u_xm, g.v_xm, g.p_xm, g.sc_xm}, {g.u_xp, g.v_xp, g.p_xp, g.sc_xp},
+                                 {g.u_ym, g.v_ym, g.p_ym, g.sc_ym}, {g.u_yp, g.v_yp, g.p_yp, g.sc_yp}};
+        std::memcpy(P.bc, bc, sizeof bc);
+        P.sc_obs = g.sc_obs;
+        P.ig_obs = g.ig_obs; P.ibeg_obs = g.ibeg_obs; P.nobs = g.nobs;
+        P.obs = nullptr;
+        if (g.nobs) {
+            CK(cudaMemcpy(x->dobs + ooff, x->obs[c].data(), sizeof(int) * x->obs[c].size(), cudaMemcpyHostToDevice));
+            x->h2d += (long long)(sizeof(int) * x->obs[c].size());
+            P.obs = x->dobs + ooff;
+            ooff += x->obs[c].size();
+        }
+        P.ig_inlt = g.ig_inlt; P.ninlt = g.ninlt; P.ig_outlt = g.ig_outlt; P.noutlt = g.noutlt;
+        for (int k = 0; k < MGFVM_MAX_PORTS; ++k) {
+            P.jf_in[k] = g.jfinlt[k]; P.jl_in[k] = g.jlinlt[k];
+            P.jf_out[k] = g.jfoutlt[k]; P.jl_out[k] = g.jloutlt[k];
+            P.in_val[k][0] = g.uinlt[k]; P.in_val[k][1] = g.vinlt[k]; P.in_val[k][2] = g.scinlt[k];
+            P.out_val[k][0] = g.uoutlt[k]; P.out_val[k][1] = g.voutlt[k]; P.out_val[k][2] = g.scoutlt[k];
+        }
+    }
+    CK(cudaMalloc(&x->dc, sizeof(CaseDev) * ncases));
+    CK(cudaMalloc(&x->dinit, sizeof(InitDev) * ncases));
+    RC(upload_profiles(x));
+    // histories
+    x->hist_cap = 0;
+    RC(push(x));
+    RC(ensure_hist(x, HIST_INITIAL));
+    RC(init_state(x, -1));
+    Builder b{x, &x->cyc};
+    b.cycle();
+    return MGFVM_OK;
+}
+
+}  // namespace
+
+// =================================================================== C ABI
+extern "C" {
+
+int mgfvm_create(const mgfvm_config *cases, int ncases, const mgfvm_options *opt, mgfvm_ctx **out)
+{
+    mgfvm_clear_error();
+    if (!out) return mgfvm_fail(MGFVM_EINVAL, "null output pointer");
+    *out = nullptr;
+    if (!cases || ncases < 1) return mgfvm_fail(MGFVM_EINVAL, "need at least one case");
+    mgfvm_ctx *x = new (std::nothrow) mgfvm_ctx();
+    if (!x) return mgfvm_fail(MGFVM_ENOMEM, "out of host memory");
+    int rc = create_impl(cases, ncases, opt, x);
+    if (rc != MGFVM_OK) {
+        std::string msg = mgfvm_last_error();
+        destroy_all(x);
+        return mgfvm_fail(rc, "%s", msg.c_str());
+    }
+    *out = x;
+    return MGFVM_OK;
+}
+
+int mgfvm_destroy(mgfvm_ctx *x)
+{
+    destroy_all(x);
+    return MGFVM_OK;
+}
+
+int mgfvm_reset(mgfvm_ctx *x)
+{
+    RC(check_ctx(x));
+    RC(pull(x));
+    return init_state(x, -1);
+}
+
+int mgfvm_set_inlet_profile(mgfvm_ctx *x, int icase, const double *u, int n)
+{
+    RC(check_ctx(x));
+    if (icase < 0 || icase >= x->ncases) return mgfvm_fail(MGFVM_EINVAL, "case %d out of range", icase);
+    if (n < 0 || (n > 0 && !u)) return mgfvm_fail(MGFVM_EINVAL, "bad inlet profile");
+    RC(pull(x));
+    x->profile[icase].assign(u, u + n);
+    RC(upload_profiles(x));
+    return init_state(x, icase);
+}
+
+int mgfvm_cycle(mgfvm_ctx *x, int ncycles)
+{
+    RC(check_ctx(x));
+    if (ncycles < 0) return mgfvm_fail(MGFVM_EINVAL, "negative cycle count");
+    RC(pull(x));
+    int need = 0;
+    for (const CaseDev &C : x->hc) need = std::max(need, C.ncyc + ncycles);
+    RC(ensure_hist(x, need));
+    RC(set_controls(x, 0, 0.0));
+    CK(cudaEventRecord(x->e0, x->stream));
+    RC(run_cycles(x, ncycles));
+    CK(cudaEventRecord(x->e1, x->stream));
+    CK(cudaEventSynchronize(x->e1));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, x->e0, x->e1));
+    x->last_ms = ms;
+    CK(cudaGetLastError());
+    return MGFVM_OK;
+}
+
+int mgfvm_solve(mgfvm_ctx *x, int max_cycles, double fp_tol, int *cycles_out)
+{
+    RC(check_ctx(x));
+    if (max_cycles < 0) return mgfvm_fail(MGFVM_EINVAL, "negative cycle limit");
+    RC(pull(x));
+    std::vector<int> start(x->ncases);
+    int need = 0;
+    for (int c = 0; c < x->ncases; ++c) {
+        start[c] = x->hc[c].ncyc;
+        need = std::max(need, x->hc[c].ncyc + max_cycles);
+    }
+    RC(ensure_hist(x, need));
+    RC(set_controls(x, 1, fp_tol));
+    CK(cudaEventRecord(x->e0, x->stream));
+    int run = 0;
+    while (run < max_cycles) {
+        const int n = std::min(x->opt.sync_every, max_cycles - run);
+        RC(run_cycles(x, n));
+        run += n;
+        CK(cudaMemcpy2DAsync(x->hflags, sizeof(int), &x->dc[0].done, sizeof(CaseDev), sizeof(int), x->ncases,
+                             cudaMemcpyDeviceToHost, x->stream));
+        CK(cudaStreamSynchronize(x->stream));
+        x->d2h += (long long)sizeof(int) * x->ncases;
+        bool all = true;
+        for (int c = 0; c < x->ncases; ++c) all &= x->hflags[c] != 0;
+        if (all) break;
+    }
+    CK(cudaEventRecord(x->e1, x->stream));
+    CK(cudaEventSynchronize(x->e1));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, x->e0, x->e1));
+    x->last_ms = ms;
+    RC(pull(x));
+    int nonfinite = 0;
+    for (int c = 0; c < x->ncases; ++c) {
+        if (cycles_out) cycles_out[c] = x->hc[c].ncyc - start[c];
+        if (x->hc[c].status & CASE_NONFINITE) nonfinite = 1;
+    }
+    if (nonfinite) return mgfvm_fail(MGFVM_ENONFINITE, "a case's mass error or fixed-point change became NaN/Inf");
+    return MGFVM_OK;
+}
+
+int mgfvm_history(mgfvm_ctx *x, int icase, double *err, double *delta, int cap, int *n_out)
+{
+    RC(check_ctx(x));
+    if (icase < 0 || icase >= x->ncases) return mgfvm_fail(MGFVM_EINVAL, "case %d out of range", icase);
+    RC(pull(x));
+    const int n = std::min(x->hc[icase].ncyc, x->hist_cap);
+    if (n_out) *n_out = x->hc[icase].ncyc;
+    const int m = std::min(n, std::max(cap, 0));
+    if (err && m) CK(cudaMemcpy(err, x->hc[icase].hist_err, sizeof(double) * m, cudaMemcpyDeviceToHost));
+    if (delta && m) CK(cudaMemcpy(delta, x->hc[icase].hist_delta, sizeof(double) * m, cudaMemcpyDeviceToHost));
+    x->d2h += (long long)sizeof(double) * m * ((err ? 1 : 0) + (delta ? 1 : 0));
+    return MGFVM_OK;
+}
+
+int mgfvm_num_levels(mgfvm_ctx *x, int icase, int *ngrid)
+{
+    if (!x || icase < 0 || icase >= x->ncases || !ngrid) return mgfvm_fail(MGFVM_EINVAL, "bad arguments");
+    *ngrid = x->cfg[icase].ngrid;
+    return MGFVM_OK;
+}
+
+int mgfvm_level_dims(mgfvm_ctx *x, int icase, int level, int *npx, int *npy)
+{
+    if (!x) return mgfvm_fail(MGFVM_EINVAL, "null context");
+    RC(check_case_level(x, icase, level));
+    if (npx) *npx = npx_of(x->cfg[icase], level);
+    if (npy) *npy = npy_of(x->cfg[icase], level);
+    return MGFVM_OK;
+}
+
+int mgfvm_get_field(mgfvm_ctx *x, int icase, int level, int field, double *out)
+{
+    RC(check_ctx(x));
+    RC(check_case_level(x, icase, level));
+    if (field < 0 || field >= MGFVM_NFIELDS || !out) return mgfvm_fail(MGFVM_EINVAL, "bad field %d", field);
+    CK(cudaStreamSynchronize(x->stream));
+    const LevelDev &L = x->hc[icase].lv[level];
+    CK(cudaMemcpy(out, L.f[field], sizeof(double) * L.npx * L.npy, cudaMemcpyDeviceToHost));
+    x->d2h += (long long)sizeof(double) * L.npx * L.npy;
+    return MGFVM_OK;
+}
+
+int mgfvm_set_field(mgfvm_ctx *x, int icase, int level, int field, const double *in)
+{
+    RC(check_ctx(x));
+    RC(check_case_level(x, icase, level));
+    if (field < 0 || field >= MGFVM_NFIELDS || !in) return mgfvm_fail(MGFVM_EINVAL, "bad field %d", field);
+    CK(cudaStreamSynchronize(x->stream));
+    const LevelDev &L = x->hc[icase].lv[level];
+    CK(cudaMemcpy(L.f[field], in, sizeof(double) * L.npx * L.npy, cudaMemcpyHostToDevice));
+    x->h2d += (long long)sizeof(double) * L.npx * L.npy;
+    return MGFVM_OK;
+}
+
+int mgfvm_get_tag(mgfvm_ctx *x, int icase, int level, int *out)
+{
+    RC(check_ctx(x));
+    RC(check_case_level(x, icase, level));
+    if (!out) return mgfvm_fail(MGFVM_EINVAL, "null output");
+    CK(cudaStreamSynchronize(x->stream));
+    const LevelDev &L = x->hc[icase].lv[level];
+    CK(cudaMemcpy(out, L.tag, sizeof(int) * L.npx * L.npy, cudaMemcpyDeviceToHost));
+    x->d2h += (long long)sizeof(int) * L.npx * L.npy;
+    return MGFVM_OK;
+}
+
+int mgfvm_get_obstacle_ranges(mgfvm_ctx *x, int icase, int level, int *out)
+{
+    if (!x) return mgfvm_fail(MGFVM_EINVAL, "null context");
+    RC(check_case_level(x, icase, level));
+    for (int k = 0; k < x->cfg[icase].nobs; ++k) mgfvm_obstacle_range(&x->cfg[icase], k, level, &out[4 * k]);
+    return MGFVM_OK;
+}
+
+int mgfvm_op(mgfvm_ctx *x, int op, int level)
+{
+    RC(check_ctx(x));
+    if (op < 0 || op >= MGFVM_NOPS) return mgfvm_fail(MGFVM_EINVAL, "unknown op %d", op);
+    if (level < 0 || level >= x->maxng) return mgfvm_fail(MGFVM_EINVAL, "level %d out of range", level);
+    if ((op == MGFVM_OP_RESTRICT || op == MGFVM_OP_PROLONG) && level + 1 >= x->maxng)
+        return mgfvm_fail(MGFVM_EINVAL, "transfer from level %d needs level %d", level, level + 1);
+    RC(set_controls(x, 0, 0.0));
+    std::vector<Launch> v;
+    Builder b{x, &v};
+    b.op(op, level);
+    RC(run_list(x, v));
+    CK(cudaStreamSynchronize(x->stream));
+    return MGFVM_OK;
+}
+
+int mgfvm_kernel_launches(mgfvm_ctx *x, long long *out)
+{
+    if (!x || !out) return mgfvm_fail(MGFVM_EINVAL, "bad arguments");
+    *out = x->launches;
+    return MGFVM_OK;
+}
+
+int mgfvm_last_elapsed_ms(mgfvm_ctx *x, double *ms)
+{
+    if (!x || !ms) return mgfvm_fail(MGFVM_EINVAL, "bad arguments");
+    *ms = x->last_ms;
+    return MGFVM_OK;
+}
+
+int mgfvm_stream(mgfvm_ctx *x, void **stream)
+{
+    if (!x || !stream) return mgfvm_fail(MGFVM_EINVAL, "bad arguments");
+    *stream = (void *)x->stream;
+    return MGFVM_OK;
+}
+
+int mgfvm_time_op(mgfvm_ctx *x, int op, int level, int reps, double *ms_total, int *launches)
+{
+    RC(check_ctx(x));
+    if (op < 0 || op >= MGFVM_NOPS || reps < 1) return mgfvm_fail(MGFVM_EINVAL, "bad op %d or reps %d", op, reps);
+    if (level < 0 || level >= x->maxng) return mgfvm_fail(MGFVM_EINVAL, "level %d out of range", level);
+    if ((op == MGFVM_OP_RESTRICT || op == MGFVM_OP_PROLONG) && level + 1 >= x->maxng)
+        return mgfvm_fail(MGFVM_EINVAL, "transfer from level %d needs level %d", level, level + 1);
+    RC(set_controls(x, 0, 0.0));
+    std::vector<Launch> v;
+    Builder b{x, &v};
+    b.op(op, level);
+    CK(cudaEventRecord(x->e0, x->stream));
+    for (int r = 0; r < reps; ++r) RC(run_list(x, v));
+    CK(cudaEventRecord(x->e1, x->stream));
+    CK(cudaEventSynchronize(x->e1));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, x->e0, x->e1));
+    if (ms_total) *ms_total = ms;
+    if (launches) *launches = (int)v.size() * reps;
+    return MGFVM_OK;
+}
+
+int mgfvm_transfer_bytes(mgfvm_ctx *x, long long *h2d, long long *d2h)
+{
+    if (!x) return mgfvm_fail(MGFVM_EINVAL, "null context");
+    if (h2d) *h2d = x->h2d;
+    if (d2h) *d2h = x->d2h;
+    return MGFVM_OK;
+}
+
+// ----------------------------------------------- raw-pointer entry points
+static int check_raw(const void *const *ptrs, int n, int npx, int npy, int nx, int ny)
+{
+    for (int k = 0; k < n; ++k)
+        if (!ptrs[k]) return mgfvm_fail(MGFVM_EINVAL, "null device pointer");
+    if (npx < 3 || npy < 3 || nx < 1 || ny < 1 || nx > npx - 1 || ny > npy - 1)
+        return mgfvm_fail(MGFVM_EINVAL, "extent nx=%d ny=%d does not fit a %d x %d level", nx, ny, npx, npy);
+    return MGFVM_OK;
+}
+
+int mgfvm_jacobi_f64(const double *aw, const double *ae, const double *as, const double *an, const double *ap,
+                     const double *su, double *phi, double *scratch, int npx, int npy, int nx, int ny, int nsw,
+                     void *stream)
+{
+    const void *p[] = {aw, ae, as, an, ap, su, phi, scratch};
+    RC(check_raw(p, 8, npx, npy, nx, ny));
+    if (nsw < 0) return mgfvm_fail(MGFVM_EINVAL, "negative sweep count");
+    CK(mg::raw_jacobi(aw, ae, as, an, ap, su, phi, scratch, npx, npy, nx, ny, nsw, (cudaStream_t)stream));
+    return MGFVM_OK;
+}
+
+int mgfvm_rbgs_f64(const double *aw, const double *ae, const double *as, const double *an, const double *ap,
+                   const double *su, double *phi, int npx, int npy, int nx, int ny, int nsw, void *stream)
+{
+    const void *p[] = {aw, ae, as, an, ap, su, phi};
+    RC(check_raw(p, 7, npx, npy, nx, ny));
+    if (nsw < 0) return mgfvm_fail(MGFVM_EINVAL, "negative sweep count");
+    CK(mg::raw_rbgs(aw, ae, as, an, ap, su, phi, npx, npy, nx, ny, nsw, (cudaStream_t)stream));
+    return MGFVM_OK;
+}
+
+size_t mgfvm_masserror_scratch_doubles(int npx, int npy)
+{
+    return mg::raw_masserror_blocks(npx, npy) * RED_STRIDE + 1;
+}
+
+int mgfvm_masserror_f64(const double *u, const double *v, const double *areax, const double *areay, double *su,
+                        double *pp, int npx, int npy, double *err_out, double *partials, void *stream)
+{
+    const void *p[] = {u, v, areax, areay, su, pp, err_out, partials};
+    RC(check_raw(p, 8, npx, npy, npx - 1, npy - 1));
+    CK(mg::raw_masserror(u, v, areax, areay, su, pp, npx, npy, err_out, partials, (cudaStream_t)stream));
+    return MGFVM_OK;
+}
+
+}  // extern "C"

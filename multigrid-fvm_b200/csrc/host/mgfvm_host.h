@@ -1,0 +1,50 @@
+/*
+ * mgfvm_host.h — host-side helpers shared by the engine and the command-line tool.
+ */
+#ifndef MGFVM_HOST_H
+#define MGFVM_HOST_H
+
+#include "mgfvm.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Record a failure message for mgfvm_last_error() and return `status`. */
+int mgfvm_fail(int status, const char *fmt, ...);
+void mgfvm_clear_error(void);
+
+/* Obstacle k mapped to level ig, {is, ie, js, je}; empty {1,0,1,0} at ig >= ig_obs. */
+void mgfvm_obstacle_range(const mgfvm_config *c, int k, int ig, int r[4]);
+
+/* Precomputed obstacle programs of one level (see obstacles.c). */
+typedef struct mgfvm_obstacle_prog {
+    /* update's pressure copy (:1153-1177) resolved to a gather:
+     * p[dst[k]] = p_before[src[k]], k < ncopy; `hazard` != 0 when some src is also a
+     * dst, so the gather must read every source before writing any destination. */
+    int ncopy;
+    int *dst, *src;
+    int hazard;
+    /* coefsc's obstacle-face diffusion (:939-963) as a per-cell sequence code:
+     * cells[k] receives, in order, the additions encoded in codes[k] (see obstacles.c). */
+    int nseq;
+    int *cells;
+    unsigned *codes;
+    int max_adds;      /* longest sequence seen */
+} mgfvm_obstacle_prog;
+
+int mgfvm_build_obstacle_prog(const mgfvm_config *c, int ig, mgfvm_obstacle_prog *out);
+void mgfvm_free_obstacle_prog(mgfvm_obstacle_prog *p);
+
+/* Output files of the reference (write_vtk_2d_cc :2261-2363,
+ * write_convergence_data_file :2544-2558). */
+int mgfvm_write_vtk(const char *path, const mgfvm_config *c, int npx, int npy, const double *u,
+                    const double *v, const double *p, const double *sc, const int *obs_ranges,
+                    int iter, double diag_out[3]);
+int mgfvm_write_convergence(const char *path, const double *hist, int nconverged, int nvcycle,
+                            int verbose);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,192 @@
+"""Python interface of the engine: a batch of cases on one GPU.
+
+It mirrors the reference program's workflow (Version-6-26-04.c:180-276): read
+InputData and pattern.txt, build the levels, run V-cycles until the mass error is
+below `convergence` (or the V-cycle reaches its fixed point), read the level-0
+fields.  Every call goes through the C ABI of libmgfvm.so; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Iterable, List, Optional, Sequence, Tuple, Union
+
+import numpy as np
+
+from . import _abi
+from ._lib import check, lib
+from .inputs import CaseConfig
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+def read_case(directory: str = ".", inputdata: str = "InputData",
+              pattern: str = "pattern.txt", verbose: bool = False) -> CaseConfig:
+    """Parse InputData + pattern.txt with the C parser (readInput :280-401)."""
+    L = lib()
+    c = _abi.Config()
+    check(L.mgfvm_config_read(os.path.join(directory, inputdata).encode(),
+                              os.path.join(directory, pattern).encode(), C.byref(c), int(verbose)))
+    try:
+        return CaseConfig.from_c(c)
+    finally:
+        L.mgfvm_config_release(C.byref(c))
+
+
+def validate(cfg: CaseConfig) -> None:
+    c, keep = cfg.to_c()
+    check(lib().mgfvm_config_validate(C.byref(c)))
+    del keep
+
+
+class Solver:
+    """`ncases` independent cases advanced together on one GPU (an mgfvm_ctx)."""
+
+    def __init__(self, cases: Union[CaseConfig, Sequence[CaseConfig]], device: int = 0,
+                 precision: str = "fp64", tail_level: int = -1, use_graph: bool = True,
+                 sync_every: int = 64):
+        if isinstance(cases, CaseConfig):
+            cases = [cases]
+        self.cases: List[CaseConfig] = list(cases)
+        L = lib()
+        arr = (_abi.Config * len(self.cases))()
+        self._keep = []
+        for k, cfg in enumerate(self.cases):
+            c, keep = cfg.to_c()
+            arr[k] = c
+            self._keep.append(keep)
+        opt = _abi.Options()
+        L.mgfvm_options_default(C.byref(opt))
+        opt.device = device
+        opt.precision = {"fp64": _abi.PREC_FP64, "mixed": _abi.PREC_MIXED}[precision]
+        opt.tail_level = tail_level
+        opt.use_graph = int(use_graph)
+        opt.sync_every = sync_every
+        h = C.c_void_p()
+        check(L.mgfvm_create(arr, len(self.cases), C.byref(opt), C.byref(h)))
+        self._h = h
+        self._lib = L
+
+    # ------------------------------------------------------------ lifetime
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.mgfvm_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------ geometry
+    @property
+    def ncases(self) -> int:
+        return len(self.cases)
+
+    def levels(self, case: int = 0) -> int:
+        n = C.c_int()
+        check(self._lib.mgfvm_num_levels(self._h, case, C.byref(n)))
+        return n.value
+
+    def dims(self, case: int, level: int) -> Tuple[int, int]:
+        a, b = C.c_int(), C.c_int()
+        check(self._lib.mgfvm_level_dims(self._h, case, level, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    # ------------------------------------------------------------ running
+    def reset(self) -> None:
+        check(self._lib.mgfvm_reset(self._h))
+
+    def set_inlet_profile(self, case: int, u: Iterable[float]) -> None:
+        a = np.ascontiguousarray(np.asarray(u, dtype=np.float64))
+        check(self._lib.mgfvm_set_inlet_profile(self._h, case, a.ctypes.data_as(_dp), a.size))
+
+    def cycle(self, n: int = 1) -> None:
+        check(self._lib.mgfvm_cycle(self._h, n))
+
+    def solve(self, max_cycles: int, fp_tol: float = 0.0) -> np.ndarray:
+        out = np.zeros(self.ncases, dtype=np.int32)
+        check(self._lib.mgfvm_solve(self._h, max_cycles, fp_tol, out.ctypes.data_as(_ip)))
+        return out
+
+    def op(self, name: Union[str, int], level: int) -> None:
+        op = _abi.OP[name] if isinstance(name, str) else name
+        check(self._lib.mgfvm_op(self._h, op, level))
+
+    # ------------------------------------------------------------ data
+    def field(self, case: int, level: int, name: Union[str, int]) -> np.ndarray:
+        npx, npy = self.dims(case, level)
+        f = _abi.FIELD[name] if isinstance(name, str) else name
+        out = np.empty(npx * npy, dtype=np.float64)
+        check(self._lib.mgfvm_get_field(self._h, case, level, f, out.ctypes.data_as(_dp)))
+        return out.reshape(npy, npx)
+
+    def set_field(self, case: int, level: int, name: Union[str, int], arr) -> None:
+        f = _abi.FIELD[name] if isinstance(name, str) else name
+        a = np.ascontiguousarray(arr, dtype=np.float64).ravel()
+        npx, npy = self.dims(case, level)
+        if a.size != npx * npy:
+            raise ValueError(f"expected {npx * npy} values, got {a.size}")
+        check(self._lib.mgfvm_set_field(self._h, case, level, f, a.ctypes.data_as(_dp)))
+
+    def tag(self, case: int, level: int) -> np.ndarray:
+        npx, npy = self.dims(case, level)
+        out = np.empty(npx * npy, dtype=np.int32)
+        check(self._lib.mgfvm_get_tag(self._h, case, level, out.ctypes.data_as(_ip)))
+        return out.reshape(npy, npx)
+
+    def obstacle_ranges(self, case: int, level: int) -> np.ndarray:
+        n = len(self.cases[case].obstacles)
+        out = np.zeros(max(4 * n, 4), dtype=np.int32)
+        check(self._lib.mgfvm_get_obstacle_ranges(self._h, case, level, out.ctypes.data_as(_ip)))
+        return out[:4 * n].reshape(-1, 4)
+
+    def history(self, case: int = 0) -> Tuple[np.ndarray, np.ndarray]:
+        n = C.c_int()
+        check(self._lib.mgfvm_history(self._h, case, None, None, 0, C.byref(n)))
+        e = np.zeros(max(n.value, 1))
+        d = np.zeros(max(n.value, 1))
+        check(self._lib.mgfvm_history(self._h, case, e.ctypes.data_as(_dp), d.ctypes.data_as(_dp),
+                                      n.value, C.byref(n)))
+        return e[:n.value], d[:n.value]
+
+    @property
+    def kernel_launches(self) -> int:
+        n = C.c_longlong()
+        check(self._lib.mgfvm_kernel_launches(self._h, C.byref(n)))
+        return n.value
+
+    @property
+    def last_elapsed_ms(self) -> float:
+        v = C.c_double()
+        check(self._lib.mgfvm_last_elapsed_ms(self._h, C.byref(v)))
+        return v.value
+
+    def time_op(self, name: Union[str, int], level: int, reps: int = 10) -> Tuple[float, int]:
+        """(milliseconds, kernel launches) of `reps` back-to-back runs of one op, timed with
+        CUDA events on the context stream."""
+        op = _abi.OP[name] if isinstance(name, str) else name
+        ms, n = C.c_double(), C.c_int()
+        check(self._lib.mgfvm_time_op(self._h, op, level, reps, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    @property
+    def transfer_bytes(self) -> Tuple[int, int]:
+        """(host->device, device->host) bytes copied by this context so far."""
+        a, b = C.c_longlong(), C.c_longlong()
+        check(self._lib.mgfvm_transfer_bytes(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    @property
+    def stream(self) -> int:
+        s = C.c_void_p()
+        check(self._lib.mgfvm_stream(self._h, C.byref(s)))
+        return s.value or 0

@@ -1,0 +1,174 @@
+"""Parity of the CUDA engine (through the C ABI) with the CPU oracle.
+
+The FP64 engine is compiled without FMA contraction and applies every reference
+operation in the reference's order, so the bar is bit-exact equality of every state
+array after every routine and every cycle; only the mass-error sums (parallel,
+fixed-order reductions) are compared with a 1e-12 relative tolerance.
+"""
+import numpy as np
+import pytest
+
+from cases import small_cases
+from conftest import assert_bitexact, interior, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+STATE = ["u", "v", "p", "pp", "sc", "su", "resu", "resv", "ressc", "apu", "apv", "cx", "cy", "c"]
+COEF = ["aw", "ae", "as", "an", "ap"]
+ERR_RTOL = 1e-12
+
+
+def _pair(cfg, **kw):
+    from mgfvm import Solver
+    from oracle import OracleCase
+    return Solver(cfg, **kw), OracleCase(cfg)
+
+
+def _domain(a, op):
+    """The cells a routine writes its coefficients on (solve_u :701, solve_v :710,
+    solve_pprime :725, solve_sc :735); elsewhere they are stale and never read."""
+    if op == "solve_u":
+        return a[1:-1, 1:-2]
+    if op == "solve_v":
+        return a[1:-2, 1:-1]
+    return interior(a)
+
+
+def _compare(s, o, fields, levels=None, case=0, what="", op=""):
+    for ig in range(o.ngrid) if levels is None else levels:
+        for f in fields:
+            a, b = s.field(case, ig, f), o.get(ig, f)
+            if f in COEF:
+                a, b = _domain(a, op), _domain(b, op)
+            assert_bitexact(a, b, f"{what} level {ig} {f}")
+
+
+@pytest.mark.parametrize("name", list(small_cases()))
+def test_initial_state_bitexact(name, oracle_built):
+    cfg = small_cases()[name]
+    s, o = _pair(cfg)
+    for ig in range(o.ngrid):
+        assert_bitexact(s.tag(0, ig), o.tag(ig), f"tag level {ig}")
+        for f in ["u", "v", "p", "pp", "sc", "apu", "apv", "spu", "spv", "spsc", "areax", "areay", "su",
+                  "resu", "resv", "ressc", "cx", "cy"]:
+            assert_bitexact(s.field(0, ig, f), o.get(ig, f), f"init level {ig} {f}")
+        assert_bitexact(s.obstacle_ranges(0, ig), o.obstacle_ranges(ig), f"ranges level {ig}")
+    s.close()
+
+
+@pytest.mark.parametrize("name", ["c0_jacobi", "obs_gs_touch", "ports", "bc_mix", "odd_sweeps"])
+def test_single_ops_bitexact(name, oracle_built):
+    """Every routine of a V-cycle on its own, in cycle order, compared after each."""
+    cfg = small_cases()[name]
+    s, o = _pair(cfg)
+    s.cycle(2)
+    o.cycle(2)
+    ng = o.ngrid
+    seq = []
+    for ig in range(ng):
+        seq += [("fluxes", ig), ("solve_u", ig), ("solve_v", ig), ("solve_pp", ig), ("pbound", ig),
+                ("outflow", ig), ("solve_sc", ig)]
+        if ig < ng - 1:
+            seq.append(("restrict", ig))
+    for ig in range(ng - 2, -1, -1):
+        seq.append(("prolong", ig))
+    for op, ig in seq:
+        s.op(op, ig)
+        o.op(op, ig)
+        fields = STATE + (COEF if op.startswith("solve") else [])
+        lv = [ig, ig + 1] if op in ("restrict", "prolong") else [ig]
+        _compare(s, o, fields, lv, what=f"after {op}({ig})", op=op)
+
+
+@pytest.mark.parametrize("name", list(small_cases()))
+@pytest.mark.parametrize("tail", [-1, 0, 99])
+def test_cycles_bitexact(name, tail, oracle_built):
+    cfg = small_cases()[name]
+    s, o = _pair(cfg, tail_level=tail)
+    for n in (1, 2, 7):
+        s.cycle(n)
+        o.cycle(n)
+        _compare(s, o, STATE, what=f"tail {tail} after +{n} cycles")
+    es, _ = s.history(0)
+    eo, _ = o.history()
+    assert len(es) == len(eo) == 10
+    np.testing.assert_allclose(es, eo, rtol=ERR_RTOL, atol=0)
+    s.close()
+
+
+def test_direct_launch_equals_graph(oracle_built):
+    from mgfvm import Solver
+    cfg = small_cases()["obs_gs_touch"]
+    a, b = Solver(cfg, use_graph=True), Solver(cfg, use_graph=False)
+    a.cycle(5)
+    b.cycle(5)
+    for f in STATE:
+        for ig in range(cfg.ngrid):
+            assert_bitexact(a.field(0, ig, f), b.field(0, ig, f), f"{f} level {ig}")
+
+
+def test_heterogeneous_batch(oracle_built):
+    """Cases of different sizes, levels, physics and obstacles advance together and each
+    matches its own oracle."""
+    from mgfvm import Solver
+    from oracle import OracleCase
+    sc = small_cases()
+    names = ["c0_gs", "obs_gs_touch", "obs_below_coarsest", "bc_mix", "rect_grid"]
+    cfgs = [sc[n] for n in names]
+    s = Solver(cfgs)
+    orcs = [OracleCase(c) for c in cfgs]
+    s.cycle(4)
+    for k, o in enumerate(orcs):
+        o.cycle(4)
+        _compare(s, o, STATE, case=k, what=names[k])
+        np.testing.assert_allclose(s.history(k)[0], o.history()[0], rtol=ERR_RTOL)
+
+
+def test_reset_and_inlet_profile(oracle_built):
+    from mgfvm import Solver, configs
+    from oracle import OracleCase
+    cfg = configs.small(32, 3, isolve=2)
+    prof = 1.0 + 0.1 * np.random.default_rng(7).standard_normal(32)
+    s = Solver([cfg, cfg])
+    s.cycle(3)
+    s.set_inlet_profile(1, prof)      # resets case 1 only
+    o0, o1 = OracleCase(cfg), OracleCase(cfg, prof)
+    o0.cycle(3)
+    _compare(s, o0, STATE, case=0, what="case 0 kept")
+    _compare(s, o1, ["u", "v", "p", "sc"], case=1, what="case 1 reset with profile")
+    s.cycle(3)
+    o0.cycle(3)
+    o1.cycle(3)
+    _compare(s, o0, STATE, case=0, what="case 0")
+    _compare(s, o1, STATE, case=1, what="case 1")
+    s.reset()
+    o2 = OracleCase(cfg)
+    _compare(s, o2, ["u", "v", "p", "sc"], case=0, what="after reset")
+
+
+def test_solve_stops_like_oracle(oracle_built):
+    """Fixed-point stop rule: same cycle count and the same converged fields."""
+    from mgfvm import Solver, configs
+    from oracle import OracleCase
+    cfg = configs.small(32, 3, isolve=2)
+    s = Solver(cfg, sync_every=16)
+    o = OracleCase(cfg)
+    n_gpu = int(s.solve(3000, fp_tol=1e-9)[0])
+    n_cpu = o.solve(3000, 1e-9)
+    assert abs(n_gpu - n_cpu) <= 1, (n_gpu, n_cpu)
+    if n_gpu == n_cpu:
+        _compare(s, o, ["u", "v", "p", "sc"], levels=[0], what="converged")
+    else:
+        for f in ["u", "v", "sc"]:
+            assert rel_l2(s.field(0, 0, f), o.get(0, f)) < 1e-6
+    _, d = s.history(0)
+    _, dd = o.history()
+    np.testing.assert_allclose(d[1:n_gpu], dd[1:n_gpu], rtol=1e-6, atol=1e-14)
+
+
+def test_reference_stop_rule(oracle_built):
+    """convergence above the first mass error stops after one cycle (:247-248)."""
+    from mgfvm import Solver, configs
+    cfg = configs.small(32, 3, convergence=1e9)
+    s = Solver(cfg)
+    assert int(s.solve(50)[0]) == 1
