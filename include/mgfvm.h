@@ -246,6 +246,20 @@ int mgfvm_pattern_random(int n_grid, double ratio, double pct1, double pct2, dou
 /* One obstacle per occupied pixel {r+1, r+1, c+1, c+1} (create_patterns_staggered.c:47-54). */
 int mgfvm_pattern_pixels(const int *grid, int dim, int *obs, int max_obs, int *count);
 
+/* ------------------------------------------------------- output files */
+/* The reference's output files, byte for byte.  Host only.
+ * write_vtk_2d_cc (Version-6-26-04.c:2261-2363): legacy ASCII VTK of the level-0
+ * interior (u, v, p, sc of npx*npy host arrays; obs_ranges = level-0 ranges from
+ * mgfvm_get_obstacle_ranges), then the three diagnostic stdout lines; diag_out (may
+ * be NULL) receives mean |velocity|, mean x-velocity and tortuosity. */
+int mgfvm_write_vtk(const char *path, const mgfvm_config *cfg, int npx, int npy, const double *u,
+                    const double *v, const double *p, const double *sc, const int *obs_ranges,
+                    int iter, double diag_out[3]);
+/* write_convergence_data_file (:2544-2558): rows 1..nconverged of the history, and a
+ * stdout line reporting `nvcycle` records when verbose. */
+int mgfvm_write_convergence(const char *path, const double *hist, int nconverged, int nvcycle,
+                            int verbose);
+
 /* ------------------------------------- raw-pointer kernel entry points */
 /* These take caller-owned DEVICE pointers to one level laid out as above and
  * launch on `stream` (a cudaStream_t, NULL = legacy default stream).  They are

@@ -36,14 +36,6 @@ typedef struct mgfvm_obstacle_prog {
 int mgfvm_build_obstacle_prog(const mgfvm_config *c, int ig, mgfvm_obstacle_prog *out);
 void mgfvm_free_obstacle_prog(mgfvm_obstacle_prog *p);
 
-/* Output files of the reference (write_vtk_2d_cc :2261-2363,
- * write_convergence_data_file :2544-2558). */
-int mgfvm_write_vtk(const char *path, const mgfvm_config *c, int npx, int npy, const double *u,
-                    const double *v, const double *p, const double *sc, const int *obs_ranges,
-                    int iter, double diag_out[3]);
-int mgfvm_write_convergence(const char *path, const double *hist, int nconverged, int nvcycle,
-                            int verbose);
-
 #ifdef __cplusplus
 }
 #endif

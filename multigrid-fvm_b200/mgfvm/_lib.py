@@ -69,6 +69,9 @@ def lib() -> C.CDLL:
         "mgfvm_pattern_random": (C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                             C.c_ulonglong, _ip, _ip, C.c_int, _ip]),
         "mgfvm_pattern_pixels": (C.c_int, [_ip, C.c_int, _ip, C.c_int, _ip]),
+        "mgfvm_write_vtk": (C.c_int, [C.c_char_p, C.POINTER(_abi.Config), C.c_int, C.c_int, _dp, _dp, _dp,
+                                       _dp, _ip, C.c_int, _dp]),
+        "mgfvm_write_convergence": (C.c_int, [C.c_char_p, _dp, C.c_int, C.c_int, C.c_int]),
         "mgfvm_jacobi_f64": (C.c_int, [_vp] * 8 + [C.c_int] * 5 + [_vp]),
         "mgfvm_rbgs_f64": (C.c_int, [_vp] * 7 + [C.c_int] * 5 + [_vp]),
         "mgfvm_masserror_f64": (C.c_int, [_vp] * 6 + [C.c_int, C.c_int, _vp, _vp, _vp]),

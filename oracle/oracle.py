@@ -143,6 +143,10 @@ class OracleCase:
         if rc != 0:
             raise RuntimeError(f"orc_op({name}, {level}) -> {rc}")
 
+    def last_err(self):
+        """Mass error of the last masserror call (any level)."""
+        return self.lib.orc_last_err(self.h)
+
     def history(self):
         n = self.lib.orc_history(self.h, None, None, 0)
         e = np.empty(max(n, 1))
