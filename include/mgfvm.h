@@ -292,6 +292,19 @@ int mgfvm_masserror_f64(const double *u, const double *v, const double *areax,
                         int npy, double *err_out, double *partials, void *stream);
 size_t mgfvm_masserror_scratch_doubles(int npx, int npy);
 
+/* mgfvm_masserror_f64 for callers that cannot allocate device memory (a host
+ * program whose device memory another runtime owns, or a path that must not enter
+ * the CUDA allocator).  No counterpart in the reference: its reduction scratch is a
+ * fixed ~512 KiB array of static device memory inside this library, held by every
+ * GPU that loads it until exit.  Levels with more than 1,048,576 interior cells
+ * ((npx-2)*(npy-2)) are rejected with MGFVM_EINVAL.  Allocates nothing.  All calls
+ * on a device share that array: calls that overlap on the GPU race.  The first call
+ * on each device looks up the array's device address; make it before any stream
+ * capture. */
+int mgfvm_masserror_f64_noalloc(const double *u, const double *v, const double *areax,
+                                const double *areay, double *su, double *pp, int npx,
+                                int npy, double *err_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -76,6 +76,7 @@ def lib() -> C.CDLL:
         "mgfvm_rbgs_f64": (C.c_int, [_vp] * 7 + [C.c_int] * 5 + [_vp]),
         "mgfvm_masserror_f64": (C.c_int, [_vp] * 6 + [C.c_int, C.c_int, _vp, _vp, _vp]),
         "mgfvm_masserror_scratch_doubles": (C.c_size_t, [C.c_int, C.c_int]),
+        "mgfvm_masserror_f64_noalloc": (C.c_int, [_vp] * 6 + [C.c_int, C.c_int, _vp, _vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
