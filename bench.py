@@ -194,6 +194,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c1", choices=["c1", "c0", "c2"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tail", type=int, default=-1, help="first level of the one-CTA coarse kernel (-1 auto)")
     ap.add_argument("--profile-cycles", type=int, default=0,
                     help="only run 3 warm-up V-cycles then this many V-cycles of the workload "
                          "(for ncu launch lists) and exit")
@@ -216,13 +217,25 @@ def main():
     from mgfvm import Solver
     cases, desc = workload(a.workload)
     n_cases = len(cases)
-    solver = Solver(cases, device=local, sync_every=64)
+    solver = Solver(cases, device=local, sync_every=64, tail_level=a.tail)
     if a.profile_cycles:
         solver.cycle(3)
         n0 = solver.kernel_launches
         solver.cycle(a.profile_cycles)
-        log(f"profile: {n0} launches before, {solver.kernel_launches - n0} in {a.profile_cycles} cycle(s), "
-            f"{solver.last_elapsed_ms:.3f} ms")
+        nprof = solver.kernel_launches - n0
+        solver.cycle(20)
+        log(f"20 cycles: {solver.last_elapsed_ms / 20:.3f} ms per cycle (tail {a.tail})")
+        log(f"profile: {n0} launches before, {nprof} in {a.profile_cycles} cycle(s)")
+        prof = [solver.profile_cycle() for _ in range(3)][-1]
+        tot = sum(p[2] for p in prof)
+        agg = {}
+        for name, lv, t in prof:
+            k = f"{name}@{lv}"
+            c, v = agg.get(k, (0, 0.0))
+            agg[k] = (c + 1, v + t)
+        log(f"live per-launch profile (events between direct launches), cycle {tot * 1e3:.1f} us:")
+        for k, (c, v) in sorted(agg.items(), key=lambda kv: -kv[1][1]):
+            log(f"  {k:22s} x{c:3d} {v * 1e3:9.1f} us  {100 * v / tot:5.1f}%  avg {v / c * 1e3:7.2f} us")
         solver.close()
         return
     stream = torch.cuda.ExternalStream(solver.stream, device=torch.device("cuda", local))

@@ -222,6 +222,12 @@ int mgfvm_stream(mgfvm_ctx *ctx, void **stream);
  * *ms_total = elapsed milliseconds, *launches = kernels launched in that window. */
 int mgfvm_time_op(mgfvm_ctx *ctx, int op, int level, int reps, double *ms_total, int *launches);
 
+/* Run one V-cycle with every kernel launched directly and a CUDA event recorded
+ * after each launch on the context stream; ms[k] = time between the events around
+ * launch k (its device duration plus any gap before it), kernel[k] = the engine's
+ * kernel id, level[k] = its level.  Up to `cap` entries; *n_out = launches. */
+int mgfvm_profile_cycle(mgfvm_ctx *ctx, double *ms, int *kernel, int *level, int cap, int *n_out);
+
 /* Bytes this context copied host->device and device->host since it was created. */
 int mgfvm_transfer_bytes(mgfvm_ctx *ctx, long long *h2d, long long *d2h);
 

@@ -1,9 +1,9 @@
 // mg_cells.cuh — the per-cell arithmetic of every V-cycle routine, shared by the
-// grid-wide kernels (one thread per cell, all cases of a batch in one launch) and
-// the coarse-level kernel (one CTA per case, all coarse levels in one launch).
+// grid-wide kernels (one thread per cell, all cases of a batch in one launch), the
+// shared-memory tile smoothers and the coarse-level kernel (one CTA per case).
 //
 // Every function restates one loop body of Version-6-26-04.c with the operations in
-// the reference's order; this file is compiled with --fmad=false so the FP64 results
+// the reference's order; this code is compiled with --fmad=false so the FP64 results
 // are bit-identical to the reference built with gcc.  Where the reference runs a
 // second loop over boundary rows or obstacle cells after the main loop, the
 // function applies that loop's additions to the cell in the same order.
@@ -21,6 +21,23 @@ __device__ __forceinline__ double hyb_m(double c, double d) { return fmax(fabs(c
 
 struct Coef { double aw, ae, as, an, ap; };
 
+// Face mass fluxes cx = 0.5 u A_x, cy = 0.5 v A_y (fluxes :678-694), either read from
+// the arrays fluxes() filled or recomputed from u, v: identical bits either way, so a
+// kernel that runs right after the fluxes would be computed may skip the round trip.
+struct FluxArrays {
+    const double *cx, *cy;
+    __device__ __forceinline__ FluxArrays(const LevelDev &L) : cx(MGF(L, S_CX)), cy(MGF(L, S_CY)) {}
+    __device__ __forceinline__ double x(int q) const { return cx[q]; }
+    __device__ __forceinline__ double y(int q) const { return cy[q]; }
+};
+struct FluxLive {
+    const double *u, *v, *ax, *ay;
+    __device__ __forceinline__ FluxLive(const LevelDev &L)
+        : u(MGF(L, S_U)), v(MGF(L, S_V)), ax(MGF(L, S_AREAX)), ay(MGF(L, S_AREAY)) {}
+    __device__ __forceinline__ double x(int q) const { return 0.5 * u[q] * ax[q]; }
+    __device__ __forceinline__ double y(int q) const { return 0.5 * v[q] * ay[q]; }
+};
+
 // ------------------------------------------------------------------ fluxes
 // fluxes :678-694, domain i in [0, npx-2], j in [0, npy-2]
 __device__ __forceinline__ void cell_fluxes(const LevelDev &L, int q)
@@ -32,14 +49,15 @@ __device__ __forceinline__ void cell_fluxes(const LevelDev &L, int q)
 // ------------------------------------------------------------ coefficients
 // coefu :815-860 at u face (i, j), i in [1, npx-3], j in [1, npy-2], including the
 // wall-shear rows j = npy-2 then j = 1 (:849-858; both use areay of row npy-2).
-__device__ __forceinline__ Coef coef_u(const LevelDev &L, int i, int j)
+template <class F>
+__device__ __forceinline__ Coef coef_u(const LevelDev &L, const F &fl, int i, int j)
 {
     const int nx = L.npx, q = j * nx + i, s = q - nx;
-    const double *cx = MGF(L, S_CX), *cy = MGF(L, S_CY);
-    double cxm = 0.5 * (cx[q] + cx[q - 1]);
-    double cxp = 0.5 * (cx[q] + cx[q + 1]);
-    double cym = 0.5 * (cy[s] + cy[s + 1]);
-    double cyp = 0.5 * (cy[q] + cy[q + 1]);
+    const double cq = fl.x(q);
+    double cxm = 0.5 * (cq + fl.x(q - 1));
+    double cxp = 0.5 * (cq + fl.x(q + 1));
+    double cym = 0.5 * (fl.y(s) + fl.y(s + 1));
+    double cyp = 0.5 * (fl.y(q) + fl.y(q + 1));
     double dxm = L.amu * (MGF(L, S_AREAX)[q] / L.dx);
     double dym = L.amu * (MGF(L, S_AREAY)[q] / L.dy);
     Coef k;
@@ -62,14 +80,15 @@ __device__ __forceinline__ Coef coef_u(const LevelDev &L, int i, int j)
 
 // coefv :966-1016 at v face (i, j), i in [1, npx-2], j in [1, npy-3], including the
 // side-wall columns i = npx-2 then i = 1 (:1005-1015; both use areay of column npx-2).
-__device__ __forceinline__ Coef coef_v(const LevelDev &L, int i, int j)
+template <class F>
+__device__ __forceinline__ Coef coef_v(const LevelDev &L, const F &fl, int i, int j)
 {
     const int nx = L.npx, q = j * nx + i, n = q + nx, s = q - nx;
-    const double *cx = MGF(L, S_CX), *cy = MGF(L, S_CY);
-    double cxm = 0.5 * (cx[q - 1] + cx[n - 1]);
-    double cxp = 0.5 * (cx[q] + cx[n]);
-    double cym = 0.5 * (cy[q] + cy[s]);
-    double cyp = 0.5 * (cy[q] + cy[n]);
+    double cxm = 0.5 * (fl.x(q - 1) + fl.x(n - 1));
+    double cxp = 0.5 * (fl.x(q) + fl.x(n));
+    const double cyq = fl.y(q);
+    double cym = 0.5 * (cyq + fl.y(s));
+    double cyp = 0.5 * (cyq + fl.y(n));
     double dx_ = L.amu * (MGF(L, S_AREAX)[q] / L.dx);
     double dy_ = L.amu * (MGF(L, S_AREAY)[q] / L.dy);
     Coef k;
@@ -94,10 +113,10 @@ __device__ __forceinline__ Coef coef_v(const LevelDev &L, int i, int j)
 // receives from the host-only loop :939-963, in that loop's order (codes built by
 // mgfvm_build_obstacle_prog: 0 ae from the east cell, 1 aw from the west cell,
 // 2 an from the north cell, 3 as from the south cell; count in bits 28-31).
-__device__ __forceinline__ Coef coef_sc(const LevelDev &L, int i, int j)
+template <class F>
+__device__ __forceinline__ Coef coef_sc(const LevelDev &L, const F &fl, int i, int j)
 {
     const int nx = L.npx, q = j * nx + i, s = q - nx;
-    const double *cx = MGF(L, S_CX), *cy = MGF(L, S_CY);
     const double *ax = MGF(L, S_AREAX), *ay = MGF(L, S_AREAY);
     const double amusc = L.amusc;
     double dxm = amusc * (ax[q - 1] / L.dx);
@@ -105,10 +124,10 @@ __device__ __forceinline__ Coef coef_sc(const LevelDev &L, int i, int j)
     double dxp = amusc * (ax[q] / L.dx);
     double dyp = amusc * (ay[q] / L.dy);
     Coef k;
-    k.aw = hyb_p(cx[q - 1], dxm);
-    k.ae = hyb_m(cx[q], dxp);
-    k.as = hyb_p(cy[s], dym);
-    k.an = hyb_m(cy[q], dyp);
+    k.aw = hyb_p(fl.x(q - 1), dxm);
+    k.ae = hyb_m(fl.x(q), dxp);
+    k.as = hyb_p(fl.y(s), dym);
+    k.an = hyb_m(fl.y(q), dyp);
     k.ap = k.aw + k.ae + k.as + k.an;
     if (L.seq) {
         unsigned code = L.seq[q];
@@ -126,19 +145,20 @@ __device__ __forceinline__ Coef coef_sc(const LevelDev &L, int i, int j)
     return k;
 }
 
-__device__ __forceinline__ void store_coef(const LevelDev &L, int q, const Coef &k)
+__device__ __forceinline__ void store_coef(const LevelDev &L, int eq, int q, const Coef &k, double su)
 {
-    MGF(L, S_AW)[q] = k.aw; MGF(L, S_AE)[q] = k.ae;
-    MGF(L, S_AS)[q] = k.as; MGF(L, S_AN)[q] = k.an;
-    MGF(L, S_AP)[q] = k.ap;
+    MGF(L, co_slot(eq, CK_AW))[q] = k.aw; MGF(L, co_slot(eq, CK_AE))[q] = k.ae;
+    MGF(L, co_slot(eq, CK_AS))[q] = k.as; MGF(L, co_slot(eq, CK_AN))[q] = k.an;
+    MGF(L, co_slot(eq, CK_AP))[q] = k.ap; MGF(L, co_slot(eq, CK_SU))[q] = su;
 }
 
 // ---------------------------------------------------------- assembly ops
 // solve_u's assembly: coefu :815-860 then umom :741-767 at one u face
-__device__ __forceinline__ void cell_mom_u(const LevelDev &L, const CaseDev &C, int i, int j)
+template <class F>
+__device__ __forceinline__ void cell_mom_u(const LevelDev &L, const CaseDev &C, const F &fl, int i, int j)
 {
     const int q = j * L.npx + i;
-    Coef k = coef_u(L, i, j);
+    Coef k = coef_u(L, fl, i, j);
     const double ax = MGF(L, S_AREAX)[q];
     const double rm = C.relxm, rm1 = 1.0 - C.relxm;
     double su = ax * (MGF(L, S_P)[q] - MGF(L, S_P)[q + 1]);
@@ -146,16 +166,16 @@ __device__ __forceinline__ void cell_mom_u(const LevelDev &L, const CaseDev &C, 
     su = su + rm1 * ap * MGF(L, S_U)[q] + MGF(L, S_RESU)[q] + C.dpdxm * ax * MGF(L, S_AREAY)[q];
     ap = ap + MGF(L, S_SPU)[q];
     k.ap = ap;
-    store_coef(L, q, k);
+    store_coef(L, EQ_U, q, k, su);
     MGF(L, S_APU)[q] = ap;
-    MGF(L, S_SU)[q] = su;
 }
 
 // solve_v's assembly: coefv :966-1016 then vmom :769-793 at one v face
-__device__ __forceinline__ void cell_mom_v(const LevelDev &L, const CaseDev &C, int i, int j)
+template <class F>
+__device__ __forceinline__ void cell_mom_v(const LevelDev &L, const CaseDev &C, const F &fl, int i, int j)
 {
     const int q = j * L.npx + i;
-    Coef k = coef_v(L, i, j);
+    Coef k = coef_v(L, fl, i, j);
     const double ay = MGF(L, S_AREAY)[q];
     const double rm = C.relxm, rm1 = 1.0 - C.relxm;
     double su = ay * (MGF(L, S_P)[q] - MGF(L, S_P)[q + L.npx]);
@@ -163,9 +183,37 @@ __device__ __forceinline__ void cell_mom_v(const LevelDev &L, const CaseDev &C, 
     su = su + rm1 * ap * MGF(L, S_V)[q] + MGF(L, S_RESV)[q] + C.dpdym * MGF(L, S_AREAX)[q] * ay;
     ap = ap + MGF(L, S_SPV)[q];
     k.ap = ap;
-    store_coef(L, q, k);
+    store_coef(L, EQ_V, q, k, su);
     MGF(L, S_APV)[q] = ap;
-    MGF(L, S_SU)[q] = su;
+}
+
+// solve_sc's assembly: coefsc :861-964 (+ obstacle faces) then scalar :795-812
+template <class F>
+__device__ __forceinline__ void cell_sc(const LevelDev &L, const CaseDev &C, const F &fl, int i, int j)
+{
+    const int q = j * L.npx + i;
+    Coef k = coef_sc(L, fl, i, j);
+    const double spsc = MGF(L, S_SPSC)[q];
+    double su = spsc * C.sc_obs + MGF(L, S_RESSC)[q];
+    k.ap = k.ap + spsc;
+    store_coef(L, EQ_SC, q, k, su);
+}
+
+// The three assemblies that depend only on the fluxes at the start of a level
+// visit, plus those fluxes, at cell (i, j) of the full padded array.
+enum AsmBits { A_FLUX = 1, A_U = 2, A_V = 4, A_SC = 8, A_SC_OUTFLOW = 16 };
+template <class F>
+__device__ __forceinline__ void cell_asm(const LevelDev &L, const CaseDev &C, const F &fl, int i, int j,
+                                         unsigned what)
+{
+    const int nx = L.npx, ny = L.npy;
+    if ((what & A_FLUX) && i <= nx - 2 && j <= ny - 2) cell_fluxes(L, j * nx + i);
+    const bool in = i >= 1 && j >= 1 && i <= nx - 2 && j <= ny - 2;
+    if ((what & A_U) && in && i <= nx - 3) cell_mom_u(L, C, fl, i, j);
+    if ((what & A_V) && in && j <= ny - 3) cell_mom_v(L, C, fl, i, j);
+    if ((what & A_SC) && in) cell_sc(L, C, fl, i, j);
+    // the scalar part of outflow (:1226), which the down leg applies before solve_sc
+    if ((what & A_SC_OUTFLOW) && i == nx - 1 && C.ibc_xp == 4) MGF(L, S_SC)[j * nx + i] = MGF(L, S_SC)[j * nx + i - 1];
 }
 
 // solve_pprime's assembly: masserror :1096-1125 then coefp :1018-1092 (with the
@@ -191,8 +239,7 @@ __device__ __forceinline__ double cell_mass_coefp(const LevelDev &L, const CaseD
     if (C.ibc_xp == 2 && i == nx - 2) { k.ap = k.ap + diag; su = 0.0; }
     if (C.ibc_ym == 2 && j == 1) { k.ap = k.ap + diag; su = 0.0; }
     if (C.ibc_yp == 2 && j == ny - 2) { k.ap = k.ap + diag; su = 0.0; }
-    store_coef(L, q, k);
-    MGF(L, S_SU)[q] = su;
+    store_coef(L, EQ_PP, q, k, su);
     return fabs(div);
 }
 
@@ -208,37 +255,44 @@ __device__ __forceinline__ void cell_update(const LevelDev &L, const CaseDev &C,
     p[q] += C.relxp * (ppq - ppref);
 }
 
-// solve_sc's assembly: coefsc :861-964 (+ obstacle faces) then scalar :795-812
-__device__ __forceinline__ void cell_sc(const LevelDev &L, const CaseDev &C, int i, int j)
-{
-    const int q = j * L.npx + i;
-    Coef k = coef_sc(L, i, j);
-    const double spsc = MGF(L, S_SPSC)[q];
-    double su = spsc * C.sc_obs + MGF(L, S_RESSC)[q];
-    k.ap = k.ap + spsc;
-    store_coef(L, q, k);
-    MGF(L, S_SU)[q] = su;
-}
-
 // --------------------------------------------------------------- smoothers
-// one Jacobi point update, wj = 1 (solver :1259-1286)
-__device__ __forceinline__ void cell_jacobi(const LevelDev &L, const double *cur, double *nxt, int q)
+__device__ __forceinline__ int eq_field(int e) { return e == EQ_U ? S_U : e == EQ_V ? S_V : e == EQ_PP ? S_PP : S_SC; }
+__device__ __forceinline__ int eq_tmp(int e) { return e == EQ_V ? S_TMP1 : e == EQ_SC ? S_TMP2 : S_TMP0; }
+
+// Jacobi point update with wj = 1 (solver :1259-1286) from neighbour values
+__device__ __forceinline__ double jacobi_value(double aw, double ae, double as, double an, double ap, double su,
+                                               double pw, double pe, double ps, double pn, double pc)
 {
-    const int nx = L.npx;
     const double wj = 1.0;
-    double nb = MGF(L, S_AW)[q] * cur[q - 1] + MGF(L, S_AE)[q] * cur[q + 1]
-              + MGF(L, S_AS)[q] * cur[q - nx] + MGF(L, S_AN)[q] * cur[q + nx];
-    double g = (nb + MGF(L, S_SU)[q]) / (MGF(L, S_AP)[q] + 1.0e-30);
-    nxt[q] = (1.0 - wj) * cur[q] + wj * g;
+    double nb = aw * pw + ae * pe + as * ps + an * pn;
+    double g = (nb + su) / (ap + 1.0e-30);
+    return (1.0 - wj) * pc + wj * g;
 }
 
-// one red-black Gauss-Seidel point update (solvergs :1308-1350)
-__device__ __forceinline__ void cell_gs(const LevelDev &L, double *phi, int q)
+// red-black Gauss-Seidel point update (solvergs :1308-1350)
+__device__ __forceinline__ double gs_value(double aw, double ae, double as, double an, double ap, double su,
+                                           double pw, double pe, double ps, double pn)
+{
+    double nb = aw * pw + ae * pe + as * ps + an * pn;
+    return (nb + su) / ap;
+}
+
+__device__ __forceinline__ void cell_jacobi(const LevelDev &L, int e, const double *cur, double *nxt, int q)
 {
     const int nx = L.npx;
-    double nb = MGF(L, S_AW)[q] * phi[q - 1] + MGF(L, S_AE)[q] * phi[q + 1]
-              + MGF(L, S_AS)[q] * phi[q - nx] + MGF(L, S_AN)[q] * phi[q + nx];
-    phi[q] = (nb + MGF(L, S_SU)[q]) / MGF(L, S_AP)[q];
+    nxt[q] = jacobi_value(MGF(L, co_slot(e, CK_AW))[q], MGF(L, co_slot(e, CK_AE))[q],
+                          MGF(L, co_slot(e, CK_AS))[q], MGF(L, co_slot(e, CK_AN))[q],
+                          MGF(L, co_slot(e, CK_AP))[q], MGF(L, co_slot(e, CK_SU))[q],
+                          cur[q - 1], cur[q + 1], cur[q - nx], cur[q + nx], cur[q]);
+}
+
+__device__ __forceinline__ void cell_gs(const LevelDev &L, int e, double *phi, int q)
+{
+    const int nx = L.npx;
+    phi[q] = gs_value(MGF(L, co_slot(e, CK_AW))[q], MGF(L, co_slot(e, CK_AE))[q],
+                      MGF(L, co_slot(e, CK_AS))[q], MGF(L, co_slot(e, CK_AN))[q],
+                      MGF(L, co_slot(e, CK_AP))[q], MGF(L, co_slot(e, CK_SU))[q],
+                      phi[q - 1], phi[q + 1], phi[q - nx], phi[q + nx]);
 }
 
 // ------------------------------------------------------------ restriction
@@ -255,10 +309,11 @@ __device__ __forceinline__ void cell_restv(const LevelDev &F, const LevelDev &K,
 }
 
 // residual of the u equation at face (i, j) (restru :1494-1512 fine, :1528-1541 coarse)
-__device__ __forceinline__ double resid_u(const LevelDev &L, const CaseDev &C, int i, int j, bool fine)
+template <class F>
+__device__ __forceinline__ double resid_u(const LevelDev &L, const CaseDev &C, const F &fl, int i, int j, bool fine)
 {
     const int nx = L.npx, q = j * nx + i;
-    Coef k = coef_u(L, i, j);
+    Coef k = coef_u(L, fl, i, j);
     const double *u = MGF(L, S_U), *p = MGF(L, S_P);
     const double ax = MGF(L, S_AREAX)[q], ay = MGF(L, S_AREAY)[q];
     double r = k.aw * u[q - 1] + k.ae * u[q + 1] + k.as * u[q - nx] + k.an * u[q + nx]
@@ -273,10 +328,11 @@ __device__ __forceinline__ double resid_u(const LevelDev &L, const CaseDev &C, i
 }
 
 // residual of the v equation (restrv :1670-1688 fine, :1704-1718 coarse)
-__device__ __forceinline__ double resid_v(const LevelDev &L, const CaseDev &C, int i, int j, bool fine)
+template <class F>
+__device__ __forceinline__ double resid_v(const LevelDev &L, const CaseDev &C, const F &fl, int i, int j, bool fine)
 {
     const int nx = L.npx, q = j * nx + i;
-    Coef k = coef_v(L, i, j);
+    Coef k = coef_v(L, fl, i, j);
     const double *v = MGF(L, S_V), *p = MGF(L, S_P);
     const double ax = MGF(L, S_AREAX)[q], ay = MGF(L, S_AREAY)[q];
     double r = k.aw * v[q - 1] + k.ae * v[q + 1] + k.as * v[q - nx] + k.an * v[q + nx]
@@ -291,10 +347,11 @@ __device__ __forceinline__ double resid_v(const LevelDev &L, const CaseDev &C, i
 }
 
 // residual of the scalar equation (restrsc :1585-1600 fine, :1618-1630 coarse)
-__device__ __forceinline__ double resid_sc(const LevelDev &L, int i, int j, bool fine)
+template <class F>
+__device__ __forceinline__ double resid_sc(const LevelDev &L, const F &fl, int i, int j, bool fine)
 {
     const int nx = L.npx, q = j * nx + i;
-    Coef k = coef_sc(L, i, j);
+    Coef k = coef_sc(L, fl, i, j);
     const double *s = MGF(L, S_SC);
     double r = k.aw * s[q - 1] + k.ae * s[q + 1] + k.as * s[q - nx] + k.an * s[q + nx] - k.ap * s[q];
     if (fine) r = r + MGF(L, S_RESSC)[q];
@@ -303,30 +360,34 @@ __device__ __forceinline__ double resid_sc(const LevelDev &L, int i, int j, bool
 
 // FAS defects of all three transported equations at coarse cell (ic, jc):
 // restru :1546-1563, restrv :1722-1738, restrsc :1634-1647, each fine residual
-// evaluated where the reference's restriction stencil reads it.
+// evaluated where the reference's restriction stencil reads it.  Fine fluxes come
+// from the arrays fluxes(fine) filled; coarse fluxes are recomputed from the coarse
+// u, v that restv just wrote.
 __device__ __forceinline__ void cell_restrict(const LevelDev &F, const LevelDev &K, const CaseDev &C,
                                               int ic, int jc)
 {
+    const FluxArrays ff(F);
+    const FluxLive fk(K);
     const int nxc = K.npx, nyc = K.npy, qc = jc * nxc + ic;
     const int i = 2 * ic, j = 2 * jc;
     if (ic <= nxc - 3) {
-        double r0 = resid_u(F, C, i, j, true), r1 = resid_u(F, C, i, j - 1, true);
-        double r2 = resid_u(F, C, i - 1, j, true), r3 = resid_u(F, C, i - 1, j - 1, true);
-        double r4 = resid_u(F, C, i + 1, j, true), r5 = resid_u(F, C, i + 1, j - 1, true);
-        double rc = resid_u(K, C, ic, jc, false);
+        double r0 = resid_u(F, C, ff, i, j, true), r1 = resid_u(F, C, ff, i, j - 1, true);
+        double r2 = resid_u(F, C, ff, i - 1, j, true), r3 = resid_u(F, C, ff, i - 1, j - 1, true);
+        double r4 = resid_u(F, C, ff, i + 1, j, true), r5 = resid_u(F, C, ff, i + 1, j - 1, true);
+        double rc = resid_u(K, C, fk, ic, jc, false);
         MGF(K, S_RESU)[qc] = (r0 + r1) + 0.5 * (r2 + r3 + r4 + r5) - rc;
     }
     if (jc <= nyc - 3) {
-        double r0 = resid_v(F, C, i, j, true), r1 = resid_v(F, C, i - 1, j, true);
-        double r2 = resid_v(F, C, i, j - 1, true), r3 = resid_v(F, C, i - 1, j - 1, true);
-        double r4 = resid_v(F, C, i, j + 1, true), r5 = resid_v(F, C, i - 1, j + 1, true);
-        double rc = resid_v(K, C, ic, jc, false);
+        double r0 = resid_v(F, C, ff, i, j, true), r1 = resid_v(F, C, ff, i - 1, j, true);
+        double r2 = resid_v(F, C, ff, i, j - 1, true), r3 = resid_v(F, C, ff, i - 1, j - 1, true);
+        double r4 = resid_v(F, C, ff, i, j + 1, true), r5 = resid_v(F, C, ff, i - 1, j + 1, true);
+        double rc = resid_v(K, C, fk, ic, jc, false);
         MGF(K, S_RESV)[qc] = (r0 + r1) + 0.5 * (r2 + r3 + r4 + r5) - rc;
     }
     {
-        double r0 = resid_sc(F, i, j, true), r1 = resid_sc(F, i, j - 1, true);
-        double r2 = resid_sc(F, i - 1, j, true), r3 = resid_sc(F, i - 1, j - 1, true);
-        double rc = resid_sc(K, ic, jc, false);
+        double r0 = resid_sc(F, ff, i, j, true), r1 = resid_sc(F, ff, i, j - 1, true);
+        double r2 = resid_sc(F, ff, i - 1, j, true), r3 = resid_sc(F, ff, i - 1, j - 1, true);
+        double rc = resid_sc(K, fk, ic, jc, false);
         MGF(K, S_RESSC)[qc] = (r0 + r1 + r2 + r3) - rc;
     }
 }
@@ -441,14 +502,14 @@ __device__ __forceinline__ void cell_prol_apply(const LevelDev &F, const LevelDe
 }
 
 // ---------------------------------------------------------- boundary lines
-// outflow :1211-1228, row j
-__device__ __forceinline__ void row_outflow(const LevelDev &L, int j)
+// outflow :1211-1228 at row j; `with_sc` also copies the scalar ghost
+__device__ __forceinline__ void row_outflow(const LevelDev &L, int j, bool with_sc)
 {
     const int q = j * L.npx + L.npx - 1;
     MGF(L, S_U)[q - 1] = MGF(L, S_U)[q - 2];
     MGF(L, S_V)[q] = MGF(L, S_V)[q - 1];
     MGF(L, S_P)[q] = MGF(L, S_P)[q - 1];
-    MGF(L, S_SC)[q] = MGF(L, S_SC)[q - 1];
+    if (with_sc) MGF(L, S_SC)[q] = MGF(L, S_SC)[q - 1];
 }
 
 // pbound x-periodic :1185-1195, row j in [1, npy-2]

@@ -1,13 +1,15 @@
 // mg_common.cuh — device-side data layout of the engine.
 //
-// HBM layout: one pool allocation per context.  Every (case, level) owns NSLOTS
+// HBM layout: one pool allocation per context.  Every (case, level) owns NSLOTS_LEVEL
 // FP64 arrays of npx*npy in the reference's row-major order (ij = j*npx + i,
 // Version-6-26-04.c:554), each aligned to 256 B, plus an int tag array and an
-// optional per-cell obstacle-code array.  Slots 0..24 are the arrays of the
-// reference's struct SoA (:42-54) in the order of enum mgfvm_field; the rest are
-// engine buffers: the Jacobi ping-pong array, one prolongation correction per
-// variable (the reference shares one `c`, :1745-2028), and the level-0 state of
-// the previous cycle for the fixed-point test.
+// optional per-cell obstacle-code array.  The reference keeps one set of
+// coefficient arrays (aw, ae, as, an, ap, su) that each equation overwrites in
+// turn (:815-1092); here each equation has its own set, so the u, v and scalar
+// equations of a level visit — which depend only on the fluxes at the start of the
+// visit — are assembled in one kernel and smoothed in the same launches.  The
+// reference's single prolongation scratch `c` (:1745-2028) becomes one correction
+// array per variable for the same reason.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -17,20 +19,23 @@
 
 namespace mg {
 
+enum Eq { EQ_U = 0, EQ_V = 1, EQ_PP = 2, EQ_SC = 3 };
+enum CoefK { CK_AW = 0, CK_AE, CK_AS, CK_AN, CK_AP, CK_SU, NCOEF };
+
 enum Slot {
-    S_U = MGFVM_F_U, S_V = MGFVM_F_V, S_P = MGFVM_F_P, S_PP = MGFVM_F_PP, S_SC = MGFVM_F_SC,
-    S_SU = MGFVM_F_SU, S_RS = MGFVM_F_RS, S_RESU = MGFVM_F_RESU, S_RESV = MGFVM_F_RESV,
-    S_RESSC = MGFVM_F_RESSC, S_C = MGFVM_F_C,     // S_C: the scalar correction (prolsc's c)
-    S_AW = MGFVM_F_AW, S_AE = MGFVM_F_AE, S_AS = MGFVM_F_AS, S_AN = MGFVM_F_AN,
-    S_AP = MGFVM_F_AP, S_APU = MGFVM_F_APU, S_APV = MGFVM_F_APV, S_SPU = MGFVM_F_SPU,
-    S_SPV = MGFVM_F_SPV, S_SPSC = MGFVM_F_SPSC, S_CX = MGFVM_F_CX, S_CY = MGFVM_F_CY,
-    S_AREAX = MGFVM_F_AREAX, S_AREAY = MGFVM_F_AREAY,
-    S_TMP = MGFVM_NFIELDS,   // Jacobi ping-pong buffer
+    S_U = 0, S_V, S_P, S_PP, S_SC,
+    S_RESU, S_RESV, S_RESSC, S_APU, S_APV, S_SPU, S_SPV, S_SPSC,
+    S_CX, S_CY, S_AREAX, S_AREAY, S_RS,
+    S_C,                     // scalar prolongation correction (the reference's c after prolsc)
     S_CU, S_CV, S_CP,        // u, v, p prolongation corrections
-    NSLOTS_LEVEL,
+    S_TMP0, S_TMP1, S_TMP2,  // Jacobi ping-pong buffers (u or p', v, sc)
+    S_CO,                    // 4 equations x {aw, ae, as, an, ap, su}
+    NSLOTS_LEVEL = S_CO + 4 * NCOEF,
     S_PREV_U = NSLOTS_LEVEL, S_PREV_V, S_PREV_P, S_PREV_SC,   // level 0 only
     NSLOTS
 };
+
+__host__ __device__ constexpr int co_slot(int eq, int k) { return S_CO + NCOEF * eq + k; }
 
 constexpr int MAXLEV = 16;
 constexpr int RED_STRIDE = 16;   // doubles per block in the reduction partials
@@ -90,9 +95,8 @@ enum Mode {
     M_UP            // up-leg SIMPLE step on level ig after M_PROLONG
 };
 
-__device__ __forceinline__ bool case_active(const CaseDev &C, int ig, int mode)
+__host__ __device__ __forceinline__ bool mode_active(const CaseDev &C, int ig, int mode)
 {
-    if (C.done) return false;
     switch (mode) {
     case M_OP: return ig < C.ngrid;
     case M_OP_PAIR: return ig + 1 < C.ngrid;
@@ -104,6 +108,11 @@ __device__ __forceinline__ bool case_active(const CaseDev &C, int ig, int mode)
     case M_UP: return ig + 1 <= C.tail && ig + 1 < C.ngrid;
     default: return false;
     }
+}
+
+__device__ __forceinline__ bool case_active(const CaseDev &C, int ig, int mode)
+{
+    return !C.done && mode_active(C, ig, mode);
 }
 
 }  // namespace mg

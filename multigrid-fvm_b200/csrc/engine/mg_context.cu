@@ -34,7 +34,7 @@ using namespace mg;
         if (r_ != MGFVM_OK) return r_; \
     } while (0)
 
-static const int TAIL_AUTO_CELLS = 70 * 70;   // levels at or below ~66x66 padded cells
+static const int TAIL_AUTO_CELLS = 0;   // automatic choice: grid kernels on every level (measured fastest)
 static const int HIST_INITIAL = 4096;
 
 struct mgfvm_ctx {
@@ -62,6 +62,7 @@ struct mgfvm_ctx {
     cudaGraphExec_t gexec = nullptr;
     std::vector<Launch> cyc;
     std::vector<int> maxcells;                // per level: max npx*npy over cases
+    int last_eq[MAXLEV];                      // per level: equation of the visible coefficient set
     long long launches = 0;
     long long h2d = 0, d2h = 0;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -76,22 +77,6 @@ static inline int nblk(long long n) { return (int)std::max<long long>(1, (n + BL
 // ------------------------------------------------------------------ schedule
 namespace {
 
-// Host mirror of case_active() in mg_common.cuh (without the per-case done flag).
-bool host_active(const CaseDev &C, int ig, int mode)
-{
-    switch (mode) {
-    case M_OP: return ig < C.ngrid;
-    case M_OP_PAIR: return ig + 1 < C.ngrid;
-    case M_OP_C: return ig >= 1 && ig < C.ngrid;
-    case M_DOWN: return ig < C.tail;
-    case M_RESTRICT: return ig < C.tail && ig + 1 < C.ngrid;
-    case M_RESTRICT_C: return ig >= 1 && ig - 1 < C.tail && ig < C.ngrid;
-    case M_PROLONG:
-    case M_UP: return ig + 1 <= C.tail && ig + 1 < C.ngrid;
-    default: return false;
-    }
-}
-
 struct Builder {
     mgfvm_ctx *x;
     std::vector<Launch> *out;
@@ -99,41 +84,59 @@ struct Builder {
     bool any(int ig, int mode) const
     {
         for (const CaseDev &C : x->hc)
-            if (host_active(C, ig, mode)) return true;
+            if (mode_active(C, ig, mode)) return true;
         return false;
     }
-    void add(int kernel, int ig, int mode, long long cells, int a0 = 0, int a1 = 0)
+    Launch &add(int kernel, int ig, int mode, long long cells, int a0 = 0, int a1 = 0, int a2 = 0, int a3 = 0)
     {
         Launch L{};
-        L.kernel = kernel; L.ig = ig; L.mode = mode; L.a0 = a0; L.a1 = a1;
+        L.kernel = kernel; L.ig = ig; L.mode = mode; L.a0 = a0; L.a1 = a1; L.a2 = a2; L.a3 = a3;
         L.grid = dim3(nblk(cells), x->ncases);
         L.block = BLOCK;
         out->push_back(L);
+        return out->back();
     }
     long long cells(int ig) const { return ig < (int)x->maxcells.size() ? x->maxcells[ig] : 0; }
-    long long half_cells(int ig) const
+    long long tiles(int ig) const
     {
         long long m = 0;
         for (const mgfvm_config &c : x->cfg)
-            if (ig < c.ngrid) m = std::max<long long>(m, (long long)(npx_of(c, ig) / 2 + 1) * npy_of(c, ig));
-        return m;
+            if (ig < c.ngrid) {
+                const long long w = npx_of(c, ig) - 2, h = npy_of(c, ig) - 2;
+                m = std::max(m, ((w + TILE_X - 1) / TILE_X) * ((h + TILE_Y - 1) / TILE_Y));
+            }
+        return std::max<long long>(m, 1);
     }
-    void smooth(int ig, int mode, int e)
+    // `nsw` sweeps of the equations in `mask`: the 2*nsw half-sweeps (Gauss-Seidel) or
+    // nsw sweeps (Jacobi) go in an even number of tile launches of at most MAX_UNITS
+    // each, alternating field -> buffer -> field; a single Jacobi sweep copies back.
+    void smooth(int ig, int mode, int mask, int nsw)
     {
-        const int nsw = e == 2 ? x->sched.nswpp : x->sched.nswpm;
-        if (x->sched.isolve == MGFVM_JACOBI) {
-            for (int it = 0; it < nsw; ++it) add(K_JACOBI, ig, mode, cells(ig), e, it);
-            if (nsw & 1) add(K_JACOBI_COPYBACK, ig, mode, cells(ig), e);
-        } else {
-            for (int it = 0; it < nsw; ++it)
-                for (int c = 0; c < 2; ++c) add(K_GS, ig, mode, half_cells(ig), e, c);
+        const int isolve = x->sched.isolve;
+        const int units = isolve == MGFVM_GAUSS_SEIDEL ? 2 * nsw : nsw;
+        if (units <= 0 || (isolve != MGFVM_JACOBI && isolve != MGFVM_GAUSS_SEIDEL)) return;
+        int chunks = (units + MAX_UNITS - 1) / MAX_UNITS;
+        if ((chunks & 1) && units >= chunks + 1) ++chunks;
+        const int neq = __builtin_popcount((unsigned)mask);
+        int u0 = 0;
+        for (int c = 0; c < chunks; ++c) {
+            const int nu = units / chunks + (c < units % chunks ? 1 : 0);
+            Launch &L = add(K_SMOOTH, ig, mode, 0, mask, u0, nu, c & 1);
+            L.grid = dim3((unsigned)tiles(ig), x->ncases, neq);
+            L.block = SMOOTH_BLOCK;
+            L.smem = smooth_smem_bytes(isolve, nu);
+            u0 += nu;
+        }
+        if (chunks & 1) {
+            Launch &L = add(K_COPY, ig, mode, cells(ig), mask);
+            L.grid.z = neq;
         }
     }
     void pfix(int ig, int mode)
     {
         int maxcopy = 0, haz = 0;
         for (int c = 0; c < x->ncases; ++c) {
-            if (!host_active(x->hc[c], ig, mode)) continue;
+            if (!mode_active(x->hc[c], ig, mode)) continue;
             const mgfvm_obstacle_prog &P = x->progs[c * MAXLEV + ig];
             maxcopy = std::max(maxcopy, P.ncopy);
             haz |= P.hazard;
@@ -142,57 +145,38 @@ struct Builder {
         if (haz) { add(K_PFIX, ig, mode, maxcopy, 0); add(K_PFIX, ig, mode, maxcopy, 1); }
         else add(K_PFIX, ig, mode, maxcopy, 2);
     }
-    bool any_bc(int which) const
+    // pbound + outflow (bits as k_bound); skipped when no case has such a boundary
+    void bound(int ig, int mode, int bits)
     {
-        for (const CaseDev &C : x->hc) {
-            if (which == 0 && (C.ibc_xm == 3 || C.ibc_ym == 3)) return true;
-            if (which == 1 && C.ibc_xp == 4) return true;
-        }
-        return false;
+        bool need = false;
+        for (const CaseDev &C : x->hc)
+            need |= ((bits & 1) && (C.ibc_xm == 3 || C.ibc_ym == 3)) || ((bits & 6) && C.ibc_xp == 4);
+        if (!need) return;
+        Launch &L = add(K_BOUND, ig, mode, 1, bits);
+        L.grid = dim3(1, x->ncases);
     }
-    void periodic(int ig, int mode)
-    {
-        if (!any_bc(0)) return;
-        Launch L{};
-        L.kernel = K_PERIODIC; L.ig = ig; L.mode = mode;
-        L.grid = dim3(1, x->ncases); L.block = BLOCK;
-        out->push_back(L);
-    }
-    void outflow(int ig, int mode)
-    {
-        if (!any_bc(1)) return;
-        long long m = 0;
-        for (const mgfvm_config &c : x->cfg) if (ig < c.ngrid) m = std::max<long long>(m, npy_of(c, ig));
-        add(K_OUTFLOW, ig, mode, m);
-    }
-    void solve_u(int ig, int mode) { add(K_MOM_U, ig, mode, cells(ig)); smooth(ig, mode, 0); }
-    void solve_v(int ig, int mode) { add(K_MOM_V, ig, mode, cells(ig)); smooth(ig, mode, 1); }
     void solve_pp(int ig, int mode, bool reduce)
     {
         add(K_MASS_COEFP, ig, mode, cells(ig), reduce ? 1 : 0);
-        smooth(ig, mode, 2);
+        smooth(ig, mode, 1 << EQ_PP, x->sched.nswpp);
         add(K_UPDATE, ig, mode, cells(ig));
         pfix(ig, mode);
     }
-    void solve_sc(int ig, int mode) { add(K_SC, ig, mode, cells(ig)); smooth(ig, mode, 3); }
-    // one SIMPLE step: down leg :201-207, up leg :235-244
+    // One SIMPLE step (down leg :201-207, up leg :235-244).  u, v and sc depend only
+    // on the visit-start fluxes, so they are assembled together and smoothed in the
+    // same launches; the scalar's outflow ghost moves with its equation.
     void step(int ig, int mode, bool down, bool reduce)
     {
-        add(K_FLUXES, ig, mode, cells(ig));
-        solve_u(ig, mode);
-        solve_v(ig, mode);
+        const int what = A_FLUX | A_U | A_V | A_SC | (down ? A_SC_OUTFLOW : 0);
+        add(K_ASM, ig, mode, cells(ig), what, 1);
+        smooth(ig, mode, (1 << EQ_U) | (1 << EQ_V) | (1 << EQ_SC), x->sched.nswpm);
         solve_pp(ig, mode, reduce);
-        periodic(ig, mode);
-        if (down) outflow(ig, mode);
-        solve_sc(ig, mode);
-        if (!down) outflow(ig, mode);
+        bound(ig, mode, down ? 3 : 7);
     }
     // :211-220
-    void restrict_(int ig, int mode_f, int mode_c)
+    void restrict_(int ig, int mode_f)
     {
-        add(K_RESTV, ig, mode_f, cells(ig + 1));
-        add(K_FLUXES, ig + 1, mode_c, cells(ig + 1));
-        add(K_FLUXES, ig, mode_f, cells(ig));
+        add(K_RESTV_FLUXES, ig, mode_f, cells(ig));
         add(K_RESTRICT, ig, mode_f, cells(ig + 1));
     }
     // :230-233
@@ -205,13 +189,22 @@ struct Builder {
     {
         for (int ig = 0; ig < x->maxng; ++ig) {
             if (any(ig, M_DOWN)) step(ig, M_DOWN, true, ig == 0);
-            if (any(ig, M_RESTRICT)) restrict_(ig, M_RESTRICT, M_RESTRICT_C);
+            if (any(ig, M_RESTRICT)) restrict_(ig, M_RESTRICT);
         }
         bool tail = false;
         for (const CaseDev &C : x->hc) tail |= C.tail < C.ngrid;
         if (tail) {
+            // shared memory: every equation of the largest coarse-kernel level at once
+            long long need = 0;
+            for (int c = 0; c < x->ncases; ++c) {
+                const CaseDev &C = x->hc[c];
+                if (C.tail < C.ngrid)
+                    need = std::max<long long>(need, 24LL * npx_of(x->cfg[c], C.tail) * npy_of(x->cfg[c], C.tail) *
+                                                         (long long)sizeof(double));
+            }
             Launch L{};
             L.kernel = K_TAIL; L.grid = dim3(x->ncases); L.block = TAIL_BLOCK;
+            L.smem = (int)std::min<long long>(need, TAIL_SMEM_MAX);
             out->push_back(L);
         }
         for (int ig = x->maxng - 1; ig > 0; --ig) {
@@ -232,22 +225,77 @@ struct Builder {
     {
         switch (op) {
         case MGFVM_OP_FLUXES: add(K_FLUXES, ig, M_OP, cells(ig)); break;
-        case MGFVM_OP_SOLVE_U: solve_u(ig, M_OP); break;
-        case MGFVM_OP_SOLVE_V: solve_v(ig, M_OP); break;
+        case MGFVM_OP_SOLVE_U:
+            add(K_ASM, ig, M_OP, cells(ig), A_U, 0);
+            smooth(ig, M_OP, 1 << EQ_U, x->sched.nswpm);
+            break;
+        case MGFVM_OP_SOLVE_V:
+            add(K_ASM, ig, M_OP, cells(ig), A_V, 0);
+            smooth(ig, M_OP, 1 << EQ_V, x->sched.nswpm);
+            break;
         case MGFVM_OP_SOLVE_PP: solve_pp(ig, M_OP, true); break;
-        case MGFVM_OP_PBOUND: periodic(ig, M_OP); break;
-        case MGFVM_OP_OUTFLOW: outflow(ig, M_OP); break;
-        case MGFVM_OP_SOLVE_SC: solve_sc(ig, M_OP); break;
-        case MGFVM_OP_RESTRICT: restrict_(ig, M_OP_PAIR, M_OP_C); break;
+        case MGFVM_OP_PBOUND: bound(ig, M_OP, 1); break;
+        case MGFVM_OP_OUTFLOW: bound(ig, M_OP, 6); break;
+        case MGFVM_OP_SOLVE_SC:
+            add(K_ASM, ig, M_OP, cells(ig), A_SC, 0);
+            smooth(ig, M_OP, 1 << EQ_SC, x->sched.nswpm);
+            break;
+        case MGFVM_OP_RESTRICT: restrict_(ig, M_OP_PAIR); break;
         case MGFVM_OP_PROLONG: prolong(ig, M_OP_PAIR); break;
-        case MGFVM_OP_SMOOTH_U: smooth(ig, M_OP, 0); break;
-        case MGFVM_OP_SMOOTH_V: smooth(ig, M_OP, 1); break;
-        case MGFVM_OP_SMOOTH_PP: smooth(ig, M_OP, 2); break;
-        case MGFVM_OP_SMOOTH_SC: smooth(ig, M_OP, 3); break;
+        case MGFVM_OP_SMOOTH_U: smooth(ig, M_OP, 1 << EQ_U, x->sched.nswpm); break;
+        case MGFVM_OP_SMOOTH_V: smooth(ig, M_OP, 1 << EQ_V, x->sched.nswpm); break;
+        case MGFVM_OP_SMOOTH_PP: smooth(ig, M_OP, 1 << EQ_PP, x->sched.nswpp); break;
+        case MGFVM_OP_SMOOTH_SC: smooth(ig, M_OP, 1 << EQ_SC, x->sched.nswpm); break;
         default: break;
         }
     }
 };
+
+// Equation whose coefficient set a single-step op leaves as "the" coefficient arrays
+// (the reference has one set that every assembly overwrites); -1: unchanged.
+int op_equation(int op)
+{
+    switch (op) {
+    case MGFVM_OP_SOLVE_U: return EQ_U;
+    case MGFVM_OP_SOLVE_V: return EQ_V;
+    case MGFVM_OP_SOLVE_PP: return EQ_PP;
+    case MGFVM_OP_SOLVE_SC: return EQ_SC;
+    default: return -1;
+    }
+}
+
+// Slot holding the reference field `f` on a level whose last assembled equation is `eq`.
+int field_slot(int f, int eq)
+{
+    switch (f) {
+    case MGFVM_F_U: return S_U;
+    case MGFVM_F_V: return S_V;
+    case MGFVM_F_P: return S_P;
+    case MGFVM_F_PP: return S_PP;
+    case MGFVM_F_SC: return S_SC;
+    case MGFVM_F_SU: return co_slot(eq, CK_SU);
+    case MGFVM_F_RS: return S_RS;
+    case MGFVM_F_RESU: return S_RESU;
+    case MGFVM_F_RESV: return S_RESV;
+    case MGFVM_F_RESSC: return S_RESSC;
+    case MGFVM_F_C: return S_C;
+    case MGFVM_F_AW: return co_slot(eq, CK_AW);
+    case MGFVM_F_AE: return co_slot(eq, CK_AE);
+    case MGFVM_F_AS: return co_slot(eq, CK_AS);
+    case MGFVM_F_AN: return co_slot(eq, CK_AN);
+    case MGFVM_F_AP: return co_slot(eq, CK_AP);
+    case MGFVM_F_APU: return S_APU;
+    case MGFVM_F_APV: return S_APV;
+    case MGFVM_F_SPU: return S_SPU;
+    case MGFVM_F_SPV: return S_SPV;
+    case MGFVM_F_SPSC: return S_SPSC;
+    case MGFVM_F_CX: return S_CX;
+    case MGFVM_F_CY: return S_CY;
+    case MGFVM_F_AREAX: return S_AREAX;
+    case MGFVM_F_AREAY: return S_AREAY;
+    default: return -1;
+    }
+}
 
 int run_list(mgfvm_ctx *x, const std::vector<Launch> &v)
 {
@@ -319,6 +367,7 @@ int build_graph(mgfvm_ctx *x)
 
 int run_cycles(mgfvm_ctx *x, int n)
 {
+    for (int ig = 0; ig < MAXLEV; ++ig) x->last_eq[ig] = EQ_SC;
     if (x->opt.use_graph) {
         RC(build_graph(x));
         for (int k = 0; k < n; ++k) CK(cudaGraphLaunch(x->gexec, x->stream));
@@ -593,6 +642,8 @@ int create_impl(const mgfvm_config *cases, int ncases, const mgfvm_options *opt_
     x->hist_cap = 0;
     RC(push(x));
     RC(ensure_hist(x, HIST_INITIAL));
+    for (int ig = 0; ig < MAXLEV; ++ig) x->last_eq[ig] = EQ_SC;
+    CK(configure_kernels());
     RC(init_state(x, -1));
     Builder b{x, &x->cyc};
     b.cycle();
@@ -745,7 +796,8 @@ int mgfvm_get_field(mgfvm_ctx *x, int icase, int level, int field, double *out)
     if (field < 0 || field >= MGFVM_NFIELDS || !out) return mgfvm_fail(MGFVM_EINVAL, "bad field %d", field);
     CK(cudaStreamSynchronize(x->stream));
     const LevelDev &L = x->hc[icase].lv[level];
-    CK(cudaMemcpy(out, L.f[field], sizeof(double) * L.npx * L.npy, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(out, L.f[field_slot(field, x->last_eq[level])], sizeof(double) * L.npx * L.npy,
+                  cudaMemcpyDeviceToHost));
     x->d2h += (long long)sizeof(double) * L.npx * L.npy;
     return MGFVM_OK;
 }
@@ -757,7 +809,8 @@ int mgfvm_set_field(mgfvm_ctx *x, int icase, int level, int field, const double 
     if (field < 0 || field >= MGFVM_NFIELDS || !in) return mgfvm_fail(MGFVM_EINVAL, "bad field %d", field);
     CK(cudaStreamSynchronize(x->stream));
     const LevelDev &L = x->hc[icase].lv[level];
-    CK(cudaMemcpy(L.f[field], in, sizeof(double) * L.npx * L.npy, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(L.f[field_slot(field, x->last_eq[level])], in, sizeof(double) * L.npx * L.npy,
+                  cudaMemcpyHostToDevice));
     x->h2d += (long long)sizeof(double) * L.npx * L.npy;
     return MGFVM_OK;
 }
@@ -795,6 +848,7 @@ int mgfvm_op(mgfvm_ctx *x, int op, int level)
     b.op(op, level);
     RC(run_list(x, v));
     CK(cudaStreamSynchronize(x->stream));
+    if (op_equation(op) >= 0) x->last_eq[level] = op_equation(op);
     return MGFVM_OK;
 }
 
@@ -838,6 +892,35 @@ int mgfvm_time_op(mgfvm_ctx *x, int op, int level, int reps, double *ms_total, i
     CK(cudaEventElapsedTime(&ms, x->e0, x->e1));
     if (ms_total) *ms_total = ms;
     if (launches) *launches = (int)v.size() * reps;
+    return MGFVM_OK;
+}
+
+int mgfvm_profile_cycle(mgfvm_ctx *x, double *ms, int *kernel, int *level, int cap, int *n_out)
+{
+    RC(check_ctx(x));
+    RC(pull(x));
+    RC(ensure_hist(x, x->hc[0].ncyc + 1));
+    RC(set_controls(x, 0, 0.0));
+    const int n = (int)x->cyc.size();
+    std::vector<cudaEvent_t> ev(n + 1);
+    for (auto &e : ev) CK(cudaEventCreate(&e));
+    CK(cudaEventRecord(ev[0], x->stream));
+    for (int k = 0; k < n; ++k) {
+        cudaError_t e = launch_one(x->cyc[k], x->dc, x->sched, x->stream);
+        if (e != cudaSuccess) return mgfvm_fail(MGFVM_ECUDA, "profile launch %d: %s", k, cudaGetErrorString(e));
+        CK(cudaEventRecord(ev[k + 1], x->stream));
+    }
+    CK(cudaEventSynchronize(ev[n]));
+    x->launches += n;
+    for (int k = 0; k < n && k < cap; ++k) {
+        float t = 0;
+        CK(cudaEventElapsedTime(&t, ev[k], ev[k + 1]));
+        if (ms) ms[k] = t;
+        if (kernel) kernel[k] = x->cyc[k].kernel;
+        if (level) level[k] = x->cyc[k].ig;
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    if (n_out) *n_out = n;
     return MGFVM_OK;
 }
 

@@ -35,9 +35,10 @@ __global__ void k_init_fill(CaseDev *cs, const InitDev *in, int ig)
     if (j == 0) { u = P.bc[2][0]; v = P.bc[2][1]; p = P.bc[2][2]; sc = P.bc[2][3]; }
     if (j == ny - 1) { u = P.bc[3][0]; v = P.bc[3][1]; p = P.bc[3][2]; sc = P.bc[3][3]; }
     MGF(L, S_U)[t] = u; MGF(L, S_V)[t] = v; MGF(L, S_P)[t] = p; MGF(L, S_SC)[t] = sc;
-    const int zero_slots[] = {S_PP, S_SU, S_RS, S_RESU, S_RESV, S_RESSC, S_C, S_AW, S_AE, S_AS, S_AN,
-                              S_AP, S_SPU, S_SPV, S_SPSC, S_CX, S_CY, S_TMP, S_CU, S_CV, S_CP};
+    const int zero_slots[] = {S_PP, S_RS, S_RESU, S_RESV, S_RESSC, S_C, S_SPU, S_SPV, S_SPSC, S_CX, S_CY,
+                              S_TMP0, S_TMP1, S_TMP2, S_CU, S_CV, S_CP};
     for (int k = 0; k < (int)(sizeof zero_slots / sizeof zero_slots[0]); ++k) MGF(L, zero_slots[k])[t] = 0.0;
+    for (int s = S_CO; s < NSLOTS_LEVEL; ++s) MGF(L, s)[t] = 0.0;
     MGF(L, S_APU)[t] = 1.0e30;
     MGF(L, S_APV)[t] = 1.0e30;
     MGF(L, S_AREAX)[t] = L.dy;

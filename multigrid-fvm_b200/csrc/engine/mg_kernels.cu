@@ -1,14 +1,20 @@
 // mg_kernels.cu — the engine's kernels.
 //
-// Two execution shapes share the per-cell arithmetic of mg_cells.cuh:
+// Three execution shapes share the per-cell arithmetic of mg_cells.cuh:
 //   * grid-wide kernels: one thread per cell, blockIdx.y selects the case, so one
 //     launch advances one routine on one level of every case in the batch;
+//   * k_smooth: shared-memory tiles that run several smoother sweeps per launch on
+//     a tile plus a halo as deep as the sweeps (temporal blocking); it reads one
+//     buffer and writes the other, so no CTA ever loads a halo another CTA of the
+//     same launch has already updated;
 //   * k_tail: one CTA per case runs every coarse level of the V-cycle (down leg,
 //     restrictions, prolongations, up leg) with __syncthreads() between routines,
 //     because coarse grids are too small to fill the GPU and would otherwise be
 //     pure launch overhead.
-// All reductions are two-level and fixed-order (block tree, then the last block
-// over the per-block partials), so results are reproducible run to run.
+// Within a level visit the u, v and scalar equations depend only on the fluxes at
+// the start of the visit (solve_u/v/sc :696-737 read cx, cy from fluxes :678-694),
+// so they are assembled in one pass and smoothed in the same launches; p' follows.
+// All reductions are two-level and fixed-order, so results are reproducible.
 #include "mg_cells.cuh"
 #include "mg_kernels.cuh"
 
@@ -16,16 +22,16 @@ namespace mg {
 
 struct Dom { int i0, j0, wi, wj; };
 
+__device__ __forceinline__ Dom dom_all(const LevelDev &L) { return {0, 0, L.npx, L.npy}; }
 __device__ __forceinline__ Dom dom_interior(const LevelDev &L) { return {1, 1, L.npx - 2, L.npy - 2}; }
-__device__ __forceinline__ Dom dom_u(const LevelDev &L) { return {1, 1, L.npx - 3, L.npy - 2}; }
-__device__ __forceinline__ Dom dom_v(const LevelDev &L) { return {1, 1, L.npx - 2, L.npy - 3}; }
 __device__ __forceinline__ Dom dom_flux(const LevelDev &L) { return {0, 0, L.npx - 1, L.npy - 1}; }
 // sweep extent of each equation (solve_u/v/pprime/sc :701, :710, :725, :735)
 __device__ __forceinline__ Dom dom_eq(const LevelDev &L, int e)
 {
-    return e == 0 ? dom_u(L) : e == 1 ? dom_v(L) : dom_interior(L);
+    if (e == EQ_U) return {1, 1, L.npx - 3, L.npy - 2};
+    if (e == EQ_V) return {1, 1, L.npx - 2, L.npy - 3};
+    return dom_interior(L);
 }
-__device__ __forceinline__ int eq_slot(int e) { return e == 0 ? S_U : e == 1 ? S_V : e == 2 ? S_PP : S_SC; }
 
 __device__ __forceinline__ bool cell_at(const Dom &d, int t, int &i, int &j)
 {
@@ -33,6 +39,16 @@ __device__ __forceinline__ bool cell_at(const Dom &d, int t, int &i, int &j)
     j = d.j0 + t / d.wi;
     i = d.i0 + t % d.wi;
     return true;
+}
+
+__device__ __forceinline__ int nth_eq(int mask, int k)
+{
+    for (int e = 0; e < 4; ++e)
+        if ((mask >> e) & 1) {
+            if (k == 0) return e;
+            --k;
+        }
+    return -1;
 }
 
 // ------------------------------------------------------------ reductions
@@ -103,25 +119,17 @@ __global__ void __launch_bounds__(BLOCK) k_fluxes(CaseDev *cs, int ig, int mode)
     if (cell_at(dom_flux(L), t, i, j)) cell_fluxes(L, j * L.npx + i);
 }
 
-__global__ void __launch_bounds__(BLOCK) k_mom_u(CaseDev *cs, int ig, int mode)
+// Fused assembly over the padded array: fluxes, coefu+umom, coefv+vmom,
+// coefsc+scalar, the scalar outflow ghost (AsmBits).  LIVE recomputes the fluxes
+// from u, v (valid at the start of a level visit, before any of them changes).
+template <int LIVE>
+__global__ void __launch_bounds__(BLOCK) k_asm(CaseDev *cs, int ig, int mode, unsigned what)
 {
     CASE_PROLOGUE(mode);
     int i, j;
-    if (cell_at(dom_u(L), t, i, j)) cell_mom_u(L, C, i, j);
-}
-
-__global__ void __launch_bounds__(BLOCK) k_mom_v(CaseDev *cs, int ig, int mode)
-{
-    CASE_PROLOGUE(mode);
-    int i, j;
-    if (cell_at(dom_v(L), t, i, j)) cell_mom_v(L, C, i, j);
-}
-
-__global__ void __launch_bounds__(BLOCK) k_sc(CaseDev *cs, int ig, int mode)
-{
-    CASE_PROLOGUE(mode);
-    int i, j;
-    if (cell_at(dom_interior(L), t, i, j)) cell_sc(L, C, i, j);
+    if (!cell_at(dom_all(L), t, i, j)) return;
+    if (LIVE) cell_asm(L, C, FluxLive(L), i, j, what);
+    else cell_asm(L, C, FluxArrays(L), i, j, what);
 }
 
 __global__ void __launch_bounds__(BLOCK) k_update(CaseDev *cs, int ig, int mode)
@@ -166,81 +174,153 @@ __global__ void __launch_bounds__(BLOCK) k_pfix(CaseDev *cs, int ig, int mode, i
     else p[L.pdst[t]] = p[L.psrc[t]];
 }
 
-// pbound :1179-1210 — one block per case
-__global__ void __launch_bounds__(BLOCK) k_periodic(CaseDev *cs, int ig, int mode)
+// pbound :1179-1210 then outflow :1211-1228 (bits: 1 periodic, 2 outflow of u, v, p,
+// 4 the scalar ghost too) — one block per case.
+__device__ __forceinline__ void bound_block(const CaseDev &C, const LevelDev &L, int bits)
+{
+    if ((bits & 1) && C.ibc_xm == 3) {
+        for (int j = 1 + threadIdx.x; j < L.npy - 1; j += blockDim.x) row_periodic_x(L, j);
+        __syncthreads();
+    }
+    if ((bits & 1) && C.ibc_ym == 3) {
+        if (threadIdx.x == 0) line_periodic_y(L);
+        __syncthreads();
+    }
+    if ((bits & 2) && C.ibc_xp == 4) {
+        for (int j = threadIdx.x; j < L.npy; j += blockDim.x) row_outflow(L, j, (bits & 4) != 0);
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(BLOCK) k_bound(CaseDev *cs, int ig, int mode, int bits)
 {
     CaseDev &C = cs[blockIdx.y];
     if (!case_active(C, ig, mode)) return;
+    bound_block(C, C.lv[ig], bits);
+}
+
+// Temporal-blocked smoother.  blockIdx.z picks an equation of `mask`, blockIdx.x a
+// TILE_X x TILE_Y tile of its sweep domain.  The CTA loads the tile plus a halo of
+// `nu` cells (clipped at the domain's boundary ring) and the equation's
+// coefficients into shared memory, runs `nu` units — half-sweeps of red-black
+// Gauss-Seidel (colour of global unit u0+h-1: even = red) or Jacobi sweeps — each on
+// a window one cell narrower on every cut side, and writes the tile (plus the
+// boundary ring where the tile touches it) to the other buffer: dir 0 reads the
+// field and writes the equation's ping-pong buffer, dir 1 the reverse.  Every cell
+// update is the reference's formula on the same neighbour values, so the result is
+// bit-identical to sweeping the whole level unit by unit.
+template <int ISOLVE>
+__global__ void __launch_bounds__(SMOOTH_BLOCK) k_smooth(CaseDev *cs, int ig, int mode, int mask, int u0, int nu,
+                                                         int dir)
+{
+    extern __shared__ double sm[];
+    CaseDev &C = cs[blockIdx.y];
+    if (!case_active(C, ig, mode)) return;
+    const int e = nth_eq(mask, blockIdx.z);
     const LevelDev &L = C.lv[ig];
-    if (C.ibc_xm == 3)
-        for (int j = 1 + threadIdx.x; j < L.npy - 1; j += blockDim.x) row_periodic_x(L, j);
+    const Dom d = dom_eq(L, e);
+    if (d.wi <= 0 || d.wj <= 0) return;
+    const int tx_n = (d.wi + TILE_X - 1) / TILE_X, ty_n = (d.wj + TILE_Y - 1) / TILE_Y;
+    if ((int)blockIdx.x >= tx_n * ty_n) return;
+    const int tx = blockIdx.x % tx_n, ty = blockIdx.x / tx_n;
+    const int dx1 = d.i0 + d.wi - 1, dy1 = d.j0 + d.wj - 1;
+    const int x0 = d.i0 + tx * TILE_X, y0 = d.j0 + ty * TILE_Y;
+    const int x1 = min(x0 + TILE_X - 1, dx1), y1 = min(y0 + TILE_Y - 1, dy1);
+    const int H = nu;
+    const int rx0 = max(x0 - H, d.i0 - 1), rx1 = min(x1 + H, dx1 + 1);
+    const int ry0 = max(y0 - H, d.j0 - 1), ry1 = min(y1 + H, dy1 + 1);
+    const int W = rx1 - rx0 + 1, R = (ry1 - ry0 + 1) * W;
+    const int npx = L.npx;
+    const int fs = e == EQ_U ? S_U : e == EQ_V ? S_V : e == EQ_PP ? S_PP : S_SC;
+    const int ts = eq_tmp(e);
+    const double *src = L.f[dir == 0 ? fs : ts];
+    double *dst = L.f[dir == 0 ? ts : fs];
+    double *sphi = sm, *saw = sm + R, *sae = saw + R, *sas = sae + R, *san = sas + R, *sap = san + R,
+           *ssu = sap + R, *sphi2 = ssu + R;
+    const double *gaw = L.f[co_slot(e, CK_AW)], *gae = L.f[co_slot(e, CK_AE)], *gas = L.f[co_slot(e, CK_AS)],
+                 *gan = L.f[co_slot(e, CK_AN)], *gap = L.f[co_slot(e, CK_AP)], *gsu = L.f[co_slot(e, CK_SU)];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const int Hr = ry1 - ry0 + 1;
+    for (int r = warp; r < Hr; r += nwarp) {                 // one warp per row of R
+        const double *srow = src + (size_t)(ry0 + r) * npx + rx0;
+        const size_t g0 = (size_t)(ry0 + r) * npx + rx0;
+        for (int c = lane; c < W; c += 32) {
+            const int k = r * W + c;
+            const double ph = srow[c];
+            sphi[k] = ph;
+            if (ISOLVE == MGFVM_JACOBI) sphi2[k] = ph;
+            saw[k] = gaw[g0 + c]; sae[k] = gae[g0 + c]; sas[k] = gas[g0 + c];
+            san[k] = gan[g0 + c]; sap[k] = gap[g0 + c]; ssu[k] = gsu[g0 + c];
+        }
+    }
     __syncthreads();
-    if (C.ibc_ym == 3 && threadIdx.x == 0) line_periodic_y(L);
+    for (int h = 1; h <= nu; ++h) {
+        const int wx0 = max(x0 - H + h, d.i0), wx1 = min(x1 + H - h, dx1);
+        const int wy0 = max(y0 - H + h, d.j0), wy1 = min(y1 + H - h, dy1);
+        if (ISOLVE == MGFVM_GAUSS_SEIDEL) {
+            const int colour = (u0 + h - 1) & 1;
+            for (int j = wy0 + warp; j <= wy1; j += nwarp) {
+                const int i0 = wx0 + ((((wx0 + j) & 1) != colour) ? 1 : 0);
+                for (int i = i0 + 2 * lane; i <= wx1; i += 64) {
+                    const int k = (j - ry0) * W + (i - rx0);
+                    sphi[k] = gs_value(saw[k], sae[k], sas[k], san[k], sap[k], ssu[k], sphi[k - 1], sphi[k + 1],
+                                       sphi[k - W], sphi[k + W]);
+                }
+            }
+        } else {
+            const double *cur = ((h - 1) & 1) ? sphi2 : sphi;
+            double *nxt = ((h - 1) & 1) ? sphi : sphi2;
+            for (int j = wy0 + warp; j <= wy1; j += nwarp)
+                for (int i = wx0 + lane; i <= wx1; i += 32) {
+                    const int k = (j - ry0) * W + (i - rx0);
+                    nxt[k] = jacobi_value(saw[k], sae[k], sas[k], san[k], sap[k], ssu[k], cur[k - 1], cur[k + 1],
+                                          cur[k - W], cur[k + W], cur[k]);
+                }
+        }
+        __syncthreads();
+    }
+    const double *res = (ISOLVE == MGFVM_JACOBI && (nu & 1)) ? sphi2 : sphi;
+    const int ox0 = x0 == d.i0 ? x0 - 1 : x0, ox1 = x1 == dx1 ? x1 + 1 : x1;
+    const int oy0 = y0 == d.j0 ? y0 - 1 : y0, oy1 = y1 == dy1 ? y1 + 1 : y1;
+    const int ow = ox1 - ox0 + 1, on = ow * (oy1 - oy0 + 1);
+    (void)on;
+    for (int j = oy0 + warp; j <= oy1; j += nwarp)
+        for (int i = ox0 + lane; i <= ox1; i += 32) dst[j * npx + i] = res[(j - ry0) * W + (i - rx0)];
 }
 
-// outflow :1211-1228
-__global__ void __launch_bounds__(BLOCK) k_outflow(CaseDev *cs, int ig, int mode)
+// After an odd number of smoothing launches the result sits in the ping-pong buffer.
+__global__ void __launch_bounds__(BLOCK) k_copy(CaseDev *cs, int ig, int mode, int mask)
 {
     CASE_PROLOGUE(mode);
-    if (C.ibc_xp != 4) return;
-    if (t < L.npy) row_outflow(L, t);
+    const int e = nth_eq(mask, blockIdx.z);
+    const int fs = e == EQ_U ? S_U : e == EQ_V ? S_V : e == EQ_PP ? S_PP : S_SC;
+    int i, j;
+    if (cell_at(dom_eq(L, e), t, i, j)) MGF(L, fs)[j * L.npx + i] = MGF(L, eq_tmp(e))[j * L.npx + i];
 }
 
-// One Jacobi sweep of equation e: sweep index `it` reads phi (even) or the
-// ping-pong buffer (odd); the first sweep also copies phi's ring into the buffer,
-// since later sweeps read it there (solver :1254-1292).
-__global__ void __launch_bounds__(BLOCK) k_jacobi(CaseDev *cs, int ig, int mode, int e, int it)
+// restv :1354-1389 on coarse level ig+1 and fluxes(fine) :216, one thread per fine cell
+__device__ __forceinline__ void cell_restv_fluxes(const LevelDev &F, const LevelDev &K, int i, int j)
 {
-    CASE_PROLOGUE(mode);
-    const Dom d = dom_eq(L, e);
-    double *phi = MGF(L, eq_slot(e)), *tmp = MGF(L, S_TMP);
-    const double *cur = (it & 1) ? tmp : phi;
-    double *nxt = (it & 1) ? phi : tmp;
-    if (it == 0) {
-        const Dom x = {d.i0 - 1, d.j0 - 1, d.wi + 2, d.wj + 2};
-        int i, j;
-        if (!cell_at(x, t, i, j)) return;
-        const int q = j * L.npx + i;
-        if (i == x.i0 || i == x.i0 + x.wi - 1 || j == x.j0 || j == x.j0 + x.wj - 1) tmp[q] = phi[q];
-        else cell_jacobi(L, cur, nxt, q);
-    } else {
-        int i, j;
-        if (cell_at(d, t, i, j)) cell_jacobi(L, cur, nxt, j * L.npx + i);
+    if (i <= F.npx - 2 && j <= F.npy - 2) cell_fluxes(F, j * F.npx + i);
+    if (((i | j) & 1) == 0) {
+        const int ic = i >> 1, jc = j >> 1;
+        if (ic >= 1 && jc >= 1 && ic <= K.npx - 2 && jc <= K.npy - 2) cell_restv(F, K, ic, jc);
     }
 }
 
-// After an odd number of sweeps the result sits in the buffer: copy it back.
-__global__ void __launch_bounds__(BLOCK) k_jacobi_copyback(CaseDev *cs, int ig, int mode, int e)
+// restru/restrv/restrsc :1474-1740 and fluxes(coarse) :215, one thread per coarse cell
+__device__ __forceinline__ void cell_restrict_fluxes(const LevelDev &F, const LevelDev &K, const CaseDev &C,
+                                                     int ic, int jc)
+{
+    if (ic <= K.npx - 2 && jc <= K.npy - 2) cell_fluxes(K, jc * K.npx + ic);
+    if (ic >= 1 && jc >= 1 && ic <= K.npx - 2 && jc <= K.npy - 2) cell_restrict(F, K, C, ic, jc);
+}
+
+__global__ void __launch_bounds__(BLOCK) k_restv_fluxes(CaseDev *cs, int ig, int mode)
 {
     CASE_PROLOGUE(mode);
     int i, j;
-    if (cell_at(dom_eq(L, e), t, i, j)) {
-        const int q = j * L.npx + i;
-        MGF(L, eq_slot(e))[q] = MGF(L, S_TMP)[q];
-    }
-}
-
-// One colour of a red-black Gauss-Seidel sweep (solvergs :1306-1350):
-// colour 0 = (i+j) even, 1 = odd; threads map to cells of that colour only.
-__global__ void __launch_bounds__(BLOCK) k_gs(CaseDev *cs, int ig, int mode, int e, int colour)
-{
-    CASE_PROLOGUE(mode);
-    const Dom d = dom_eq(L, e);
-    const int wr = (d.wi + 1) >> 1;
-    if (t >= wr * d.wj) return;
-    const int j = d.j0 + t / wr, k = t % wr;
-    const int i = d.i0 + (((d.i0 + j) & 1) != colour ? 1 : 0) + 2 * k;
-    if (i > d.i0 + d.wi - 1) return;
-    cell_gs(L, MGF(L, eq_slot(e)), j * L.npx + i);
-}
-
-// restv on coarse level ig+1 from fine level ig
-__global__ void __launch_bounds__(BLOCK) k_restv(CaseDev *cs, int ig, int mode)
-{
-    CASE_PROLOGUE(mode);
-    const LevelDev &K = C.lv[ig + 1];
-    int i, j;
-    if (cell_at(dom_interior(K), t, i, j)) cell_restv(L, K, i, j);
+    if (cell_at(dom_all(L), t, i, j)) cell_restv_fluxes(L, C.lv[ig + 1], i, j);
 }
 
 __global__ void __launch_bounds__(BLOCK) k_restrict(CaseDev *cs, int ig, int mode)
@@ -248,7 +328,7 @@ __global__ void __launch_bounds__(BLOCK) k_restrict(CaseDev *cs, int ig, int mod
     CASE_PROLOGUE(mode);
     const LevelDev &K = C.lv[ig + 1];
     int i, j;
-    if (cell_at(dom_interior(K), t, i, j)) cell_restrict(L, K, C, i, j);
+    if (cell_at(dom_all(K), t, i, j)) cell_restrict_fluxes(L, K, C, i, j);
 }
 
 __global__ void __launch_bounds__(BLOCK) k_prol_corr(CaseDev *cs, int ig, int mode)
@@ -287,7 +367,7 @@ __global__ void __launch_bounds__(BLOCK) k_endcycle(CaseDev *cs)
     int i, j;
     if (cell_at(d, t, i, j)) {
         const int q = j * L.npx + i;
-        const int cur[4] = {S_U, S_V, S_SC, S_P}, prv[4] = {S_PREV_U, S_PREV_V, S_PREV_SC, S_PREV_P};
+        const int cur[3] = {S_U, S_V, S_SC}, prv[3] = {S_PREV_U, S_PREV_V, S_PREV_SC};
 #pragma unroll
         for (int f = 0; f < 3; ++f) {
             double x = MGF(L, cur[f])[q], y = MGF(L, prv[f])[q], dd = x - y;
@@ -347,55 +427,144 @@ __device__ __forceinline__ void for_cells(const Dom &d, F f)
     for (int t = threadIdx.x; t < n; t += blockDim.x) f(d.i0 + t % d.wi, d.j0 + t / d.wi);
 }
 
-__device__ void tail_smooth(const LevelDev &L, int e, const Sched &S)
+// Smooth the equations of `mask` on one level, in place in global memory, every
+// equation's unit h in the same phase.
+__device__ void tail_smooth_global(const LevelDev &L, const int *eqs, int ne, int nsw, int isolve)
 {
-    const Dom d = dom_eq(L, e);
-    double *phi = MGF(L, eq_slot(e)), *tmp = MGF(L, S_TMP);
-    const int nsw = e == 2 ? S.nswpp : S.nswpm;
-    if (S.isolve == MGFVM_JACOBI) {
-        {
+    if (isolve == MGFVM_JACOBI) {
+        for (int k = 0; k < ne; ++k) {
+            const int e = eqs[k];
+            const Dom d = dom_eq(L, e);
             const Dom x = {d.i0 - 1, d.j0 - 1, d.wi + 2, d.wj + 2};
+            double *phi = MGF(L, eq_field(e)), *tmp = MGF(L, eq_tmp(e));
             for_cells(x, [&](int i, int j) {
                 if (i == x.i0 || i == x.i0 + x.wi - 1 || j == x.j0 || j == x.j0 + x.wj - 1)
                     tmp[j * L.npx + i] = phi[j * L.npx + i];
             });
         }
         for (int it = 0; it < nsw; ++it) {
-            const double *cur = (it & 1) ? tmp : phi;
-            double *nxt = (it & 1) ? phi : tmp;
-            for_cells(d, [&](int i, int j) { cell_jacobi(L, cur, nxt, j * L.npx + i); });
+            for (int k = 0; k < ne; ++k) {
+                const int e = eqs[k];
+                double *phi = MGF(L, eq_field(e)), *tmp = MGF(L, eq_tmp(e));
+                const double *cur = (it & 1) ? tmp : phi;
+                double *nxt = (it & 1) ? phi : tmp;
+                for_cells(dom_eq(L, e), [&](int i, int j) { cell_jacobi(L, e, cur, nxt, j * L.npx + i); });
+            }
             __syncthreads();
         }
         if (nsw & 1) {
-            for_cells(d, [&](int i, int j) { phi[j * L.npx + i] = tmp[j * L.npx + i]; });
+            for (int k = 0; k < ne; ++k) {
+                const int e = eqs[k];
+                double *phi = MGF(L, eq_field(e)), *tmp = MGF(L, eq_tmp(e));
+                for_cells(dom_eq(L, e), [&](int i, int j) { phi[j * L.npx + i] = tmp[j * L.npx + i]; });
+            }
             __syncthreads();
         }
-    } else if (S.isolve == MGFVM_GAUSS_SEIDEL) {
-        for (int it = 0; it < nsw; ++it)
-            for (int colour = 0; colour < 2; ++colour) {
+    } else if (isolve == MGFVM_GAUSS_SEIDEL) {
+        for (int h = 0; h < 2 * nsw; ++h) {
+            const int colour = h & 1;
+            for (int k = 0; k < ne; ++k) {
+                const int e = eqs[k];
+                const Dom d = dom_eq(L, e);
+                double *phi = MGF(L, eq_field(e));
                 const int wr = (d.wi + 1) >> 1, n = wr * d.wj;
                 for (int t = threadIdx.x; t < n; t += blockDim.x) {
-                    const int j = d.j0 + t / wr, k = t % wr;
-                    const int i = d.i0 + (((d.i0 + j) & 1) != colour ? 1 : 0) + 2 * k;
-                    if (i <= d.i0 + d.wi - 1) cell_gs(L, phi, j * L.npx + i);
+                    const int j = d.j0 + t / wr;
+                    const int i = d.i0 + (((d.i0 + j) & 1) != colour ? 1 : 0) + 2 * (t % wr);
+                    if (i <= d.i0 + d.wi - 1) cell_gs(L, e, phi, j * L.npx + i);
                 }
-                __syncthreads();
             }
+            __syncthreads();
+        }
+    }
+}
+
+// The same sweeps with each equation's field and coefficients staged in shared
+// memory for the whole level (indices as in global memory), as many equations at a
+// time as `sm_doubles` holds; results are the same bits, only the latency changes.
+__device__ void tail_smooth(const LevelDev &L, int mask, int nsw, int isolve, double *sm, int sm_doubles)
+{
+    int eqs[4], ne = 0;
+    for (int e = 0; e < 4; ++e)
+        if ((mask >> e) & 1) eqs[ne++] = e;
+    if (nsw <= 0 || (isolve != MGFVM_JACOBI && isolve != MGFVM_GAUSS_SEIDEL)) return;
+    const int n = L.npx * L.npy, npx = L.npx;
+    const int per = isolve == MGFVM_JACOBI ? 8 : 7;
+    int k = 0;
+    while (k < ne) {
+        int g = 0;
+        while (k + g < ne && (long long)(g + 1) * per * n <= sm_doubles) ++g;
+        if (g == 0) {
+            tail_smooth_global(L, eqs + k, 1, nsw, isolve);
+            ++k;
+            continue;
+        }
+        for (int m = 0; m < g; ++m) {
+            const int e = eqs[k + m];
+            double *b = sm + (size_t)m * per * n;
+            const double *phi = MGF(L, eq_field(e));
+            const double *cw = MGF(L, co_slot(e, CK_AW)), *ce = MGF(L, co_slot(e, CK_AE)),
+                         *cs_ = MGF(L, co_slot(e, CK_AS)), *cn = MGF(L, co_slot(e, CK_AN)),
+                         *cp = MGF(L, co_slot(e, CK_AP)), *cu = MGF(L, co_slot(e, CK_SU));
+            for (int q = threadIdx.x; q < n; q += blockDim.x) {
+                const double ph = phi[q];
+                b[q] = ph;
+                b[n + q] = cw[q]; b[2 * n + q] = ce[q]; b[3 * n + q] = cs_[q];
+                b[4 * n + q] = cn[q]; b[5 * n + q] = cp[q]; b[6 * n + q] = cu[q];
+                if (per == 8) b[7 * n + q] = ph;
+            }
+        }
+        __syncthreads();
+        const int units = isolve == MGFVM_GAUSS_SEIDEL ? 2 * nsw : nsw;
+        for (int h = 0; h < units; ++h) {
+            for (int m = 0; m < g; ++m) {
+                const int e = eqs[k + m];
+                const Dom d = dom_eq(L, e);
+                double *b = sm + (size_t)m * per * n;
+                const double *aw = b + n, *ae = b + 2 * n, *as = b + 3 * n, *an = b + 4 * n, *ap = b + 5 * n,
+                             *su = b + 6 * n;
+                if (isolve == MGFVM_GAUSS_SEIDEL) {
+                    const int colour = h & 1, wr = (d.wi + 1) >> 1, cnt = wr * d.wj;
+                    for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
+                        const int j = d.j0 + t / wr;
+                        const int i = d.i0 + (((d.i0 + j) & 1) != colour ? 1 : 0) + 2 * (t % wr);
+                        if (i > d.i0 + d.wi - 1) continue;
+                        const int q = j * npx + i;
+                        b[q] = gs_value(aw[q], ae[q], as[q], an[q], ap[q], su[q], b[q - 1], b[q + 1], b[q - npx],
+                                        b[q + npx]);
+                    }
+                } else {
+                    const double *cur = (h & 1) ? b + 7 * n : b;
+                    double *nxt = (h & 1) ? b : b + 7 * n;
+                    for_cells(d, [&](int i, int j) {
+                        const int q = j * npx + i;
+                        nxt[q] = jacobi_value(aw[q], ae[q], as[q], an[q], ap[q], su[q], cur[q - 1], cur[q + 1],
+                                              cur[q - npx], cur[q + npx], cur[q]);
+                    });
+                }
+            }
+            __syncthreads();
+        }
+        for (int m = 0; m < g; ++m) {
+            const int e = eqs[k + m];
+            const double *res = sm + (size_t)m * per * n + ((isolve == MGFVM_JACOBI && (units & 1)) ? 7 * n : 0);
+            double *phi = MGF(L, eq_field(e));
+            for_cells(dom_eq(L, e), [&](int i, int j) { phi[j * npx + i] = res[j * npx + i]; });
+        }
+        __syncthreads();
+        k += g;
     }
 }
 
 // One SIMPLE step on level ig (down leg :201-207, up leg :235-244).
-__device__ void tail_step(CaseDev &C, int ig, bool down, const Sched &S)
+__device__ void tail_step(CaseDev &C, int ig, bool down, const Sched &S, double *sm, int smd)
 {
     const LevelDev &L = C.lv[ig];
-    for_cells(dom_flux(L), [&](int i, int j) { cell_fluxes(L, j * L.npx + i); });
+    const FluxLive fl(L);
+    const unsigned what = A_FLUX | A_U | A_V | A_SC | (down ? A_SC_OUTFLOW : 0u);
+    for_cells(dom_all(L), [&](int i, int j) { cell_asm(L, C, fl, i, j, what); });
     __syncthreads();
-    for_cells(dom_u(L), [&](int i, int j) { cell_mom_u(L, C, i, j); });
-    __syncthreads();
-    tail_smooth(L, 0, S);
-    for_cells(dom_v(L), [&](int i, int j) { cell_mom_v(L, C, i, j); });
-    __syncthreads();
-    tail_smooth(L, 1, S);
+    tail_smooth(L, (1 << EQ_U) | (1 << EQ_V) | (1 << EQ_SC), S.nswpm, S.isolve, sm, smd);
     double acc[1] = {0.0};
     for_cells(dom_interior(L), [&](int i, int j) { acc[0] += cell_mass_coefp(L, C, i, j); });
     if (ig == 0 && down) {
@@ -403,7 +572,7 @@ __device__ void tail_step(CaseDev &C, int ig, bool down, const Sched &S)
         if (threadIdx.x == 0) C.last_err = acc[0];
     }
     __syncthreads();
-    tail_smooth(L, 2, S);
+    tail_smooth(L, 1 << EQ_PP, S.nswpp, S.isolve, sm, smd);
     for_cells(dom_interior(L), [&](int i, int j) { cell_update(L, C, j * L.npx + i); });
     __syncthreads();
     if (L.ncopy > 0) {
@@ -417,37 +586,15 @@ __device__ void tail_step(CaseDev &C, int ig, bool down, const Sched &S)
         }
         __syncthreads();
     }
-    if (C.ibc_xm == 3) {
-        for (int j = 1 + threadIdx.x; j < L.npy - 1; j += blockDim.x) row_periodic_x(L, j);
-        __syncthreads();
-    }
-    if (C.ibc_ym == 3) {
-        if (threadIdx.x == 0) line_periodic_y(L);
-        __syncthreads();
-    }
-    const bool outflow = C.ibc_xp == 4;
-    if (down && outflow) {
-        for (int j = threadIdx.x; j < L.npy; j += blockDim.x) row_outflow(L, j);
-        __syncthreads();
-    }
-    for_cells(dom_interior(L), [&](int i, int j) { cell_sc(L, C, i, j); });
-    __syncthreads();
-    tail_smooth(L, 3, S);
-    if (!down && outflow) {
-        for (int j = threadIdx.x; j < L.npy; j += blockDim.x) row_outflow(L, j);
-        __syncthreads();
-    }
+    bound_block(C, L, down ? 3 : 7);
 }
 
 __device__ void tail_restrict(CaseDev &C, int ig)
 {
     const LevelDev &F = C.lv[ig], &K = C.lv[ig + 1];
-    for_cells(dom_interior(K), [&](int i, int j) { cell_restv(F, K, i, j); });
+    for_cells(dom_all(F), [&](int i, int j) { cell_restv_fluxes(F, K, i, j); });
     __syncthreads();
-    for_cells(dom_flux(K), [&](int i, int j) { cell_fluxes(K, j * K.npx + i); });
-    for_cells(dom_flux(F), [&](int i, int j) { cell_fluxes(F, j * F.npx + i); });
-    __syncthreads();
-    for_cells(dom_interior(K), [&](int i, int j) { cell_restrict(F, K, C, i, j); });
+    for_cells(dom_all(K), [&](int i, int j) { cell_restrict_fluxes(F, K, C, i, j); });
     __syncthreads();
 }
 
@@ -462,43 +609,66 @@ __device__ void tail_prolong(CaseDev &C, int ig)
 
 // Every level at or below C.tail of one case (blockIdx.x): the down leg from
 // C.tail, the restrictions between those levels, and the up leg back to C.tail.
-__global__ void __launch_bounds__(TAIL_BLOCK, 1) k_tail(CaseDev *cs, Sched S)
+__global__ void __launch_bounds__(TAIL_BLOCK, 1) k_tail(CaseDev *cs, Sched S, int smem_doubles)
 {
+    extern __shared__ double tsm[];
     CaseDev &C = cs[blockIdx.x];
     if (C.done || C.tail >= C.ngrid) return;
     for (int ig = C.tail; ig < C.ngrid; ++ig) {
-        tail_step(C, ig, true, S);
+        tail_step(C, ig, true, S, tsm, smem_doubles);
         if (ig != C.ngrid - 1) tail_restrict(C, ig);
     }
     for (int ig = C.ngrid - 1; ig > C.tail; --ig) {
         tail_prolong(C, ig - 1);
-        if (ig != 1) tail_step(C, ig - 1, false, S);
+        if (ig != 1) tail_step(C, ig - 1, false, S, tsm, smem_doubles);
     }
 }
 
 // ------------------------------------------------------------- launcher
+int smooth_smem_bytes(int isolve, int units)
+{
+    const int w = TILE_X + 2 * units, h = TILE_Y + 2 * units;
+    return (isolve == MGFVM_JACOBI ? 8 : 7) * w * h * (int)sizeof(double);
+}
+
+cudaError_t configure_kernels()
+{
+    cudaError_t e = cudaFuncSetAttribute(k_smooth<MGFVM_JACOBI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         smooth_smem_bytes(MGFVM_JACOBI, MAX_UNITS));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_smooth<MGFVM_GAUSS_SEIDEL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 smooth_smem_bytes(MGFVM_GAUSS_SEIDEL, MAX_UNITS));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, TAIL_SMEM_MAX);
+    return e;
+}
+
 cudaError_t launch_one(const Launch &X, CaseDev *dc, const Sched &S, cudaStream_t st)
 {
     const dim3 g = X.grid;
     const int b = X.block;
     switch (X.kernel) {
     case K_FLUXES: k_fluxes<<<g, b, 0, st>>>(dc, X.ig, X.mode); break;
-    case K_MOM_U: k_mom_u<<<g, b, 0, st>>>(dc, X.ig, X.mode); break;
-    case K_MOM_V: k_mom_v<<<g, b, 0, st>>>(dc, X.ig, X.mode); break;
+    case K_ASM:
+        if (X.a1) k_asm<1><<<g, b, 0, st>>>(dc, X.ig, X.mode, (unsigned)X.a0);
+        else k_asm<0><<<g, b, 0, st>>>(dc, X.ig, X.mode, (unsigned)X.a0);
+        break;
     case K_MASS_COEFP: k_mass_coefp<<<g, b, 0, st>>>(dc, X.ig, X.mode, X.a0); break;
     case K_UPDATE: k_update<<<g, b, 0, st>>>(dc, X.ig, X.mode); break;
     case K_PFIX: k_pfix<<<g, b, 0, st>>>(dc, X.ig, X.mode, X.a0); break;
-    case K_PERIODIC: k_periodic<<<g, b, 0, st>>>(dc, X.ig, X.mode); break;
-    case K_OUTFLOW: k_outflow<<<g, b, 0, st>>>(dc, X.ig, X.mode); break;
-    case K_SC: k_sc<<<g, b, 0, st>>>(dc, X.ig, X.mode); break;
-    case K_JACOBI: k_jacobi<<<g, b, 0, st>>>(dc, X.ig, X.mode, X.a0, X.a1); break;
-    case K_JACOBI_COPYBACK: k_jacobi_copyback<<<g, b, 0, st>>>(dc, X.ig, X.mode, X.a0); break;
-    case K_GS: k_gs<<<g, b, 0, st>>>(dc, X.ig, X.mode, X.a0, X.a1); break;
-    case K_RESTV: k_restv<<<g, b, 0, st>>>(dc, X.ig, X.mode); break;
+    case K_BOUND: k_bound<<<g, b, 0, st>>>(dc, X.ig, X.mode, X.a0); break;
+    case K_SMOOTH:
+        if (S.isolve == MGFVM_JACOBI)
+            k_smooth<MGFVM_JACOBI><<<g, b, X.smem, st>>>(dc, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3);
+        else
+            k_smooth<MGFVM_GAUSS_SEIDEL><<<g, b, X.smem, st>>>(dc, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3);
+        break;
+    case K_COPY: k_copy<<<g, b, 0, st>>>(dc, X.ig, X.mode, X.a0); break;
+    case K_RESTV_FLUXES: k_restv_fluxes<<<g, b, 0, st>>>(dc, X.ig, X.mode); break;
     case K_RESTRICT: k_restrict<<<g, b, 0, st>>>(dc, X.ig, X.mode); break;
     case K_PROL_CORR: k_prol_corr<<<g, b, 0, st>>>(dc, X.ig, X.mode); break;
     case K_PROL_APPLY: k_prol_apply<<<g, b, 0, st>>>(dc, X.ig, X.mode); break;
-    case K_TAIL: k_tail<<<g, b, 0, st>>>(dc, S); break;
+    case K_TAIL: k_tail<<<g, b, X.smem, st>>>(dc, S, X.smem / (int)sizeof(double)); break;
     case K_ENDCYCLE: k_endcycle<<<g, b, 0, st>>>(dc); break;
     default: return cudaErrorInvalidValue;
     }
@@ -517,10 +687,8 @@ __global__ void __launch_bounds__(BLOCK) r_jacobi(const double *__restrict__ aw,
     if (wi <= 0 || wj <= 0 || t >= wi * wj) return;
     const int i = o + t % wi, j = o + t / wi, q = j * npx + i;
     if (first && (i == 0 || i == nx || j == 0 || j == ny)) { tmp[q] = phi[q]; return; }
-    const double wj1 = 1.0;
-    double nb = aw[q] * cur[q - 1] + ae[q] * cur[q + 1] + as[q] * cur[q - npx] + an[q] * cur[q + npx];
-    double g = (nb + su[q]) / (ap[q] + 1.0e-30);
-    nxt[q] = (1.0 - wj1) * cur[q] + wj1 * g;
+    nxt[q] = jacobi_value(aw[q], ae[q], as[q], an[q], ap[q], su[q], cur[q - 1], cur[q + 1], cur[q - npx],
+                          cur[q + npx], cur[q]);
 }
 
 __global__ void __launch_bounds__(BLOCK) r_copy(const double *src, double *dst, int npx, int nx, int ny)
@@ -543,8 +711,7 @@ __global__ void __launch_bounds__(BLOCK) r_gs(const double *__restrict__ aw, con
     const int i = 1 + (((1 + j) & 1) != colour ? 1 : 0) + 2 * k;
     if (i > nx - 1) return;
     const int q = j * npx + i;
-    double nb = aw[q] * phi[q - 1] + ae[q] * phi[q + 1] + as[q] * phi[q - npx] + an[q] * phi[q + npx];
-    phi[q] = (nb + su[q]) / ap[q];
+    phi[q] = gs_value(aw[q], ae[q], as[q], an[q], ap[q], su[q], phi[q - 1], phi[q + 1], phi[q - npx], phi[q + npx]);
 }
 
 __global__ void __launch_bounds__(BLOCK) r_masserror(const double *u, const double *v, const double *ax,

@@ -5,28 +5,44 @@
 
 namespace mg {
 
-// One kernel launch of the V-cycle schedule.
+// One kernel launch of a V-cycle (or single-op) schedule.
 enum KernelId {
-    K_FLUXES = 0, K_MOM_U, K_MOM_V, K_MASS_COEFP, K_UPDATE, K_PFIX, K_PERIODIC, K_OUTFLOW,
-    K_SC, K_JACOBI, K_JACOBI_COPYBACK, K_GS, K_RESTV, K_RESTRICT, K_PROL_CORR, K_PROL_APPLY,
+    K_FLUXES = 0,    // fluxes only (single-op)
+    K_ASM,           // fused assembly: a0 = AsmBits, a1 = 1: fluxes recomputed live
+    K_MASS_COEFP,    // a0 = reduce the mass error into CaseDev::last_err
+    K_UPDATE,
+    K_PFIX,          // a0 = phase (0 gather, 1 scatter, 2 both)
+    K_BOUND,         // a0 = bits: 1 periodic, 2 outflow u/v/p, 4 outflow sc
+    K_SMOOTH,        // tile smoother: a0 = eq mask, a1 = first unit, a2 = units, a3 = dir
+    K_COPY,          // copy equations' buffers back: a0 = eq mask
+    K_RESTV_FLUXES,  // restv + fine fluxes
+    K_RESTRICT,      // restr{u,v,sc} + coarse fluxes
+    K_PROL_CORR, K_PROL_APPLY,
     K_TAIL, K_ENDCYCLE, K_NKERNELS
 };
 
 struct Launch {
-    int kernel;     // KernelId
-    int ig;         // level (fine level for transfers)
-    int mode;       // enum Mode
-    int a0, a1, a2; // kernel-specific: equation, sweep/colour, flags
+    int kernel;
+    int ig;            // level (fine level for transfers)
+    int mode;          // enum Mode
+    int a0, a1, a2, a3;
     dim3 grid;
     int block;
+    int smem;
 };
 
 struct Sched {
     int isolve, nswpm, nswpp;
 };
 
-// Launch one schedule entry on `stream`; returns the CUDA error of the launch.
+// Shared-memory tile smoother geometry.
+constexpr int TILE_X = 32, TILE_Y = 32;
+constexpr int SMOOTH_BLOCK = 1024;
+constexpr int MAX_UNITS = 10;   // half-sweeps (GS) or sweeps (Jacobi) per launch
+int smooth_smem_bytes(int isolve, int units);
+
 cudaError_t launch_one(const Launch &L, CaseDev *dcases, const Sched &S, cudaStream_t stream);
+cudaError_t configure_kernels();
 
 // Kernels of the raw-pointer entry points.
 cudaError_t raw_jacobi(const double *aw, const double *ae, const double *as, const double *an,
@@ -42,5 +58,6 @@ size_t raw_masserror_blocks(int npx, int npy);
 
 constexpr int BLOCK = 256;
 constexpr int TAIL_BLOCK = 512;
+constexpr int TAIL_SMEM_MAX = 220 * 1024;   // dynamic shared memory of the coarse kernel (+ its static 256 B)
 
 }  // namespace mg

@@ -62,6 +62,7 @@ def lib() -> C.CDLL:
         "mgfvm_last_elapsed_ms": (C.c_int, [_vp, _dp]),
         "mgfvm_stream": (C.c_int, [_vp, C.POINTER(_vp)]),
         "mgfvm_time_op": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _dp, _ip]),
+        "mgfvm_profile_cycle": (C.c_int, [_vp, _dp, _ip, _ip, C.c_int, _ip]),
         "mgfvm_transfer_bytes": (C.c_int, [_vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
         "mgfvm_last_error": (C.c_char_p, []),
         "mgfvm_pattern_staggered": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,

@@ -178,6 +178,21 @@ class Solver:
         check(self._lib.mgfvm_time_op(self._h, op, level, reps, C.byref(ms), C.byref(n)))
         return ms.value, n.value
 
+    KERNELS = ["fluxes", "asm", "mass_coefp", "update", "pfix", "bound", "smooth", "copy", "restv_fluxes",
+               "restrict", "prol_corr", "prol_apply", "tail", "endcycle"]
+
+    def profile_cycle(self):
+        """One directly-launched V-cycle with an event after every kernel: a list of
+        (kernel name, level, milliseconds)."""
+        cap = 4096
+        ms = np.zeros(cap)
+        kid = np.zeros(cap, dtype=np.int32)
+        lvl = np.zeros(cap, dtype=np.int32)
+        n = C.c_int()
+        check(self._lib.mgfvm_profile_cycle(self._h, ms.ctypes.data_as(_dp), kid.ctypes.data_as(_ip),
+                                            lvl.ctypes.data_as(_ip), cap, C.byref(n)))
+        return [(self.KERNELS[kid[k]], int(lvl[k]), float(ms[k])) for k in range(min(n.value, cap))]
+
     @property
     def transfer_bytes(self) -> Tuple[int, int]:
         """(host->device, device->host) bytes copied by this context so far."""
