@@ -202,6 +202,15 @@ __device__ __forceinline__ void cell_sc(const LevelDev &L, const CaseDev &C, con
 // The three assemblies that depend only on the fluxes at the start of a level
 // visit, plus those fluxes, at cell (i, j) of the full padded array.
 enum AsmBits { A_FLUX = 1, A_U = 2, A_V = 4, A_SC = 8, A_SC_OUTFLOW = 16 };
+
+// The part of `what` thread slice z of 3 does when a launch spreads the assemblies
+// over blockIdx.z (slice 0: fluxes and u, 1: v, 2: scalar and its outflow ghost).
+__host__ __device__ __forceinline__ unsigned asm_slice(unsigned what, int z, int nz)
+{
+    if (nz <= 1) return what;
+    const unsigned part[3] = {A_FLUX | A_U, A_V, A_SC | A_SC_OUTFLOW};
+    return what & part[z];
+}
 template <class F>
 __device__ __forceinline__ void cell_asm(const LevelDev &L, const CaseDev &C, const F &fl, int i, int j,
                                          unsigned what)
@@ -358,37 +367,44 @@ __device__ __forceinline__ double resid_sc(const LevelDev &L, const F &fl, int i
     return r;
 }
 
-// FAS defects of all three transported equations at coarse cell (ic, jc):
-// restru :1546-1563, restrv :1722-1738, restrsc :1634-1647, each fine residual
-// evaluated where the reference's restriction stencil reads it.  Fine fluxes come
-// from the arrays fluxes(fine) filled; coarse fluxes are recomputed from the coarse
-// u, v that restv just wrote.
-__device__ __forceinline__ void cell_restrict(const LevelDev &F, const LevelDev &K, const CaseDev &C,
-                                              int ic, int jc)
+// Fine-level residuals of the three transported equations at fine cell (i, j) where
+// each is defined (restru :1494-1512, restrv :1670-1688, restrsc :1585-1600), stored
+// in the level's ping-pong buffers (free between smoothing calls): u in TMP0, v in
+// TMP1, sc in TMP2.  Fluxes are recomputed from the fine u, v (fluxes(fine) :216).
+__device__ __forceinline__ void cell_fine_residuals(const LevelDev &F, const CaseDev &C, int i, int j, int which)
 {
-    const FluxArrays ff(F);
+    const FluxLive ff(F);
+    const int nx = F.npx, ny = F.npy, q = j * nx + i;
+    const bool in = i >= 1 && j >= 1 && i <= nx - 2 && j <= ny - 2;
+    if (!in) return;
+    if (which == 0 && i <= nx - 3) MGF(F, S_TMP0)[q] = resid_u(F, C, ff, i, j, true);
+    if (which == 1 && j <= ny - 3) MGF(F, S_TMP1)[q] = resid_v(F, C, ff, i, j, true);
+    if (which == 2) MGF(F, S_TMP2)[q] = resid_sc(F, ff, i, j, true);
+}
+
+// FAS defects at coarse cell (ic, jc): restru :1546-1563 (which 0), restrv :1722-1738
+// (1), restrsc :1634-1647 (2), from the fine residuals above and the coarse
+// residual of the restricted state (coarse fluxes recomputed from the coarse u, v).
+__device__ __forceinline__ void cell_restrict(const LevelDev &F, const LevelDev &K, const CaseDev &C,
+                                              int ic, int jc, int which)
+{
     const FluxLive fk(K);
-    const int nxc = K.npx, nyc = K.npy, qc = jc * nxc + ic;
-    const int i = 2 * ic, j = 2 * jc;
-    if (ic <= nxc - 3) {
-        double r0 = resid_u(F, C, ff, i, j, true), r1 = resid_u(F, C, ff, i, j - 1, true);
-        double r2 = resid_u(F, C, ff, i - 1, j, true), r3 = resid_u(F, C, ff, i - 1, j - 1, true);
-        double r4 = resid_u(F, C, ff, i + 1, j, true), r5 = resid_u(F, C, ff, i + 1, j - 1, true);
+    const int nxf = F.npx, nxc = K.npx, nyc = K.npy, qc = jc * nxc + ic;
+    const int q = 2 * jc * nxf + 2 * ic;
+    if (which == 0 && ic <= nxc - 3) {
+        const double *rf = MGF(F, S_TMP0);
         double rc = resid_u(K, C, fk, ic, jc, false);
-        MGF(K, S_RESU)[qc] = (r0 + r1) + 0.5 * (r2 + r3 + r4 + r5) - rc;
+        MGF(K, S_RESU)[qc] = (rf[q] + rf[q - nxf]) + 0.5 * (rf[q - 1] + rf[q - 1 - nxf] + rf[q + 1] + rf[q + 1 - nxf]) - rc;
     }
-    if (jc <= nyc - 3) {
-        double r0 = resid_v(F, C, ff, i, j, true), r1 = resid_v(F, C, ff, i - 1, j, true);
-        double r2 = resid_v(F, C, ff, i, j - 1, true), r3 = resid_v(F, C, ff, i - 1, j - 1, true);
-        double r4 = resid_v(F, C, ff, i, j + 1, true), r5 = resid_v(F, C, ff, i - 1, j + 1, true);
+    if (which == 1 && jc <= nyc - 3) {
+        const double *rf = MGF(F, S_TMP1);
         double rc = resid_v(K, C, fk, ic, jc, false);
-        MGF(K, S_RESV)[qc] = (r0 + r1) + 0.5 * (r2 + r3 + r4 + r5) - rc;
+        MGF(K, S_RESV)[qc] = (rf[q] + rf[q - 1]) + 0.5 * (rf[q - nxf] + rf[q - nxf - 1] + rf[q + nxf] + rf[q + nxf - 1]) - rc;
     }
-    {
-        double r0 = resid_sc(F, ff, i, j, true), r1 = resid_sc(F, ff, i, j - 1, true);
-        double r2 = resid_sc(F, ff, i - 1, j, true), r3 = resid_sc(F, ff, i - 1, j - 1, true);
+    if (which == 2) {
+        const double *rf = MGF(F, S_TMP2);
         double rc = resid_sc(K, fk, ic, jc, false);
-        MGF(K, S_RESSC)[qc] = (r0 + r1 + r2 + r3) - rc;
+        MGF(K, S_RESSC)[qc] = (rf[q] + rf[q - nxf] + rf[q - 1] + rf[q - 1 - nxf]) - rc;
     }
 }
 

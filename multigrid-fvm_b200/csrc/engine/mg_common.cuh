@@ -60,25 +60,33 @@ struct LevelDev {
 enum CaseStatus { CASE_RUNNING = 0, CASE_CONVERGED_REF = 1, CASE_CONVERGED_FP = 2,
                   CASE_NONFINITE = 4 };
 
+// Read-only description of one case during a launch (the host rewrites it between
+// launches): physics, boundary codes, the level table and where histories and
+// reduction scratch live.  Kernels take it through a const __restrict__ pointer so
+// the level pointers can be cached instead of reloaded after every store.
 struct CaseDev {
     // physics and boundary codes shared by every level (Version-6-26-04.c:30-35)
     double relxm, relxp, sc_obs, dpdxm, dpdym, convergence;
     int ibc_xm, ibc_xp, ibc_ym, ibc_yp;
     int ngrid;
     int tail;           // first level run by the one-CTA coarse kernel (== ngrid: none)
-    int done;           // stop rule fired; every kernel skips this case
-    int status;         // enum CaseStatus bits
-    int ncyc;           // cycles recorded in the history
     int hist_cap;
-    int have_prev;      // level-0 state of a previous cycle is in S_PREV_*
     int stop_enabled;   // evaluate the stop rule at the end of every cycle
     double fp_tol;
-    double last_err;    // level-0 sum|div| of the current cycle
-    double shift_d, shift_p;  // last cycle's mean p change and mean p (shifted sums)
     double *hist_err, *hist_delta;
     double *partials;   // RED_STRIDE doubles per block, reduction scratch
     unsigned *counters; // [0] mass error, [1] end of cycle
     LevelDev lv[MAXLEV];
+};
+
+// The part of a case that kernels write.
+struct CaseState {
+    int done;           // stop rule fired; every kernel skips this case
+    int status;         // enum CaseStatus bits
+    int ncyc;           // cycles recorded in the history
+    int have_prev;      // level-0 state of a previous cycle is in S_PREV_*
+    double last_err;    // level-0 sum|div| of the current cycle
+    double shift_d, shift_p;  // last cycle's mean p change and mean p (shifted sums)
 };
 
 // ---------------------------------------------------------------- modes
@@ -110,9 +118,9 @@ __host__ __device__ __forceinline__ bool mode_active(const CaseDev &C, int ig, i
     }
 }
 
-__device__ __forceinline__ bool case_active(const CaseDev &C, int ig, int mode)
+__device__ __forceinline__ bool case_active(const CaseDev &C, const CaseState &S, int ig, int mode)
 {
-    return !C.done && mode_active(C, ig, mode);
+    return !S.done && mode_active(C, ig, mode);
 }
 
 }  // namespace mg

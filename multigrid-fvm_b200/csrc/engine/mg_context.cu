@@ -48,8 +48,10 @@ struct mgfvm_ctx {
     std::vector<std::vector<double>> profile;
     std::vector<mgfvm_obstacle_prog> progs;   // ncases * MAXLEV
     std::vector<CaseDev> hc;
+    std::vector<CaseState> hs;
     std::vector<InitDev> hinit;
     CaseDev *dc = nullptr;
+    CaseState *ds = nullptr;
     InitDev *dinit = nullptr;
     char *pool = nullptr;
     double *hist = nullptr;
@@ -97,15 +99,23 @@ struct Builder {
         return out->back();
     }
     long long cells(int ig) const { return ig < (int)x->maxcells.size() ? x->maxcells[ig] : 0; }
-    long long tiles(int ig) const
+    long long tiles(int ig, int tile) const
     {
         long long m = 0;
         for (const mgfvm_config &c : x->cfg)
             if (ig < c.ngrid) {
                 const long long w = npx_of(c, ig) - 2, h = npy_of(c, ig) - 2;
-                m = std::max(m, ((w + TILE_X - 1) / TILE_X) * ((h + TILE_Y - 1) / TILE_Y));
+                m = std::max(m, ((w + tile - 1) / tile) * ((h + tile - 1) / tile));
             }
         return std::max<long long>(m, 1);
+    }
+    // Smaller tiles shorten each CTA's chain of dependent half-sweeps; they pay off
+    // while the level's 32-wide tiles would not fill two CTAs per SM.
+    int tile_for(int ig) const
+    {
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, x->device);
+        return x->ncases * tiles(ig, 32) < sms / 8 ? 16 : 32;
     }
     // `nsw` sweeps of the equations in `mask`: the 2*nsw half-sweeps (Gauss-Seidel) or
     // nsw sweeps (Jacobi) go in an even number of tile launches of at most MAX_UNITS
@@ -115,16 +125,25 @@ struct Builder {
         const int isolve = x->sched.isolve;
         const int units = isolve == MGFVM_GAUSS_SEIDEL ? 2 * nsw : nsw;
         if (units <= 0 || (isolve != MGFVM_JACOBI && isolve != MGFVM_GAUSS_SEIDEL)) return;
+        if (cells(ig) <= LEVEL_SMEM_CELLS) {       // small level: one CTA per (case, equation)
+            Launch &L = add(K_SMOOTH_LEVEL, ig, mode, 0, mask, nsw);
+            L.grid = dim3(__builtin_popcount((unsigned)mask), x->ncases);
+            L.block = SMOOTH_BLOCK;
+            L.smem = (isolve == MGFVM_JACOBI ? 8 : 7) * (int)cells(ig) * (int)sizeof(double);
+            return;
+        }
         int chunks = (units + MAX_UNITS - 1) / MAX_UNITS;
         if ((chunks & 1) && units >= chunks + 1) ++chunks;
         const int neq = __builtin_popcount((unsigned)mask);
+        const int tile = tile_for(ig);
         int u0 = 0;
         for (int c = 0; c < chunks; ++c) {
             const int nu = units / chunks + (c < units % chunks ? 1 : 0);
             Launch &L = add(K_SMOOTH, ig, mode, 0, mask, u0, nu, c & 1);
-            L.grid = dim3((unsigned)tiles(ig), x->ncases, neq);
+            L.a4 = tile;
+            L.grid = dim3((unsigned)tiles(ig, tile), x->ncases, neq);
             L.block = SMOOTH_BLOCK;
-            L.smem = smooth_smem_bytes(isolve, nu);
+            L.smem = smooth_smem_bytes(isolve, nu, tile);
             u0 += nu;
         }
         if (chunks & 1) {
@@ -155,29 +174,49 @@ struct Builder {
         Launch &L = add(K_BOUND, ig, mode, 1, bits);
         L.grid = dim3(1, x->ncases);
     }
-    void solve_pp(int ig, int mode, bool reduce)
+    // Can outflow run inside update on this level?  Not if pbound (periodic) or the
+    // obstacle pressure copy sits between them on the outlet columns for any case.
+    bool outflow_fusable(int ig, int mode) const
+    {
+        for (int c = 0; c < x->ncases; ++c) {
+            const CaseDev &C = x->hc[c];
+            if (!mode_active(C, ig, mode)) continue;
+            if (C.ibc_xm == 3 || C.ibc_ym == 3) return false;
+            if (x->progs[(size_t)c * MAXLEV + ig].touches_outlet) return false;
+        }
+        return true;
+    }
+    // returns the update's fuse bits (0: outflow still to do)
+    int solve_pp(int ig, int mode, bool reduce, int fuse)
     {
         add(K_MASS_COEFP, ig, mode, cells(ig), reduce ? 1 : 0);
         smooth(ig, mode, 1 << EQ_PP, x->sched.nswpp);
-        add(K_UPDATE, ig, mode, cells(ig));
+        add(K_UPDATE, ig, mode, cells(ig) + 2, fuse);
         pfix(ig, mode);
+        return fuse;
     }
     // One SIMPLE step (down leg :201-207, up leg :235-244).  u, v and sc depend only
     // on the visit-start fluxes, so they are assembled together and smoothed in the
     // same launches; the scalar's outflow ghost moves with its equation.
-    void step(int ig, int mode, bool down, bool reduce)
+    static int asm_bits(bool down) { return A_FLUX | A_U | A_V | A_SC | (down ? A_SC_OUTFLOW : 0); }
+    void step(int ig, int mode, bool down, bool reduce, bool asm_done = false)
     {
-        const int what = A_FLUX | A_U | A_V | A_SC | (down ? A_SC_OUTFLOW : 0);
-        add(K_ASM, ig, mode, cells(ig), what, 1);
+        if (!asm_done) {
+            Launch &L = add(K_ASM, ig, mode, cells(ig), asm_bits(down), 1);
+            L.grid.z = 3;                       // one thread per (cell, equation)
+        }
         smooth(ig, mode, (1 << EQ_U) | (1 << EQ_V) | (1 << EQ_SC), x->sched.nswpm);
-        solve_pp(ig, mode, reduce);
-        bound(ig, mode, down ? 3 : 7);
+        const int fuse = outflow_fusable(ig, mode) ? (down ? 1 : 3) : 0;
+        solve_pp(ig, mode, reduce, fuse);
+        if (!fuse) bound(ig, mode, down ? 3 : 7);
     }
     // :211-220
-    void restrict_(int ig, int mode_f)
+    // `coarse_asm`: also run the coarse level's down-leg assembly (see k_restrict)
+    void restrict_(int ig, int mode_f, bool coarse_asm = false)
     {
-        add(K_RESTV_FLUXES, ig, mode_f, cells(ig));
-        add(K_RESTRICT, ig, mode_f, cells(ig + 1));
+        add(K_RESTV_FLUXES, ig, mode_f, cells(ig)).grid.z = 3;
+        Launch &L = add(K_RESTRICT, ig, mode_f, cells(ig + 1), coarse_asm ? asm_bits(true) : 0);
+        L.grid.z = 3;                           // one thread per (coarse cell, equation)
     }
     // :230-233
     void prolong(int ig, int mode)
@@ -187,9 +226,14 @@ struct Builder {
     }
     void cycle()
     {
+        bool asm_done = false;
         for (int ig = 0; ig < x->maxng; ++ig) {
-            if (any(ig, M_DOWN)) step(ig, M_DOWN, true, ig == 0);
-            if (any(ig, M_RESTRICT)) restrict_(ig, M_RESTRICT);
+            if (any(ig, M_DOWN)) step(ig, M_DOWN, true, ig == 0, asm_done);
+            asm_done = false;
+            if (any(ig, M_RESTRICT)) {
+                asm_done = any(ig + 1, M_DOWN);
+                restrict_(ig, M_RESTRICT, asm_done);
+            }
         }
         bool tail = false;
         for (const CaseDev &C : x->hc) tail |= C.tail < C.ngrid;
@@ -212,6 +256,14 @@ struct Builder {
             prolong(ig - 1, M_PROLONG);
             if (ig != 1) step(ig - 1, M_UP, false, false);
         }
+        // the final prolongation into level 0 can carry the end-of-cycle norms when
+        // every case reaches level 0 through it
+        bool fuse_end = !out->empty() && out->back().kernel == K_PROL_APPLY && out->back().ig == 0;
+        for (const CaseDev &C : x->hc) fuse_end &= C.ngrid >= 2 && C.tail >= 1;
+        if (fuse_end) {
+            out->back().kernel = K_PROL_APPLY_END;
+            return;
+        }
         Launch L{};
         L.kernel = K_ENDCYCLE;
         long long n0 = 0;
@@ -233,7 +285,7 @@ struct Builder {
             add(K_ASM, ig, M_OP, cells(ig), A_V, 0);
             smooth(ig, M_OP, 1 << EQ_V, x->sched.nswpm);
             break;
-        case MGFVM_OP_SOLVE_PP: solve_pp(ig, M_OP, true); break;
+        case MGFVM_OP_SOLVE_PP: solve_pp(ig, M_OP, true, 0); break;
         case MGFVM_OP_PBOUND: bound(ig, M_OP, 1); break;
         case MGFVM_OP_OUTFLOW: bound(ig, M_OP, 6); break;
         case MGFVM_OP_SOLVE_SC:
@@ -300,7 +352,7 @@ int field_slot(int f, int eq)
 int run_list(mgfvm_ctx *x, const std::vector<Launch> &v)
 {
     for (const Launch &L : v) {
-        cudaError_t e = launch_one(L, x->dc, x->sched, x->stream);
+        cudaError_t e = launch_one(L, x->dc, x->ds, x->sched, x->stream);
         if (e != cudaSuccess)
             return mgfvm_fail(MGFVM_ECUDA, "kernel %d at level %d failed to launch: %s", L.kernel, L.ig,
                               cudaGetErrorString(e));
@@ -312,15 +364,16 @@ int run_list(mgfvm_ctx *x, const std::vector<Launch> &v)
 int pull(mgfvm_ctx *x)
 {
     CK(cudaStreamSynchronize(x->stream));
-    CK(cudaMemcpy(x->hc.data(), x->dc, sizeof(CaseDev) * x->ncases, cudaMemcpyDeviceToHost));
-    x->d2h += (long long)sizeof(CaseDev) * x->ncases;
+    CK(cudaMemcpy(x->hs.data(), x->ds, sizeof(CaseState) * x->ncases, cudaMemcpyDeviceToHost));
+    x->d2h += (long long)sizeof(CaseState) * x->ncases;
     return MGFVM_OK;
 }
 
 int push(mgfvm_ctx *x)
 {
     CK(cudaMemcpy(x->dc, x->hc.data(), sizeof(CaseDev) * x->ncases, cudaMemcpyHostToDevice));
-    x->h2d += (long long)sizeof(CaseDev) * x->ncases;
+    CK(cudaMemcpy(x->ds, x->hs.data(), sizeof(CaseState) * x->ncases, cudaMemcpyHostToDevice));
+    x->h2d += (long long)(sizeof(CaseDev) + sizeof(CaseState)) * x->ncases;
     return MGFVM_OK;
 }
 
@@ -352,7 +405,7 @@ int build_graph(mgfvm_ctx *x)
     if (x->gexec) return MGFVM_OK;
     CK(cudaStreamBeginCapture(x->stream, cudaStreamCaptureModeThreadLocal));
     for (const Launch &L : x->cyc) {
-        cudaError_t e = launch_one(L, x->dc, x->sched, x->stream);
+        cudaError_t e = launch_one(L, x->dc, x->ds, x->sched, x->stream);
         if (e != cudaSuccess) {
             cudaGraph_t g;
             cudaStreamEndCapture(x->stream, &g);
@@ -382,10 +435,10 @@ int set_controls(mgfvm_ctx *x, int stop, double fp_tol)
 {
     RC(pull(x));
     for (CaseDev &C : x->hc) {
-        C.done = 0;
         C.stop_enabled = stop;
         C.fp_tol = fp_tol;
     }
+    for (CaseState &S : x->hs) S.done = 0;
     return push(x);
 }
 
@@ -393,9 +446,8 @@ int init_state(mgfvm_ctx *x, int only_case)
 {
     for (int c = 0; c < x->ncases; ++c) {
         if (only_case >= 0 && c != only_case) continue;
-        CaseDev &C = x->hc[c];
-        C.done = 0; C.status = 0; C.ncyc = 0; C.have_prev = 0; C.stop_enabled = 0;
-        C.last_err = 0.0; C.shift_d = 0.0; C.shift_p = 0.0;
+        x->hs[c] = CaseState{};
+        x->hc[c].stop_enabled = 0;
     }
     RC(push(x));
     int max_obs = 0, max_npy = 0;
@@ -448,6 +500,7 @@ void destroy_all(mgfvm_ctx *x)
     if (x->dprofile) cudaFree(x->dprofile);
     if (x->dobs) cudaFree(x->dobs);
     if (x->dc) cudaFree(x->dc);
+    if (x->ds) cudaFree(x->ds);
     if (x->dinit) cudaFree(x->dinit);
     if (x->hflags) cudaFreeHost(x->hflags);
     if (x->e0) cudaEventDestroy(x->e0);
@@ -521,6 +574,7 @@ int create_impl(const mgfvm_config *cases, int ncases, const mgfvm_options *opt_
 
     // pool layout: pass 0 sizes, pass 1 assigns
     x->hc.assign(ncases, CaseDev{});
+    x->hs.assign(ncases, CaseState{});
     std::vector<size_t> off_slots;
     size_t off = 0;
     auto take = [&](size_t bytes) { off = align_up(off, 256); size_t o = off; off += std::max<size_t>(bytes, 8); return o; };
@@ -544,7 +598,7 @@ int create_impl(const mgfvm_config *cases, int ncases, const mgfvm_options *opt_
             pend.push_back(p);
         }
         const long long n0 = (long long)(npx_of(g, 0) - 2) * (npy_of(g, 0) - 2);
-        part_off[c] = take((size_t)nblk(n0) * RED_STRIDE * sizeof(double));
+        part_off[c] = take((size_t)std::max(nblk(n0), 64) * RED_STRIDE * sizeof(double));
         cnt_off[c] = take(16 * sizeof(unsigned));
     }
     const size_t pool_bytes = align_up(off, 256);
@@ -636,6 +690,7 @@ int create_impl(const mgfvm_config *cases, int ncases, const mgfvm_options *opt_
         }
     }
     CK(cudaMalloc(&x->dc, sizeof(CaseDev) * ncases));
+    CK(cudaMalloc(&x->ds, sizeof(CaseState) * ncases));
     CK(cudaMalloc(&x->dinit, sizeof(InitDev) * ncases));
     RC(upload_profiles(x));
     // histories
@@ -703,7 +758,7 @@ int mgfvm_cycle(mgfvm_ctx *x, int ncycles)
     if (ncycles < 0) return mgfvm_fail(MGFVM_EINVAL, "negative cycle count");
     RC(pull(x));
     int need = 0;
-    for (const CaseDev &C : x->hc) need = std::max(need, C.ncyc + ncycles);
+    for (const CaseState &S : x->hs) need = std::max(need, S.ncyc + ncycles);
     RC(ensure_hist(x, need));
     RC(set_controls(x, 0, 0.0));
     CK(cudaEventRecord(x->e0, x->stream));
@@ -725,8 +780,8 @@ int mgfvm_solve(mgfvm_ctx *x, int max_cycles, double fp_tol, int *cycles_out)
     std::vector<int> start(x->ncases);
     int need = 0;
     for (int c = 0; c < x->ncases; ++c) {
-        start[c] = x->hc[c].ncyc;
-        need = std::max(need, x->hc[c].ncyc + max_cycles);
+        start[c] = x->hs[c].ncyc;
+        need = std::max(need, x->hs[c].ncyc + max_cycles);
     }
     RC(ensure_hist(x, need));
     RC(set_controls(x, 1, fp_tol));
@@ -736,7 +791,7 @@ int mgfvm_solve(mgfvm_ctx *x, int max_cycles, double fp_tol, int *cycles_out)
         const int n = std::min(x->opt.sync_every, max_cycles - run);
         RC(run_cycles(x, n));
         run += n;
-        CK(cudaMemcpy2DAsync(x->hflags, sizeof(int), &x->dc[0].done, sizeof(CaseDev), sizeof(int), x->ncases,
+        CK(cudaMemcpy2DAsync(x->hflags, sizeof(int), &x->ds[0].done, sizeof(CaseState), sizeof(int), x->ncases,
                              cudaMemcpyDeviceToHost, x->stream));
         CK(cudaStreamSynchronize(x->stream));
         x->d2h += (long long)sizeof(int) * x->ncases;
@@ -752,8 +807,8 @@ int mgfvm_solve(mgfvm_ctx *x, int max_cycles, double fp_tol, int *cycles_out)
     RC(pull(x));
     int nonfinite = 0;
     for (int c = 0; c < x->ncases; ++c) {
-        if (cycles_out) cycles_out[c] = x->hc[c].ncyc - start[c];
-        if (x->hc[c].status & CASE_NONFINITE) nonfinite = 1;
+        if (cycles_out) cycles_out[c] = x->hs[c].ncyc - start[c];
+        if (x->hs[c].status & CASE_NONFINITE) nonfinite = 1;
     }
     if (nonfinite) return mgfvm_fail(MGFVM_ENONFINITE, "a case's mass error or fixed-point change became NaN/Inf");
     return MGFVM_OK;
@@ -764,8 +819,8 @@ int mgfvm_history(mgfvm_ctx *x, int icase, double *err, double *delta, int cap, 
     RC(check_ctx(x));
     if (icase < 0 || icase >= x->ncases) return mgfvm_fail(MGFVM_EINVAL, "case %d out of range", icase);
     RC(pull(x));
-    const int n = std::min(x->hc[icase].ncyc, x->hist_cap);
-    if (n_out) *n_out = x->hc[icase].ncyc;
+    const int n = std::min(x->hs[icase].ncyc, x->hist_cap);
+    if (n_out) *n_out = x->hs[icase].ncyc;
     const int m = std::min(n, std::max(cap, 0));
     if (err && m) CK(cudaMemcpy(err, x->hc[icase].hist_err, sizeof(double) * m, cudaMemcpyDeviceToHost));
     if (delta && m) CK(cudaMemcpy(delta, x->hc[icase].hist_delta, sizeof(double) * m, cudaMemcpyDeviceToHost));
@@ -899,14 +954,14 @@ int mgfvm_profile_cycle(mgfvm_ctx *x, double *ms, int *kernel, int *level, int c
 {
     RC(check_ctx(x));
     RC(pull(x));
-    RC(ensure_hist(x, x->hc[0].ncyc + 1));
+    RC(ensure_hist(x, x->hs[0].ncyc + 1));
     RC(set_controls(x, 0, 0.0));
     const int n = (int)x->cyc.size();
     std::vector<cudaEvent_t> ev(n + 1);
     for (auto &e : ev) CK(cudaEventCreate(&e));
     CK(cudaEventRecord(ev[0], x->stream));
     for (int k = 0; k < n; ++k) {
-        cudaError_t e = launch_one(x->cyc[k], x->dc, x->sched, x->stream);
+        cudaError_t e = launch_one(x->cyc[k], x->dc, x->ds, x->sched, x->stream);
         if (e != cudaSuccess) return mgfvm_fail(MGFVM_ECUDA, "profile launch %d: %s", k, cudaGetErrorString(e));
         CK(cudaEventRecord(ev[k + 1], x->stream));
     }

@@ -18,9 +18,9 @@
 
 namespace mg {
 
-__global__ void k_init_fill(CaseDev *cs, const InitDev *in, int ig)
+__global__ void k_init_fill(const CaseDev *__restrict__ cs, const InitDev *in, int ig)
 {
-    CaseDev &C = cs[blockIdx.y];
+    const CaseDev &C = cs[blockIdx.y];
     if (ig >= C.ngrid) return;
     const InitDev &P = in[blockIdx.y];
     const LevelDev &L = C.lv[ig];
@@ -59,9 +59,9 @@ __device__ __forceinline__ void obstacle_range(const InitDev &P, int k, int ig, 
     r[3] = o[3] * fac;
 }
 
-__global__ void k_init_obstacles(CaseDev *cs, const InitDev *in, int ig)
+__global__ void k_init_obstacles(const CaseDev *__restrict__ cs, const InitDev *in, int ig)
 {
-    CaseDev &C = cs[blockIdx.y];
+    const CaseDev &C = cs[blockIdx.y];
     const InitDev &P = in[blockIdx.y];
     const int k = blockIdx.x;
     if (ig >= C.ngrid || ig >= P.ig_obs || k >= P.nobs) return;
@@ -83,9 +83,9 @@ __global__ void k_init_obstacles(CaseDev *cs, const InitDev *in, int ig)
     }
 }
 
-__global__ void k_init_ports(CaseDev *cs, const InitDev *in, int ig)
+__global__ void k_init_ports(const CaseDev *__restrict__ cs, const InitDev *in, int ig)
 {
-    CaseDev &C = cs[blockIdx.y];
+    const CaseDev &C = cs[blockIdx.y];
     const InitDev &P = in[blockIdx.y];
     if (ig >= C.ngrid) return;
     const LevelDev &L = C.lv[ig];
@@ -114,9 +114,9 @@ __global__ void k_init_ports(CaseDev *cs, const InitDev *in, int ig)
     }
 }
 
-__global__ void k_init_profile(CaseDev *cs, const InitDev *in)
+__global__ void k_init_profile(const CaseDev *__restrict__ cs, const InitDev *in)
 {
-    CaseDev &C = cs[blockIdx.y];
+    const CaseDev &C = cs[blockIdx.y];
     const InitDev &P = in[blockIdx.y];
     if (!P.profile || P.nprofile <= 0) return;
     const LevelDev &L = C.lv[0];
@@ -125,9 +125,9 @@ __global__ void k_init_profile(CaseDev *cs, const InitDev *in)
     MGF(L, S_U)[j * L.npx] = P.profile[j - 1];
 }
 
-__global__ void k_rest_geom(CaseDev *cs, int ig)
+__global__ void k_rest_geom(const CaseDev *__restrict__ cs, int ig)
 {
-    CaseDev &C = cs[blockIdx.y];
+    const CaseDev &C = cs[blockIdx.y];
     if (ig >= C.ngrid || ig < 1) return;
     const LevelDev &F = C.lv[ig - 1], &K = C.lv[ig];
     const int nxf = F.npx, nxc = K.npx, nyc = K.npy;

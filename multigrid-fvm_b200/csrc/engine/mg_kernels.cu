@@ -107,12 +107,13 @@ __device__ __forceinline__ void gather_partials(const double *partials, int nblo
 
 // ------------------------------------------------------ grid-wide kernels
 #define CASE_PROLOGUE(mode)                          \
-    CaseDev &C = cs[blockIdx.y];                     \
-    if (!case_active(C, ig, (mode))) return;         \
+    const CaseDev &C = cs[blockIdx.y];               \
+    CaseState &ST = st[blockIdx.y];                  \
+    if (!case_active(C, ST, ig, (mode))) return;     \
     const LevelDev &L = C.lv[ig];                    \
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
 
-__global__ void __launch_bounds__(BLOCK) k_fluxes(CaseDev *cs, int ig, int mode)
+__global__ void __launch_bounds__(BLOCK) k_fluxes(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode)
 {
     CASE_PROLOGUE(mode);
     int i, j;
@@ -123,24 +124,54 @@ __global__ void __launch_bounds__(BLOCK) k_fluxes(CaseDev *cs, int ig, int mode)
 // coefsc+scalar, the scalar outflow ghost (AsmBits).  LIVE recomputes the fluxes
 // from u, v (valid at the start of a level visit, before any of them changes).
 template <int LIVE>
-__global__ void __launch_bounds__(BLOCK) k_asm(CaseDev *cs, int ig, int mode, unsigned what)
+__global__ void __launch_bounds__(BLOCK) k_asm(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode, unsigned what)
 {
     CASE_PROLOGUE(mode);
     int i, j;
     if (!cell_at(dom_all(L), t, i, j)) return;
-    if (LIVE) cell_asm(L, C, FluxLive(L), i, j, what);
-    else cell_asm(L, C, FluxArrays(L), i, j, what);
+    const unsigned w = asm_slice(what, blockIdx.z, gridDim.z);
+    if (LIVE) cell_asm(L, C, FluxLive(L), i, j, w);
+    else cell_asm(L, C, FluxArrays(L), i, j, w);
 }
 
-__global__ void __launch_bounds__(BLOCK) k_update(CaseDev *cs, int ig, int mode)
+// update :1127-1152; with `fuse` (bit 1) also outflow :1211-1228 of u, v, p (bit 2:
+// and sc), legal when nothing between them in the reference (pbound, the obstacle
+// pressure copy) touches the outlet columns: the cell at i = npx-3 writes its new u
+// to both its face and the outlet face, the cell at i = npx-2 its new v and p to the
+// ghost column, and two extra threads copy the ghosts of the boundary rows.
+__global__ void __launch_bounds__(BLOCK) k_update(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode,
+                                                  int fuse)
 {
     CASE_PROLOGUE(mode);
+    const Dom d = dom_interior(L);
+    const int n = d.wi * d.wj, nx = L.npx;
+    const bool out = (fuse & 1) && C.ibc_xp == 4;
     int i, j;
-    if (cell_at(dom_interior(L), t, i, j)) cell_update(L, C, j * L.npx + i);
+    if (cell_at(d, t, i, j)) {
+        const int q = j * nx + i;
+        double *u = MGF(L, S_U), *v = MGF(L, S_V), *p = MGF(L, S_P);
+        const double *pp = MGF(L, S_PP);
+        const double ppref = 0.0, ppq = pp[q];
+        const double un = u[q] + MGF(L, S_AREAX)[q] * (ppq - pp[q + 1]) / MGF(L, S_APU)[q];
+        const double vn = v[q] + MGF(L, S_AREAY)[q] * (ppq - pp[q + nx]) / MGF(L, S_APV)[q];
+        const double pn = p[q] + C.relxp * (ppq - ppref);
+        if (!out || i != nx - 2) u[q] = un;
+        v[q] = vn;
+        p[q] = pn;
+        if (out && i == nx - 3) u[q + 1] = un;
+        if (out && i == nx - 2) {
+            v[q + 1] = vn;
+            p[q + 1] = pn;
+            if (fuse & 2) MGF(L, S_SC)[q + 1] = MGF(L, S_SC)[q];
+        }
+    } else if (out && t < n + 2) {
+        const int jb = t == n ? 0 : L.npy - 1;
+        row_outflow(L, jb, (fuse & 2) != 0);
+    }
 }
 
 // masserror + coefp; with `reduce`, sum|div| of this level lands in C.last_err.
-__global__ void __launch_bounds__(BLOCK) k_mass_coefp(CaseDev *cs, int ig, int mode, int reduce)
+__global__ void __launch_bounds__(BLOCK) k_mass_coefp(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode, int reduce)
 {
     CASE_PROLOGUE(mode);
     const Dom d = dom_interior(L);
@@ -155,7 +186,7 @@ __global__ void __launch_bounds__(BLOCK) k_mass_coefp(CaseDev *cs, int ig, int m
         double s[1];
         gather_partials<1>(C.partials, nb, s);
         if (threadIdx.x == 0) {
-            C.last_err = s[0];
+            ST.last_err = s[0];
             C.counters[0] = 0;
         }
     }
@@ -164,7 +195,7 @@ __global__ void __launch_bounds__(BLOCK) k_mass_coefp(CaseDev *cs, int ig, int m
 // update's obstacle pressure copy as a gather (obstacles.c): phase 0 reads every
 // source into pbuf, phase 1 writes them; phase 2 does both in one pass when no
 // source is also a destination.
-__global__ void __launch_bounds__(BLOCK) k_pfix(CaseDev *cs, int ig, int mode, int phase)
+__global__ void __launch_bounds__(BLOCK) k_pfix(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode, int phase)
 {
     CASE_PROLOGUE(mode);
     if (t >= L.ncopy) return;
@@ -192,15 +223,15 @@ __device__ __forceinline__ void bound_block(const CaseDev &C, const LevelDev &L,
     }
 }
 
-__global__ void __launch_bounds__(BLOCK) k_bound(CaseDev *cs, int ig, int mode, int bits)
+__global__ void __launch_bounds__(BLOCK) k_bound(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode, int bits)
 {
-    CaseDev &C = cs[blockIdx.y];
-    if (!case_active(C, ig, mode)) return;
+    const CaseDev &C = cs[blockIdx.y];
+    if (!case_active(C, st[blockIdx.y], ig, mode)) return;
     bound_block(C, C.lv[ig], bits);
 }
 
 // Temporal-blocked smoother.  blockIdx.z picks an equation of `mask`, blockIdx.x a
-// TILE_X x TILE_Y tile of its sweep domain.  The CTA loads the tile plus a halo of
+// tile x tile block of its sweep domain.  The CTA loads the tile plus a halo of
 // `nu` cells (clipped at the domain's boundary ring) and the equation's
 // coefficients into shared memory, runs `nu` units — half-sweeps of red-black
 // Gauss-Seidel (colour of global unit u0+h-1: even = red) or Jacobi sweeps — each on
@@ -210,22 +241,22 @@ __global__ void __launch_bounds__(BLOCK) k_bound(CaseDev *cs, int ig, int mode, 
 // update is the reference's formula on the same neighbour values, so the result is
 // bit-identical to sweeping the whole level unit by unit.
 template <int ISOLVE>
-__global__ void __launch_bounds__(SMOOTH_BLOCK) k_smooth(CaseDev *cs, int ig, int mode, int mask, int u0, int nu,
-                                                         int dir)
+__global__ void __launch_bounds__(SMOOTH_BLOCK) k_smooth(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode, int mask, int u0, int nu,
+                                                         int dir, int tile)
 {
     extern __shared__ double sm[];
-    CaseDev &C = cs[blockIdx.y];
-    if (!case_active(C, ig, mode)) return;
+    const CaseDev &C = cs[blockIdx.y];
+    if (!case_active(C, st[blockIdx.y], ig, mode)) return;
     const int e = nth_eq(mask, blockIdx.z);
     const LevelDev &L = C.lv[ig];
     const Dom d = dom_eq(L, e);
     if (d.wi <= 0 || d.wj <= 0) return;
-    const int tx_n = (d.wi + TILE_X - 1) / TILE_X, ty_n = (d.wj + TILE_Y - 1) / TILE_Y;
+    const int tx_n = (d.wi + tile - 1) / tile, ty_n = (d.wj + tile - 1) / tile;
     if ((int)blockIdx.x >= tx_n * ty_n) return;
     const int tx = blockIdx.x % tx_n, ty = blockIdx.x / tx_n;
     const int dx1 = d.i0 + d.wi - 1, dy1 = d.j0 + d.wj - 1;
-    const int x0 = d.i0 + tx * TILE_X, y0 = d.j0 + ty * TILE_Y;
-    const int x1 = min(x0 + TILE_X - 1, dx1), y1 = min(y0 + TILE_Y - 1, dy1);
+    const int x0 = d.i0 + tx * tile, y0 = d.j0 + ty * tile;
+    const int x1 = min(x0 + tile - 1, dx1), y1 = min(y0 + tile - 1, dy1);
     const int H = nu;
     const int rx0 = max(x0 - H, d.i0 - 1), rx1 = min(x1 + H, dx1 + 1);
     const int ry0 = max(y0 - H, d.j0 - 1), ry1 = min(y1 + H, dy1 + 1);
@@ -288,8 +319,23 @@ __global__ void __launch_bounds__(SMOOTH_BLOCK) k_smooth(CaseDev *cs, int ig, in
         for (int i = ox0 + lane; i <= ox1; i += 32) dst[j * npx + i] = res[(j - ry0) * W + (i - rx0)];
 }
 
+// Whole-level smoother for small levels: one CTA per (case, equation of `mask`)
+// stages the equation's field and coefficients for the entire level in shared
+// memory and runs every sweep there (no halo, no second buffer).
+__device__ void tail_smooth(const LevelDev &L, int mask, int nsw, int isolve, double *sm, int sm_doubles);
+
+__global__ void __launch_bounds__(SMOOTH_BLOCK) k_smooth_level(const CaseDev *__restrict__ cs, CaseState *st, int ig,
+                                                               int mode, int mask, int nsw, int isolve, int smd)
+{
+    extern __shared__ double sm[];
+    const CaseDev &C = cs[blockIdx.y];
+    if (!case_active(C, st[blockIdx.y], ig, mode)) return;
+    const int e = nth_eq(mask, blockIdx.x);
+    tail_smooth(C.lv[ig], 1 << e, nsw, isolve, sm, smd);
+}
+
 // After an odd number of smoothing launches the result sits in the ping-pong buffer.
-__global__ void __launch_bounds__(BLOCK) k_copy(CaseDev *cs, int ig, int mode, int mask)
+__global__ void __launch_bounds__(BLOCK) k_copy(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode, int mask)
 {
     CASE_PROLOGUE(mode);
     const int e = nth_eq(mask, blockIdx.z);
@@ -298,40 +344,67 @@ __global__ void __launch_bounds__(BLOCK) k_copy(CaseDev *cs, int ig, int mode, i
     if (cell_at(dom_eq(L, e), t, i, j)) MGF(L, fs)[j * L.npx + i] = MGF(L, eq_tmp(e))[j * L.npx + i];
 }
 
-// restv :1354-1389 on coarse level ig+1 and fluxes(fine) :216, one thread per fine cell
-__device__ __forceinline__ void cell_restv_fluxes(const LevelDev &F, const LevelDev &K, int i, int j)
+// restv :1354-1389 on coarse level ig+1, fluxes(fine) :216 and the fine residuals of
+// restr{u,v,sc}, one thread per (fine cell, slice `which` of 3)
+__device__ __forceinline__ void cell_restv_fluxes(const LevelDev &F, const LevelDev &K, const CaseDev &C, int i,
+                                                  int j, int which, int nwhich)
 {
-    if (i <= F.npx - 2 && j <= F.npy - 2) cell_fluxes(F, j * F.npx + i);
-    if (((i | j) & 1) == 0) {
-        const int ic = i >> 1, jc = j >> 1;
-        if (ic >= 1 && jc >= 1 && ic <= K.npx - 2 && jc <= K.npy - 2) cell_restv(F, K, ic, jc);
+    if (which == 0) {
+        if (i <= F.npx - 2 && j <= F.npy - 2) cell_fluxes(F, j * F.npx + i);
+        if (((i | j) & 1) == 0) {
+            const int ic = i >> 1, jc = j >> 1;
+            if (ic >= 1 && jc >= 1 && ic <= K.npx - 2 && jc <= K.npy - 2) cell_restv(F, K, ic, jc);
+        }
     }
+    for (int w = which; w < 3; w += nwhich) cell_fine_residuals(F, C, i, j, w);
 }
 
-// restru/restrv/restrsc :1474-1740 and fluxes(coarse) :215, one thread per coarse cell
+// restru/restrv/restrsc :1474-1740 and fluxes(coarse) :215, one thread per
+// (coarse cell, slice `which` of 3)
 __device__ __forceinline__ void cell_restrict_fluxes(const LevelDev &F, const LevelDev &K, const CaseDev &C,
-                                                     int ic, int jc)
+                                                     int ic, int jc, int which, int nwhich)
 {
-    if (ic <= K.npx - 2 && jc <= K.npy - 2) cell_fluxes(K, jc * K.npx + ic);
-    if (ic >= 1 && jc >= 1 && ic <= K.npx - 2 && jc <= K.npy - 2) cell_restrict(F, K, C, ic, jc);
+    if (which == 0 && ic <= K.npx - 2 && jc <= K.npy - 2) cell_fluxes(K, jc * K.npx + ic);
+    if (ic >= 1 && jc >= 1 && ic <= K.npx - 2 && jc <= K.npy - 2)
+        for (int w = which; w < 3; w += nwhich) cell_restrict(F, K, C, ic, jc, w);
 }
 
-__global__ void __launch_bounds__(BLOCK) k_restv_fluxes(CaseDev *cs, int ig, int mode)
+__global__ void __launch_bounds__(BLOCK) k_restv_fluxes(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode)
 {
     CASE_PROLOGUE(mode);
     int i, j;
-    if (cell_at(dom_all(L), t, i, j)) cell_restv_fluxes(L, C.lv[ig + 1], i, j);
+    if (cell_at(dom_all(L), t, i, j)) cell_restv_fluxes(L, C.lv[ig + 1], C, i, j, blockIdx.z, gridDim.z);
 }
 
-__global__ void __launch_bounds__(BLOCK) k_restrict(CaseDev *cs, int ig, int mode)
+// restr{u,v,sc} + fluxes(coarse); with `what` != 0 also the coarse level's first
+// down-leg routine (the fused assembly): the defects a coarse cell's assembly reads
+// (resu, resv, ressc of that cell) come from the same thread, everything else from
+// restv, which finished in the previous launch.
+__global__ void __launch_bounds__(BLOCK) k_restrict(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode,
+                                                    unsigned what)
 {
     CASE_PROLOGUE(mode);
     const LevelDev &K = C.lv[ig + 1];
     int i, j;
-    if (cell_at(dom_all(K), t, i, j)) cell_restrict_fluxes(L, K, C, i, j);
+    if (!cell_at(dom_all(K), t, i, j)) return;
+    const int z = blockIdx.z, nz = gridDim.z;
+    cell_restrict_fluxes(L, K, C, i, j, z, nz);
+    if (!what || !mode_active(C, ig + 1, M_DOWN)) return;
+    // slice z assembles the equation whose defect it just computed
+    cell_asm(K, C, FluxLive(K), i, j, asm_slice(what, z, nz) & ~(unsigned)(A_FLUX | A_SC_OUTFLOW));
+    if (nz > 1 && z != 2) return;
+    // the scalar outflow ghost of an interior row is read by this kernel only in the
+    // defect of the cell west of it, so that cell (this thread, after its defect)
+    // writes it; ghosts of the boundary rows are read by nobody here
+    if ((what & A_SC_OUTFLOW) && C.ibc_xp == 4) {
+        double *sc = MGF(K, S_SC);
+        const int q = j * K.npx + i;
+        if (i == K.npx - 2 && j >= 1 && j <= K.npy - 2) sc[q + 1] = sc[q];
+        if (i == K.npx - 1 && (j == 0 || j == K.npy - 1)) sc[q] = sc[q - 1];
+    }
 }
 
-__global__ void __launch_bounds__(BLOCK) k_prol_corr(CaseDev *cs, int ig, int mode)
+__global__ void __launch_bounds__(BLOCK) k_prol_corr(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode)
 {
     CASE_PROLOGUE(mode);
     const LevelDev &K = C.lv[ig + 1];
@@ -339,7 +412,7 @@ __global__ void __launch_bounds__(BLOCK) k_prol_corr(CaseDev *cs, int ig, int mo
     if (cell_at(dom_interior(K), t, i, j)) cell_prol_corr(L, K, i, j);
 }
 
-__global__ void __launch_bounds__(BLOCK) k_prol_apply(CaseDev *cs, int ig, int mode)
+__global__ void __launch_bounds__(BLOCK) k_prol_apply(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode)
 {
     CASE_PROLOGUE(mode);
     const LevelDev &K = C.lv[ig + 1];
@@ -351,16 +424,13 @@ __global__ void __launch_bounds__(BLOCK) k_prol_apply(CaseDev *cs, int ig, int m
 // with its mean removed against the previous cycle, the history entry, the stop
 // rule, and prev <- current.  p sums are shifted by the previous cycle's means so a
 // uniform pressure drift does not cancel catastrophically.
-__global__ void __launch_bounds__(BLOCK) k_endcycle(CaseDev *cs)
+// The end-of-cycle work for level-0 cell index t of this block (see k_endcycle).
+__device__ __forceinline__ void end_of_cycle(const CaseDev &C, CaseState &ST, int t, int nb)
 {
-    CaseDev &C = cs[blockIdx.y];
-    if (C.done) return;
     const LevelDev &L = C.lv[0];
     const Dom d = dom_interior(L);
-    const int n = d.wi * d.wj, nb = (n + blockDim.x - 1) / blockDim.x;
-    if ((int)blockIdx.x >= nb) return;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const double kd = C.shift_d, kp = C.shift_p;
+    const int n = d.wi * d.wj;
+    const double kd = ST.shift_d, kp = ST.shift_p;
     double a[10];
 #pragma unroll
     for (int k = 0; k < 10; ++k) a[k] = 0.0;
@@ -399,24 +469,49 @@ __global__ void __launch_bounds__(BLOCK) k_endcycle(CaseDev *cs)
         double r = num == 0.0 ? 0.0 : (den <= 0.0 ? (double)INFINITY : sqrt(num / den));
         if (r > worst || r != r) worst = r;
     }
-    const double err = C.last_err;
-    const int k = C.ncyc;
-    const double delta = C.have_prev ? worst : 0.0;
+    const double err = ST.last_err;
+    const int k = ST.ncyc;
+    const double delta = ST.have_prev ? worst : 0.0;
     if (k < C.hist_cap) {
         C.hist_err[k] = err;
         C.hist_delta[k] = delta;
     }
-    C.ncyc = k + 1;
-    C.shift_d = kd + s[6] / N;
-    C.shift_p = kp + s[8] / N;
+    ST.ncyc = k + 1;
+    ST.shift_d = kd + s[6] / N;
+    ST.shift_p = kp + s[8] / N;
     const bool finite = isfinite(err) && isfinite(delta);
-    if (!finite) C.status |= CASE_NONFINITE;
+    if (!finite) ST.status |= CASE_NONFINITE;
     if (C.stop_enabled) {
-        if (!finite) C.done = 1;
-        else if (err < C.convergence) { C.done = 1; C.status |= CASE_CONVERGED_REF; }
-        else if (C.fp_tol > 0.0 && C.have_prev && delta < C.fp_tol) { C.done = 1; C.status |= CASE_CONVERGED_FP; }
+        if (!finite) ST.done = 1;
+        else if (err < C.convergence) { ST.done = 1; ST.status |= CASE_CONVERGED_REF; }
+        else if (C.fp_tol > 0.0 && ST.have_prev && delta < C.fp_tol) { ST.done = 1; ST.status |= CASE_CONVERGED_FP; }
     }
-    C.have_prev = 1;
+    ST.have_prev = 1;
+}
+
+__global__ void __launch_bounds__(BLOCK) k_endcycle(const CaseDev *__restrict__ cs, CaseState *st)
+{
+    const CaseDev &C = cs[blockIdx.y];
+    CaseState &ST = st[blockIdx.y];
+    if (ST.done) return;
+    const Dom d = dom_interior(C.lv[0]);
+    const int n = d.wi * d.wj, nb = (n + blockDim.x - 1) / blockDim.x;
+    if ((int)blockIdx.x >= nb) return;
+    end_of_cycle(C, ST, blockIdx.x * blockDim.x + threadIdx.x, nb);
+}
+
+// prolongation into level 0 followed by the end of the cycle: every thread reads
+// back only the level-0 cell it just wrote.
+__global__ void __launch_bounds__(BLOCK) k_prol_apply_end(const CaseDev *__restrict__ cs, CaseState *st, int mode)
+{
+    const int ig = 0;
+    CASE_PROLOGUE(mode);
+    const Dom d = dom_interior(L);
+    const int n = d.wi * d.wj, nb = (n + blockDim.x - 1) / blockDim.x;
+    if ((int)blockIdx.x >= nb) return;
+    int i, j;
+    if (cell_at(d, t, i, j)) cell_prol_apply(L, C.lv[1], i, j);
+    end_of_cycle(C, ST, t, nb);
 }
 
 // ------------------------------------------------- one-CTA coarse kernel
@@ -557,7 +652,7 @@ __device__ void tail_smooth(const LevelDev &L, int mask, int nsw, int isolve, do
 }
 
 // One SIMPLE step on level ig (down leg :201-207, up leg :235-244).
-__device__ void tail_step(CaseDev &C, int ig, bool down, const Sched &S, double *sm, int smd)
+__device__ void tail_step(const CaseDev &C, CaseState &ST, int ig, bool down, const Sched &S, double *sm, int smd)
 {
     const LevelDev &L = C.lv[ig];
     const FluxLive fl(L);
@@ -569,7 +664,7 @@ __device__ void tail_step(CaseDev &C, int ig, bool down, const Sched &S, double 
     for_cells(dom_interior(L), [&](int i, int j) { acc[0] += cell_mass_coefp(L, C, i, j); });
     if (ig == 0 && down) {
         block_sum<1>(acc);
-        if (threadIdx.x == 0) C.last_err = acc[0];
+        if (threadIdx.x == 0) ST.last_err = acc[0];
     }
     __syncthreads();
     tail_smooth(L, 1 << EQ_PP, S.nswpp, S.isolve, sm, smd);
@@ -589,16 +684,16 @@ __device__ void tail_step(CaseDev &C, int ig, bool down, const Sched &S, double 
     bound_block(C, L, down ? 3 : 7);
 }
 
-__device__ void tail_restrict(CaseDev &C, int ig)
+__device__ void tail_restrict(const CaseDev &C, int ig)
 {
     const LevelDev &F = C.lv[ig], &K = C.lv[ig + 1];
-    for_cells(dom_all(F), [&](int i, int j) { cell_restv_fluxes(F, K, i, j); });
+    for_cells(dom_all(F), [&](int i, int j) { cell_restv_fluxes(F, K, C, i, j, 0, 1); });
     __syncthreads();
-    for_cells(dom_all(K), [&](int i, int j) { cell_restrict_fluxes(F, K, C, i, j); });
+    for_cells(dom_all(K), [&](int i, int j) { cell_restrict_fluxes(F, K, C, i, j, 0, 1); });
     __syncthreads();
 }
 
-__device__ void tail_prolong(CaseDev &C, int ig)
+__device__ void tail_prolong(const CaseDev &C, int ig)
 {
     const LevelDev &F = C.lv[ig], &K = C.lv[ig + 1];
     for_cells(dom_interior(K), [&](int i, int j) { cell_prol_corr(F, K, i, j); });
@@ -609,67 +704,76 @@ __device__ void tail_prolong(CaseDev &C, int ig)
 
 // Every level at or below C.tail of one case (blockIdx.x): the down leg from
 // C.tail, the restrictions between those levels, and the up leg back to C.tail.
-__global__ void __launch_bounds__(TAIL_BLOCK, 1) k_tail(CaseDev *cs, Sched S, int smem_doubles)
+__global__ void __launch_bounds__(TAIL_BLOCK, 1) k_tail(const CaseDev *__restrict__ cs, CaseState *st, Sched S,
+                                                        int smem_doubles)
 {
     extern __shared__ double tsm[];
-    CaseDev &C = cs[blockIdx.x];
-    if (C.done || C.tail >= C.ngrid) return;
+    const CaseDev &C = cs[blockIdx.x];
+    CaseState &ST = st[blockIdx.x];
+    if (ST.done || C.tail >= C.ngrid) return;
     for (int ig = C.tail; ig < C.ngrid; ++ig) {
-        tail_step(C, ig, true, S, tsm, smem_doubles);
+        tail_step(C, ST, ig, true, S, tsm, smem_doubles);
         if (ig != C.ngrid - 1) tail_restrict(C, ig);
     }
     for (int ig = C.ngrid - 1; ig > C.tail; --ig) {
         tail_prolong(C, ig - 1);
-        if (ig != 1) tail_step(C, ig - 1, false, S, tsm, smem_doubles);
+        if (ig != 1) tail_step(C, ST, ig - 1, false, S, tsm, smem_doubles);
     }
 }
 
 // ------------------------------------------------------------- launcher
-int smooth_smem_bytes(int isolve, int units)
+int smooth_smem_bytes(int isolve, int units, int tile)
 {
-    const int w = TILE_X + 2 * units, h = TILE_Y + 2 * units;
+    const int w = tile + 2 * units, h = tile + 2 * units;
     return (isolve == MGFVM_JACOBI ? 8 : 7) * w * h * (int)sizeof(double);
 }
 
 cudaError_t configure_kernels()
 {
     cudaError_t e = cudaFuncSetAttribute(k_smooth<MGFVM_JACOBI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         smooth_smem_bytes(MGFVM_JACOBI, MAX_UNITS));
+                                         smooth_smem_bytes(MGFVM_JACOBI, MAX_UNITS, MAX_TILE));
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_smooth<MGFVM_GAUSS_SEIDEL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 smooth_smem_bytes(MGFVM_GAUSS_SEIDEL, MAX_UNITS));
+                                 smooth_smem_bytes(MGFVM_GAUSS_SEIDEL, MAX_UNITS, MAX_TILE));
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, TAIL_SMEM_MAX);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_smooth_level, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 8 * LEVEL_SMEM_CELLS * (int)sizeof(double));
     return e;
 }
 
-cudaError_t launch_one(const Launch &X, CaseDev *dc, const Sched &S, cudaStream_t st)
+cudaError_t launch_one(const Launch &X, const CaseDev *dc, CaseState *ds, const Sched &S, cudaStream_t st)
 {
     const dim3 g = X.grid;
     const int b = X.block;
     switch (X.kernel) {
-    case K_FLUXES: k_fluxes<<<g, b, 0, st>>>(dc, X.ig, X.mode); break;
+    case K_FLUXES: k_fluxes<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode); break;
     case K_ASM:
-        if (X.a1) k_asm<1><<<g, b, 0, st>>>(dc, X.ig, X.mode, (unsigned)X.a0);
-        else k_asm<0><<<g, b, 0, st>>>(dc, X.ig, X.mode, (unsigned)X.a0);
+        if (X.a1) k_asm<1><<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, (unsigned)X.a0);
+        else k_asm<0><<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, (unsigned)X.a0);
         break;
-    case K_MASS_COEFP: k_mass_coefp<<<g, b, 0, st>>>(dc, X.ig, X.mode, X.a0); break;
-    case K_UPDATE: k_update<<<g, b, 0, st>>>(dc, X.ig, X.mode); break;
-    case K_PFIX: k_pfix<<<g, b, 0, st>>>(dc, X.ig, X.mode, X.a0); break;
-    case K_BOUND: k_bound<<<g, b, 0, st>>>(dc, X.ig, X.mode, X.a0); break;
+    case K_MASS_COEFP: k_mass_coefp<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, X.a0); break;
+    case K_UPDATE: k_update<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, X.a0); break;
+    case K_PFIX: k_pfix<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, X.a0); break;
+    case K_BOUND: k_bound<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, X.a0); break;
     case K_SMOOTH:
         if (S.isolve == MGFVM_JACOBI)
-            k_smooth<MGFVM_JACOBI><<<g, b, X.smem, st>>>(dc, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3);
+            k_smooth<MGFVM_JACOBI><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
         else
-            k_smooth<MGFVM_GAUSS_SEIDEL><<<g, b, X.smem, st>>>(dc, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3);
+            k_smooth<MGFVM_GAUSS_SEIDEL><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
         break;
-    case K_COPY: k_copy<<<g, b, 0, st>>>(dc, X.ig, X.mode, X.a0); break;
-    case K_RESTV_FLUXES: k_restv_fluxes<<<g, b, 0, st>>>(dc, X.ig, X.mode); break;
-    case K_RESTRICT: k_restrict<<<g, b, 0, st>>>(dc, X.ig, X.mode); break;
-    case K_PROL_CORR: k_prol_corr<<<g, b, 0, st>>>(dc, X.ig, X.mode); break;
-    case K_PROL_APPLY: k_prol_apply<<<g, b, 0, st>>>(dc, X.ig, X.mode); break;
-    case K_TAIL: k_tail<<<g, b, X.smem, st>>>(dc, S, X.smem / (int)sizeof(double)); break;
-    case K_ENDCYCLE: k_endcycle<<<g, b, 0, st>>>(dc); break;
+    case K_COPY: k_copy<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, X.a0); break;
+    case K_SMOOTH_LEVEL:
+        k_smooth_level<<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, S.isolve, X.smem / (int)sizeof(double));
+        break;
+    case K_RESTV_FLUXES: k_restv_fluxes<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode); break;
+    case K_RESTRICT: k_restrict<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, (unsigned)X.a0); break;
+    case K_PROL_CORR: k_prol_corr<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode); break;
+    case K_PROL_APPLY: k_prol_apply<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode); break;
+    case K_TAIL: k_tail<<<g, b, X.smem, st>>>(dc, ds, S, X.smem / (int)sizeof(double)); break;
+    case K_ENDCYCLE: k_endcycle<<<g, b, 0, st>>>(dc, ds); break;
+    case K_PROL_APPLY_END: k_prol_apply_end<<<g, b, 0, st>>>(dc, ds, X.mode); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

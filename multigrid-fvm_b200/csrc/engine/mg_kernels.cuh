@@ -15,17 +15,18 @@ enum KernelId {
     K_BOUND,         // a0 = bits: 1 periodic, 2 outflow u/v/p, 4 outflow sc
     K_SMOOTH,        // tile smoother: a0 = eq mask, a1 = first unit, a2 = units, a3 = dir
     K_COPY,          // copy equations' buffers back: a0 = eq mask
+    K_SMOOTH_LEVEL,  // whole level in shared memory: a0 = eq mask, a1 = sweeps
     K_RESTV_FLUXES,  // restv + fine fluxes
     K_RESTRICT,      // restr{u,v,sc} + coarse fluxes
     K_PROL_CORR, K_PROL_APPLY,
-    K_TAIL, K_ENDCYCLE, K_NKERNELS
+    K_TAIL, K_ENDCYCLE, K_PROL_APPLY_END, K_NKERNELS
 };
 
 struct Launch {
     int kernel;
     int ig;            // level (fine level for transfers)
     int mode;          // enum Mode
-    int a0, a1, a2, a3;
+    int a0, a1, a2, a3, a4;
     dim3 grid;
     int block;
     int smem;
@@ -36,12 +37,14 @@ struct Sched {
 };
 
 // Shared-memory tile smoother geometry.
-constexpr int TILE_X = 32, TILE_Y = 32;
+constexpr int MAX_TILE = 32;   // tile side of the shared-memory smoother (16 or 32)
 constexpr int SMOOTH_BLOCK = 1024;
 constexpr int MAX_UNITS = 10;   // half-sweeps (GS) or sweeps (Jacobi) per launch
-int smooth_smem_bytes(int isolve, int units);
+constexpr int LEVEL_SMEM_CELLS = 3400;   // levels up to this many padded cells smooth in one CTA
+int smooth_smem_bytes(int isolve, int units, int tile);
 
-cudaError_t launch_one(const Launch &L, CaseDev *dcases, const Sched &S, cudaStream_t stream);
+cudaError_t launch_one(const Launch &L, const CaseDev *dcases, CaseState *dstate, const Sched &S,
+                       cudaStream_t stream);
 cudaError_t configure_kernels();
 
 // Kernels of the raw-pointer entry points.

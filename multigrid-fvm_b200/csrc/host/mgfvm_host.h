@@ -31,6 +31,7 @@ typedef struct mgfvm_obstacle_prog {
     int *cells;
     unsigned *codes;
     int max_adds;      /* longest sequence seen */
+    int touches_outlet; /* a copy reads or writes column npx-2 or npx-1 (the outflow's columns) */
 } mgfvm_obstacle_prog;
 
 int mgfvm_build_obstacle_prog(const mgfvm_config *c, int ig, mgfvm_obstacle_prog *out);

@@ -99,13 +99,15 @@ int mgfvm_build_obstacle_prog(const mgfvm_config *c, int ig, mgfvm_obstacle_prog
     for (size_t q = 0; q < n; ++q)
         if (written[q] && origin[q] != (int)q) { pairs[2 * m] = (int)q; pairs[2 * m + 1] = origin[q]; ++m; }
     qsort(pairs, (size_t)m, 2 * sizeof(int), cmp_pair);
-    int hazard = 0;
+    int hazard = 0, outlet = 0;
     for (int k = 0; k < m; ++k) {
         out->dst[k] = pairs[2 * k];
         out->src[k] = pairs[2 * k + 1];
         int s = out->src[k];
         if (written[s] && origin[s] != s) hazard = 1;
+        if (out->dst[k] % nx >= nx - 2 || s % nx >= nx - 2) outlet = 1;
     }
+    out->touches_outlet = outlet;
     out->ncopy = m;
     out->hazard = hazard;
     m = 0;
