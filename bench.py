@@ -65,6 +65,40 @@ def cell_sweeps_per_cycle(cfg):
     return (3 * cfg.nswpm + cfg.nswpp) * tot
 
 
+def load_peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+# DRAM bytes (read + write) per k_smooth launch of the p' smoothing on level 0, from one
+# ncu capture of `python bench.py --profile-cycles 1` (profiles/k_smooth_c1.md).
+ROOFLINE_TRAFFIC = {}
+
+
+def smoother_roofline(solver, cases, traffic=None, reps=20):
+    """Roofline entry of k_smooth: the p' smoothing of level 0 (nswpp red-black sweeps,
+    split into launches of up to 10 half-sweeps each), timed with CUDA events on the
+    context stream.  Algorithmic bytes: 64 B per cell-sweep (6 coefficients + phi read
+    + phi write, FP64) x nswpp x interior cells, per launch."""
+    solver.time_op("smooth_pp", 0, 2)
+    kms, klaunch = solver.time_op("smooth_pp", 0, reps)
+    per_launch_ms = kms / klaunch
+    bytes_per_op = sum(64 * c.nswpp * c.nfx * c.nfy for c in cases)
+    algo_bytes = bytes_per_op * reps / klaunch
+    peaks = load_peaks()
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = algo_bytes / (per_launch_ms / 1e3) / 1e9
+    return {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "traffic": traffic,
+            "kernel": "k_smooth (shared-memory tile smoother, p' equation, level 0)",
+            "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+            "per_launch_us": round(per_launch_ms * 1e3, 3), "launches_per_op": klaunch // reps,
+            "algorithmic_bytes_per_launch": int(algo_bytes)}
+
+
 # --------------------------------------------------------------- clocks
 class ClockSampler:
     def __init__(self, index):
@@ -277,27 +311,8 @@ def main():
     sweeps = sum(cell_sweeps_per_cycle(c) * int(n) for c, n in zip(cases, cycles_per_solve))
     cell_sweeps_per_s = sweeps * a.steps * world / (ms / 1e3)
 
-    # ---- dominant kernel: one colour of the red-black p' sweep on level 0 (live)
-    import mgfvm
-    reps = 20
-    solver.time_op("smooth_pp", 0, 2)
-    kms, klaunch = solver.time_op("smooth_pp", 0, reps)
-    per_launch_ms = kms / klaunch
-    colour_cells = sum(((c.nfx * c.nfy) + 1) // 2 for c in cases)
-    algo_bytes = colour_cells * 64          # 6 coefficients + phi read + phi write, 8 B each
-    peaks = {}
-    try:
-        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
-            peaks = json.load(f)
-    except Exception:
-        pass
-    peak = peaks.get("hbm_gbs", 6650.0)
-    achieved = algo_bytes / (per_launch_ms / 1e3) / 1e9
-    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": None,
-                "kernel": "k_gs (one colour of a red-black sweep, p' equation, level 0)",
-                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
-                "per_launch_us": round(per_launch_ms * 1e3, 3), "algorithmic_bytes_per_launch": algo_bytes}
+    # ---- dominant kernel: the shared-memory tile smoother on level 0, p' equation (live)
+    roofline = smoother_roofline(solver, cases, ROOFLINE_TRAFFIC.get(a.workload))
 
     # ---- end to end through the public API with host buffers
     e2e = None

@@ -65,6 +65,7 @@ struct mgfvm_ctx {
     std::vector<Launch> cyc;
     std::vector<int> maxcells;                // per level: max npx*npy over cases
     int last_eq[MAXLEV];                      // per level: equation of the visible coefficient set
+    int units_cap[MAXLEV] = {};               // per level: smoother units per tile launch (0: default)
     long long launches = 0;
     long long h2d = 0, d2h = 0;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -109,41 +110,53 @@ struct Builder {
             }
         return std::max<long long>(m, 1);
     }
-    // Smaller tiles shorten each CTA's chain of dependent half-sweeps; they pay off
-    // while the level's 32-wide tiles would not fill two CTAs per SM.
-    int tile_for(int ig) const
+    // Whether one CTA per (case, equation) holds the level: its padded grid has at
+    // most SMOOTH_BLOCK vertical cell pairs in every case.
+    bool whole_level(int ig, int &mx, int &my) const
     {
-        int sms = 148;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, x->device);
-        return x->ncases * tiles(ig, 32) < sms / 8 ? 16 : 32;
+        mx = my = 0;
+        for (const mgfvm_config &c : x->cfg)
+            if (ig < c.ngrid) {
+                mx = std::max(mx, npx_of(c, ig));
+                my = std::max(my, npy_of(c, ig));
+            }
+        return mx > 0 && mx * ((my + 1) / 2) <= SMOOTH_BLOCK;
     }
-    // `nsw` sweeps of the equations in `mask`: the 2*nsw half-sweeps (Gauss-Seidel) or
-    // nsw sweeps (Jacobi) go in an even number of tile launches of at most MAX_UNITS
-    // each, alternating field -> buffer -> field; a single Jacobi sweep copies back.
+    static int round32(int n) { return std::max(32, (n + 31) / 32 * 32); }
+    // `nsw` sweeps of the equations in `mask`.  A level that fits one CTA runs every
+    // unit (half-sweep of red-black GS, sweep of Jacobi) in one in-place launch;
+    // otherwise the units go in an even number of tile launches of at most the level's
+    // cap each, alternating field -> buffer -> field (a single launch copies back).
     void smooth(int ig, int mode, int mask, int nsw)
     {
         const int isolve = x->sched.isolve;
         const int units = isolve == MGFVM_GAUSS_SEIDEL ? 2 * nsw : nsw;
         if (units <= 0 || (isolve != MGFVM_JACOBI && isolve != MGFVM_GAUSS_SEIDEL)) return;
-        if (cells(ig) <= LEVEL_SMEM_CELLS) {       // small level: one CTA per (case, equation)
-            Launch &L = add(K_SMOOTH_LEVEL, ig, mode, 0, mask, nsw);
-            L.grid = dim3(__builtin_popcount((unsigned)mask), x->ncases);
-            L.block = SMOOTH_BLOCK;
-            L.smem = (isolve == MGFVM_JACOBI ? 8 : 7) * (int)cells(ig) * (int)sizeof(double);
+        const int neq = __builtin_popcount((unsigned)mask);
+        const int bufs = isolve == MGFVM_JACOBI ? 2 : 1;
+        int mx, my;
+        if (whole_level(ig, mx, my)) {
+            Launch &L = add(K_SMOOTH, ig, mode, 0, mask, 0, units, 2);
+            L.a4 = std::max(mx, my);
+            L.grid = dim3(1, x->ncases, neq);
+            L.block = round32(mx * ((my + 1) / 2));
+            L.smem = bufs * mx * my * (int)sizeof(double);
             return;
         }
-        int chunks = (units + MAX_UNITS - 1) / MAX_UNITS;
+        const int cap = x->units_cap[ig] > 0 ? x->units_cap[ig] : MAX_UNITS;
+        int chunks = (units + cap - 1) / cap;
         if ((chunks & 1) && units >= chunks + 1) ++chunks;
-        const int neq = __builtin_popcount((unsigned)mask);
-        const int tile = tile_for(ig);
+        const int hmax = (units + chunks - 1) / chunks;
+        const int tile = std::max(1, smooth_pairs_side(hmax));
+        const int side = tile + 2 * hmax;
         int u0 = 0;
         for (int c = 0; c < chunks; ++c) {
             const int nu = units / chunks + (c < units % chunks ? 1 : 0);
             Launch &L = add(K_SMOOTH, ig, mode, 0, mask, u0, nu, c & 1);
             L.a4 = tile;
             L.grid = dim3((unsigned)tiles(ig, tile), x->ncases, neq);
-            L.block = SMOOTH_BLOCK;
-            L.smem = smooth_smem_bytes(isolve, nu, tile);
+            L.block = std::min(SMOOTH_BLOCK, round32(side * ((side + 1) / 2)));
+            L.smem = bufs * side * side * (int)sizeof(double);
             u0 += nu;
         }
         if (chunks & 1) {
@@ -752,6 +765,15 @@ int mgfvm_set_inlet_profile(mgfvm_ctx *x, int icase, const double *u, int n)
     return init_state(x, icase);
 }
 
+// A kernel found its launch shape too small for its tile (a schedule bug): fail loudly.
+static int check_status(mgfvm_ctx *x)
+{
+    for (int c = 0; c < x->ncases; ++c)
+        if (x->hs[c].status & CASE_BAD_LAUNCH)
+            return mgfvm_fail(MGFVM_ECUDA, "case %d: a smoother launch was too small for its tile", c);
+    return MGFVM_OK;
+}
+
 int mgfvm_cycle(mgfvm_ctx *x, int ncycles)
 {
     RC(check_ctx(x));
@@ -769,7 +791,8 @@ int mgfvm_cycle(mgfvm_ctx *x, int ncycles)
     CK(cudaEventElapsedTime(&ms, x->e0, x->e1));
     x->last_ms = ms;
     CK(cudaGetLastError());
-    return MGFVM_OK;
+    RC(pull(x));
+    return check_status(x);
 }
 
 int mgfvm_solve(mgfvm_ctx *x, int max_cycles, double fp_tol, int *cycles_out)
@@ -811,7 +834,7 @@ int mgfvm_solve(mgfvm_ctx *x, int max_cycles, double fp_tol, int *cycles_out)
         if (x->hs[c].status & CASE_NONFINITE) nonfinite = 1;
     }
     if (nonfinite) return mgfvm_fail(MGFVM_ENONFINITE, "a case's mass error or fixed-point change became NaN/Inf");
-    return MGFVM_OK;
+    return check_status(x);
 }
 
 int mgfvm_history(mgfvm_ctx *x, int icase, double *err, double *delta, int cap, int *n_out)

@@ -231,15 +231,18 @@ __global__ void __launch_bounds__(BLOCK) k_bound(const CaseDev *__restrict__ cs,
 }
 
 // Temporal-blocked smoother.  blockIdx.z picks an equation of `mask`, blockIdx.x a
-// tile x tile block of its sweep domain.  The CTA loads the tile plus a halo of
-// `nu` cells (clipped at the domain's boundary ring) and the equation's
-// coefficients into shared memory, runs `nu` units — half-sweeps of red-black
-// Gauss-Seidel (colour of global unit u0+h-1: even = red) or Jacobi sweeps — each on
-// a window one cell narrower on every cut side, and writes the tile (plus the
-// boundary ring where the tile touches it) to the other buffer: dir 0 reads the
-// field and writes the equation's ping-pong buffer, dir 1 the reverse.  Every cell
-// update is the reference's formula on the same neighbour values, so the result is
-// bit-identical to sweeping the whole level unit by unit.
+// tile x tile block of its sweep domain.  The CTA stages the tile plus a halo of `nu`
+// cells (clipped at the domain's boundary ring): every thread owns one vertical pair
+// of cells, one of each colour, holds both cells' six coefficients in registers and
+// their field values in shared memory, so a half-sweep is one update per thread.  It
+// runs `nu` units — half-sweeps of red-black Gauss-Seidel (colour of global unit
+// u0+h-1: even = red, i+j even) or Jacobi sweeps — each on a window one cell narrower
+// on every cut side, then writes the tile (plus the boundary ring where the tile
+// touches it): dir 0 from the field to the equation's ping-pong buffer, dir 1 the
+// reverse, dir 2 in place (a single tile covering the domain: it reads everything
+// before it writes).  Every cell update is the reference's formula on the same
+// neighbour values, so the result is bit-identical to sweeping the whole level unit
+// by unit.
 template <int ISOLVE>
 __global__ void __launch_bounds__(SMOOTH_BLOCK) k_smooth(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode, int mask, int u0, int nu,
                                                          int dir, int tile)
@@ -260,78 +263,85 @@ __global__ void __launch_bounds__(SMOOTH_BLOCK) k_smooth(const CaseDev *__restri
     const int H = nu;
     const int rx0 = max(x0 - H, d.i0 - 1), rx1 = min(x1 + H, dx1 + 1);
     const int ry0 = max(y0 - H, d.j0 - 1), ry1 = min(y1 + H, dy1 + 1);
-    const int W = rx1 - rx0 + 1, R = (ry1 - ry0 + 1) * W;
+    const int W = rx1 - rx0 + 1, Hh = ry1 - ry0 + 1;
+    const int npairs = W * ((Hh + 1) >> 1);
+    if (npairs > (int)blockDim.x) {     // the schedule sizes blocks to fit; never taken
+        if (threadIdx.x == 0) atomicOr(&st[blockIdx.y].status, (int)CASE_BAD_LAUNCH);
+        return;
+    }
     const int npx = L.npx;
-    const int fs = e == EQ_U ? S_U : e == EQ_V ? S_V : e == EQ_PP ? S_PP : S_SC;
-    const int ts = eq_tmp(e);
-    const double *src = L.f[dir == 0 ? fs : ts];
+    const int fs = eq_field(e), ts = eq_tmp(e);
+    const double *src = L.f[dir == 1 ? ts : fs];
     double *dst = L.f[dir == 0 ? ts : fs];
-    double *sphi = sm, *saw = sm + R, *sae = saw + R, *sas = sae + R, *san = sas + R, *sap = san + R,
-           *ssu = sap + R, *sphi2 = ssu + R;
-    const double *gaw = L.f[co_slot(e, CK_AW)], *gae = L.f[co_slot(e, CK_AE)], *gas = L.f[co_slot(e, CK_AS)],
-                 *gan = L.f[co_slot(e, CK_AN)], *gap = L.f[co_slot(e, CK_AP)], *gsu = L.f[co_slot(e, CK_SU)];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-    const int Hr = ry1 - ry0 + 1;
-    for (int r = warp; r < Hr; r += nwarp) {                 // one warp per row of R
-        const double *srow = src + (size_t)(ry0 + r) * npx + rx0;
-        const size_t g0 = (size_t)(ry0 + r) * npx + rx0;
-        for (int c = lane; c < W; c += 32) {
-            const int k = r * W + c;
-            const double ph = srow[c];
-            sphi[k] = ph;
-            if (ISOLVE == MGFVM_JACOBI) sphi2[k] = ph;
-            saw[k] = gaw[g0 + c]; sae[k] = gae[g0 + c]; sas[k] = gas[g0 + c];
-            san[k] = gan[g0 + c]; sap[k] = gap[g0 + c]; ssu[k] = gsu[g0 + c];
-        }
+    double *phi = sm, *phi2 = sm + W * Hh;
+    const double *__restrict__ gaw = L.f[co_slot(e, CK_AW)];
+    const double *__restrict__ gae = L.f[co_slot(e, CK_AE)];
+    const double *__restrict__ gas = L.f[co_slot(e, CK_AS)];
+    const double *__restrict__ gan = L.f[co_slot(e, CK_AN)];
+    const double *__restrict__ gap = L.f[co_slot(e, CK_AP)];
+    const double *__restrict__ gsu = L.f[co_slot(e, CK_SU)];
+
+    const int t = threadIdx.x;
+    const bool own = t < npairs;
+    const int c = own ? t % W : 0, r = own ? 2 * (t / W) : 0;
+    const int i = rx0 + c, jr = ry0 + r;                   // the pair (i, jr), (i, jr + 1)
+    const bool two = own && r + 1 < Hh;
+    const int jA = ((i + jr) & 1) == 0 ? jr : jr + 1;      // red cell
+    const int jB = jA == jr ? jr + 1 : jr;                 // black cell
+    const bool okA = own && (jA == jr || two), okB = own && (jB == jr || two);
+    const int kA = (jA - ry0) * W + c, kB = (jB - ry0) * W + c;
+    double A[6] = {0, 0, 0, 0, 0, 0}, B[6] = {0, 0, 0, 0, 0, 0}, pA = 0.0, pB = 0.0;
+    if (okA) {
+        const size_t g = (size_t)jA * npx + i;
+        pA = src[g];
+        A[0] = gaw[g]; A[1] = gae[g]; A[2] = gas[g]; A[3] = gan[g]; A[4] = gap[g]; A[5] = gsu[g];
+    }
+    if (okB) {
+        const size_t g = (size_t)jB * npx + i;
+        pB = src[g];
+        B[0] = gaw[g]; B[1] = gae[g]; B[2] = gas[g]; B[3] = gan[g]; B[4] = gap[g]; B[5] = gsu[g];
+    }
+    if (okA) {
+        phi[kA] = pA;
+        if (ISOLVE == MGFVM_JACOBI) phi2[kA] = pA;
+    }
+    if (okB) {
+        phi[kB] = pB;
+        if (ISOLVE == MGFVM_JACOBI) phi2[kB] = pB;
     }
     __syncthreads();
     for (int h = 1; h <= nu; ++h) {
         const int wx0 = max(x0 - H + h, d.i0), wx1 = min(x1 + H - h, dx1);
         const int wy0 = max(y0 - H + h, d.j0), wy1 = min(y1 + H - h, dy1);
+        const bool inx = i >= wx0 && i <= wx1;
         if (ISOLVE == MGFVM_GAUSS_SEIDEL) {
-            const int colour = (u0 + h - 1) & 1;
-            for (int j = wy0 + warp; j <= wy1; j += nwarp) {
-                const int i0 = wx0 + ((((wx0 + j) & 1) != colour) ? 1 : 0);
-                for (int i = i0 + 2 * lane; i <= wx1; i += 64) {
-                    const int k = (j - ry0) * W + (i - rx0);
-                    sphi[k] = gs_value(saw[k], sae[k], sas[k], san[k], sap[k], ssu[k], sphi[k - 1], sphi[k + 1],
-                                       sphi[k - W], sphi[k + W]);
-                }
+            if (((u0 + h - 1) & 1) == 0) {
+                if (okA && inx && jA >= wy0 && jA <= wy1)
+                    phi[kA] = gs_value(A[0], A[1], A[2], A[3], A[4], A[5], phi[kA - 1], phi[kA + 1], phi[kA - W],
+                                       phi[kA + W]);
+            } else {
+                if (okB && inx && jB >= wy0 && jB <= wy1)
+                    phi[kB] = gs_value(B[0], B[1], B[2], B[3], B[4], B[5], phi[kB - 1], phi[kB + 1], phi[kB - W],
+                                       phi[kB + W]);
             }
         } else {
-            const double *cur = ((h - 1) & 1) ? sphi2 : sphi;
-            double *nxt = ((h - 1) & 1) ? sphi : sphi2;
-            for (int j = wy0 + warp; j <= wy1; j += nwarp)
-                for (int i = wx0 + lane; i <= wx1; i += 32) {
-                    const int k = (j - ry0) * W + (i - rx0);
-                    nxt[k] = jacobi_value(saw[k], sae[k], sas[k], san[k], sap[k], ssu[k], cur[k - 1], cur[k + 1],
-                                          cur[k - W], cur[k + W], cur[k]);
-                }
+            const double *cur = ((h - 1) & 1) ? phi2 : phi;
+            double *nxt = ((h - 1) & 1) ? phi : phi2;
+            if (okA && inx && jA >= wy0 && jA <= wy1)
+                nxt[kA] = jacobi_value(A[0], A[1], A[2], A[3], A[4], A[5], cur[kA - 1], cur[kA + 1], cur[kA - W],
+                                       cur[kA + W], cur[kA]);
+            if (okB && inx && jB >= wy0 && jB <= wy1)
+                nxt[kB] = jacobi_value(B[0], B[1], B[2], B[3], B[4], B[5], cur[kB - 1], cur[kB + 1], cur[kB - W],
+                                       cur[kB + W], cur[kB]);
         }
         __syncthreads();
     }
-    const double *res = (ISOLVE == MGFVM_JACOBI && (nu & 1)) ? sphi2 : sphi;
+    const double *res = (ISOLVE == MGFVM_JACOBI && (nu & 1)) ? phi2 : phi;
     const int ox0 = x0 == d.i0 ? x0 - 1 : x0, ox1 = x1 == dx1 ? x1 + 1 : x1;
     const int oy0 = y0 == d.j0 ? y0 - 1 : y0, oy1 = y1 == dy1 ? y1 + 1 : y1;
-    const int ow = ox1 - ox0 + 1, on = ow * (oy1 - oy0 + 1);
-    (void)on;
-    for (int j = oy0 + warp; j <= oy1; j += nwarp)
-        for (int i = ox0 + lane; i <= ox1; i += 32) dst[j * npx + i] = res[(j - ry0) * W + (i - rx0)];
-}
-
-// Whole-level smoother for small levels: one CTA per (case, equation of `mask`)
-// stages the equation's field and coefficients for the entire level in shared
-// memory and runs every sweep there (no halo, no second buffer).
-__device__ void tail_smooth(const LevelDev &L, int mask, int nsw, int isolve, double *sm, int sm_doubles);
-
-__global__ void __launch_bounds__(SMOOTH_BLOCK) k_smooth_level(const CaseDev *__restrict__ cs, CaseState *st, int ig,
-                                                               int mode, int mask, int nsw, int isolve, int smd)
-{
-    extern __shared__ double sm[];
-    const CaseDev &C = cs[blockIdx.y];
-    if (!case_active(C, st[blockIdx.y], ig, mode)) return;
-    const int e = nth_eq(mask, blockIdx.x);
-    tail_smooth(C.lv[ig], 1 << e, nsw, isolve, sm, smd);
+    const bool outx = i >= ox0 && i <= ox1;
+    if (okA && outx && jA >= oy0 && jA <= oy1) dst[(size_t)jA * npx + i] = res[kA];
+    if (okB && outx && jB >= oy0 && jB <= oy1) dst[(size_t)jB * npx + i] = res[kB];
 }
 
 // After an odd number of smoothing launches the result sits in the ping-pong buffer.
@@ -602,10 +612,11 @@ __device__ void tail_smooth(const LevelDev &L, int mask, int nsw, int isolve, do
                          *cs_ = MGF(L, co_slot(e, CK_AS)), *cn = MGF(L, co_slot(e, CK_AN)),
                          *cp = MGF(L, co_slot(e, CK_AP)), *cu = MGF(L, co_slot(e, CK_SU));
             for (int q = threadIdx.x; q < n; q += blockDim.x) {
-                const double ph = phi[q];
+                // every load before the first store: the stores may not be moved above them
+                const double ph = phi[q], w = cw[q], ea = ce[q], so = cs_[q], no = cn[q], pc = cp[q], s0 = cu[q];
                 b[q] = ph;
-                b[n + q] = cw[q]; b[2 * n + q] = ce[q]; b[3 * n + q] = cs_[q];
-                b[4 * n + q] = cn[q]; b[5 * n + q] = cp[q]; b[6 * n + q] = cu[q];
+                b[n + q] = w; b[2 * n + q] = ea; b[3 * n + q] = so;
+                b[4 * n + q] = no; b[5 * n + q] = pc; b[6 * n + q] = s0;
                 if (per == 8) b[7 * n + q] = ph;
             }
         }
@@ -722,25 +733,16 @@ __global__ void __launch_bounds__(TAIL_BLOCK, 1) k_tail(const CaseDev *__restric
 }
 
 // ------------------------------------------------------------- launcher
-int smooth_smem_bytes(int isolve, int units, int tile)
+int smooth_pairs_side(int units)
 {
-    const int w = tile + 2 * units, h = tile + 2 * units;
-    return (isolve == MGFVM_JACOBI ? 8 : 7) * w * h * (int)sizeof(double);
+    int s = 1;
+    while ((s + 1) * ((s + 2) / 2) <= SMOOTH_BLOCK) ++s;   // largest square region of <= SMOOTH_BLOCK pairs
+    return s - 2 * units;
 }
 
 cudaError_t configure_kernels()
 {
-    cudaError_t e = cudaFuncSetAttribute(k_smooth<MGFVM_JACOBI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         smooth_smem_bytes(MGFVM_JACOBI, MAX_UNITS, MAX_TILE));
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_smooth<MGFVM_GAUSS_SEIDEL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 smooth_smem_bytes(MGFVM_GAUSS_SEIDEL, MAX_UNITS, MAX_TILE));
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, TAIL_SMEM_MAX);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_smooth_level, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 8 * LEVEL_SMEM_CELLS * (int)sizeof(double));
-    return e;
+    return cudaFuncSetAttribute(k_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, TAIL_SMEM_MAX);
 }
 
 cudaError_t launch_one(const Launch &X, const CaseDev *dc, CaseState *ds, const Sched &S, cudaStream_t st)
@@ -764,9 +766,6 @@ cudaError_t launch_one(const Launch &X, const CaseDev *dc, CaseState *ds, const 
             k_smooth<MGFVM_GAUSS_SEIDEL><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
         break;
     case K_COPY: k_copy<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, X.a0); break;
-    case K_SMOOTH_LEVEL:
-        k_smooth_level<<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, S.isolve, X.smem / (int)sizeof(double));
-        break;
     case K_RESTV_FLUXES: k_restv_fluxes<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode); break;
     case K_RESTRICT: k_restrict<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, (unsigned)X.a0); break;
     case K_PROL_CORR: k_prol_corr<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode); break;

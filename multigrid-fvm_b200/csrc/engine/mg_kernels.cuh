@@ -13,9 +13,8 @@ enum KernelId {
     K_UPDATE,
     K_PFIX,          // a0 = phase (0 gather, 1 scatter, 2 both)
     K_BOUND,         // a0 = bits: 1 periodic, 2 outflow u/v/p, 4 outflow sc
-    K_SMOOTH,        // tile smoother: a0 = eq mask, a1 = first unit, a2 = units, a3 = dir
+    K_SMOOTH,        // tile smoother: a0 = eq mask, a1 = first unit, a2 = units, a3 = dir, a4 = tile
     K_COPY,          // copy equations' buffers back: a0 = eq mask
-    K_SMOOTH_LEVEL,  // whole level in shared memory: a0 = eq mask, a1 = sweeps
     K_RESTV_FLUXES,  // restv + fine fluxes
     K_RESTRICT,      // restr{u,v,sc} + coarse fluxes
     K_PROL_CORR, K_PROL_APPLY,
@@ -36,12 +35,11 @@ struct Sched {
     int isolve, nswpm, nswpp;
 };
 
-// Shared-memory tile smoother geometry.
-constexpr int MAX_TILE = 32;   // tile side of the shared-memory smoother (16 or 32)
+// Tile smoother geometry: a CTA of at most SMOOTH_BLOCK threads, one vertical cell pair
+// per thread, covers a tile plus a halo of one cell per unit on every side.
 constexpr int SMOOTH_BLOCK = 1024;
-constexpr int MAX_UNITS = 10;   // half-sweeps (GS) or sweeps (Jacobi) per launch
-constexpr int LEVEL_SMEM_CELLS = 3400;   // levels up to this many padded cells smooth in one CTA
-int smooth_smem_bytes(int isolve, int units, int tile);
+constexpr int MAX_UNITS = 10;   // default cap of half-sweeps (GS) or sweeps (Jacobi) per launch
+int smooth_pairs_side(int units);   // tile side whose region fits SMOOTH_BLOCK pairs
 
 cudaError_t launch_one(const Launch &L, const CaseDev *dcases, CaseState *dstate, const Sched &S,
                        cudaStream_t stream);

@@ -178,7 +178,7 @@ class Solver:
         check(self._lib.mgfvm_time_op(self._h, op, level, reps, C.byref(ms), C.byref(n)))
         return ms.value, n.value
 
-    KERNELS = ["fluxes", "asm", "mass_coefp", "update", "pfix", "bound", "smooth", "copy", "smooth_level", "restv_fluxes",
+    KERNELS = ["fluxes", "asm", "mass_coefp", "update", "pfix", "bound", "smooth", "copy", "restv_fluxes",
                "restrict", "prol_corr", "prol_apply", "tail", "endcycle", "prol_apply_end"]
 
     def profile_cycle(self):
