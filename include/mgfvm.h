@@ -135,6 +135,17 @@ typedef struct mgfvm_options {
     int sync_every;    /* cycles between host reads of the stop flags in mgfvm_solve */
 } mgfvm_options;
 
+/* Per-level schedule choices (index = level; 0 = the engine's default).  Every choice
+ * gives the same bits; only the launch shapes change. */
+#define MGFVM_MAX_LEVELS 16
+typedef struct mgfvm_tuning {
+    int smooth_units[MGFVM_MAX_LEVELS];    /* smoother units (GS half-sweeps or Jacobi
+                                              sweeps) per tile launch, >= 1             */
+    int smooth_threads[MGFVM_MAX_LEVELS];  /* smoother CTA: 1024 (one per SM) or 512   */
+    int asm_slices[MGFVM_MAX_LEVELS];      /* assembly threads per cell: 1 or 3         */
+    int restrict_slices[MGFVM_MAX_LEVELS]; /* restriction threads per cell: 1 or 3      */
+} mgfvm_tuning;
+
 typedef struct mgfvm_ctx mgfvm_ctx;
 
 /* ------------------------------------------------------ configuration */
@@ -228,6 +239,19 @@ int mgfvm_time_op(mgfvm_ctx *ctx, int op, int level, int reps, double *ms_total,
  * kernel id, level[k] = its level.  Up to `cap` entries; *n_out = launches. */
 int mgfvm_profile_cycle(mgfvm_ctx *ctx, double *ms, int *kernel, int *level, int cap, int *n_out);
 
+/* The context's schedule choices, and replacing them (the V-cycle graph is rebuilt).
+ * Values outside the allowed sets are rejected with MGFVM_EINVAL. */
+int mgfvm_get_tuning(mgfvm_ctx *ctx, mgfvm_tuning *t);
+int mgfvm_set_tuning(mgfvm_ctx *ctx, const mgfvm_tuning *t);
+
+/* Autotuner: time V-cycles of this batch under candidate schedule choices (level by
+ * level, `cycles` graph-replayed cycles per candidate, best of two) and keep the
+ * fastest.  The batch's state is saved before and restored after, so results are as
+ * if the call had not happened.  *ms_before / *ms_after = milliseconds per cycle
+ * under the initial and the chosen schedule (either may be NULL); `chosen` may be
+ * NULL.  No counterpart in the reference. */
+int mgfvm_autotune(mgfvm_ctx *ctx, int cycles, mgfvm_tuning *chosen, double *ms_before, double *ms_after);
+
 /* Bytes this context copied host->device and device->host since it was created. */
 int mgfvm_transfer_bytes(mgfvm_ctx *ctx, long long *h2d, long long *d2h);
 
@@ -297,6 +321,13 @@ int mgfvm_masserror_f64(const double *u, const double *v, const double *areax,
                         const double *areay, double *su, double *pp, int npx,
                         int npy, double *err_out, double *partials, void *stream);
 size_t mgfvm_masserror_scratch_doubles(int npx, int npy);
+
+/* Self-test of the smoothers' division by a precomputed reciprocal (two Markstein
+ * correction steps after RN(1/b), with the IEEE division outside its safe range):
+ * n pseudo-random operand pairs from `seed` (half raw bit patterns, half values of
+ * moderate exponent) are divided both ways on `device`; *mismatches counts results
+ * whose bits differ from a / b.  No counterpart in the reference. */
+int mgfvm_check_division(int device, long long n, unsigned long long seed, long long *mismatches);
 
 /* mgfvm_masserror_f64 for callers that cannot allocate device memory (a host
  * program whose device memory another runtime owns, or a path that must not enter

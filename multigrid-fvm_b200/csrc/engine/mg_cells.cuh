@@ -286,6 +286,60 @@ __device__ __forceinline__ double gs_value(double aw, double ae, double as, doub
     return (nb + su) / ap;
 }
 
+// ------------------------------------------------------------ division by a fixed divisor
+// A smoother divides by the same ap in every unit of a launch.  The reciprocal y =
+// RN(1/b) is taken once with the IEEE division; each quotient is then finished with
+// Markstein's correction steps (P. Markstein, IBM J. Res. Develop. 34(1):111-119, 1990;
+// J.-M. Muller et al., Handbook of Floating-Point Arithmetic, 2nd ed., sec. 4.7):
+// q0 = RN(a y); r0 = a - b q0 and q1 = RN(q0 + r0 y) make q1 faithful (|q1 - a/b| <
+// ulp), so r1 = a - b q1 is exact and q2 = RN(q1 + r1 y) = RN(a/b).  The theorem needs
+// no underflow or overflow anywhere: operands outside [2^-450, 2^450] in magnitude
+// (which keeps the quotient within [2^-900, 2^900]), zero, Inf and NaN take the IEEE
+// division.  Results are therefore the bits of a / b in every case.
+struct Recip {
+    double b, y;
+    bool ok;
+};
+
+__device__ __forceinline__ Recip make_recip(double b)
+{
+    const double m = fabs(b);
+    return {b, 1.0 / b, m >= 0x1p-450 && m <= 0x1p450};
+}
+
+__device__ __forceinline__ double ieee_div(double a, double b) { return a / b; }
+
+__device__ __forceinline__ double div_by(double a, const Recip &R)
+{
+    const double m = fabs(a);
+    if (R.ok && m >= 0x1p-450 && m <= 0x1p450) {
+        const double q0 = a * R.y;
+        const double r0 = fma(-R.b, q0, a);
+        const double q1 = fma(r0, R.y, q0);
+        const double r1 = fma(-R.b, q1, a);
+        return fma(r1, R.y, q1);
+    }
+    return ieee_div(a, R.b);
+}
+
+// gs_value with the divisor's reciprocal precomputed (R = make_recip(ap))
+__device__ __forceinline__ double gs_value_r(double aw, double ae, double as, double an, const Recip &R, double su,
+                                             double pw, double pe, double ps, double pn)
+{
+    double nb = aw * pw + ae * pe + as * ps + an * pn;
+    return div_by(nb + su, R);
+}
+
+// jacobi_value with R = make_recip(ap + 1.0e-30)
+__device__ __forceinline__ double jacobi_value_r(double aw, double ae, double as, double an, const Recip &R,
+                                                 double su, double pw, double pe, double ps, double pn, double pc)
+{
+    const double wj = 1.0;
+    double nb = aw * pw + ae * pe + as * ps + an * pn;
+    double g = div_by(nb + su, R);
+    return (1.0 - wj) * pc + wj * g;
+}
+
 __device__ __forceinline__ void cell_jacobi(const LevelDev &L, int e, const double *cur, double *nxt, int q)
 {
     const int nx = L.npx;

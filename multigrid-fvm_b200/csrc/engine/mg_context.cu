@@ -54,6 +54,7 @@ struct mgfvm_ctx {
     CaseState *ds = nullptr;
     InitDev *dinit = nullptr;
     char *pool = nullptr;
+    size_t pool_bytes = 0;
     double *hist = nullptr;
     int hist_cap = 0;
     double *dprofile = nullptr;
@@ -65,7 +66,7 @@ struct mgfvm_ctx {
     std::vector<Launch> cyc;
     std::vector<int> maxcells;                // per level: max npx*npy over cases
     int last_eq[MAXLEV];                      // per level: equation of the visible coefficient set
-    int units_cap[MAXLEV] = {};               // per level: smoother units per tile launch (0: default)
+    mgfvm_tuning tune{};                      // per-level schedule choices (0: default)
     long long launches = 0;
     long long h2d = 0, d2h = 0;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -143,11 +144,13 @@ struct Builder {
             L.smem = bufs * mx * my * (int)sizeof(double);
             return;
         }
-        const int cap = x->units_cap[ig] > 0 ? x->units_cap[ig] : MAX_UNITS;
+        const int nt = x->tune.smooth_threads[ig] == SMOOTH_BLOCK / 2 ? SMOOTH_BLOCK / 2 : SMOOTH_BLOCK;
+        const int most = (smooth_pairs_side(0, nt) - MIN_TILE) / 2;   // units that leave a MIN_TILE tile
+        const int cap = std::min(most, x->tune.smooth_units[ig] > 0 ? x->tune.smooth_units[ig] : MAX_UNITS);
         int chunks = (units + cap - 1) / cap;
         if ((chunks & 1) && units >= chunks + 1) ++chunks;
         const int hmax = (units + chunks - 1) / chunks;
-        const int tile = std::max(1, smooth_pairs_side(hmax));
+        const int tile = smooth_pairs_side(hmax, nt);
         const int side = tile + 2 * hmax;
         int u0 = 0;
         for (int c = 0; c < chunks; ++c) {
@@ -155,7 +158,7 @@ struct Builder {
             Launch &L = add(K_SMOOTH, ig, mode, 0, mask, u0, nu, c & 1);
             L.a4 = tile;
             L.grid = dim3((unsigned)tiles(ig, tile), x->ncases, neq);
-            L.block = std::min(SMOOTH_BLOCK, round32(side * ((side + 1) / 2)));
+            L.block = std::min(nt, round32(side * ((side + 1) / 2)));
             L.smem = bufs * side * side * (int)sizeof(double);
             u0 += nu;
         }
@@ -212,11 +215,20 @@ struct Builder {
     // on the visit-start fluxes, so they are assembled together and smoothed in the
     // same launches; the scalar's outflow ghost moves with its equation.
     static int asm_bits(bool down) { return A_FLUX | A_U | A_V | A_SC | (down ? A_SC_OUTFLOW : 0); }
+    // Assembly and restriction run one thread per (cell, equation) — 3 slices — while a
+    // level's cells alone would not fill the GPU, one thread per cell otherwise.
+    int slices(int ig, int knob) const
+    {
+        if (knob == 1 || knob == 3) return knob;
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, x->device);
+        return (long long)x->ncases * cells(ig) < (long long)sms * 2048 ? 3 : 1;
+    }
     void step(int ig, int mode, bool down, bool reduce, bool asm_done = false)
     {
         if (!asm_done) {
             Launch &L = add(K_ASM, ig, mode, cells(ig), asm_bits(down), 1);
-            L.grid.z = 3;                       // one thread per (cell, equation)
+            L.grid.z = slices(ig, x->tune.asm_slices[ig]);
         }
         smooth(ig, mode, (1 << EQ_U) | (1 << EQ_V) | (1 << EQ_SC), x->sched.nswpm);
         const int fuse = outflow_fusable(ig, mode) ? (down ? 1 : 3) : 0;
@@ -227,9 +239,10 @@ struct Builder {
     // `coarse_asm`: also run the coarse level's down-leg assembly (see k_restrict)
     void restrict_(int ig, int mode_f, bool coarse_asm = false)
     {
-        add(K_RESTV_FLUXES, ig, mode_f, cells(ig)).grid.z = 3;
+        const int z = slices(ig, x->tune.restrict_slices[ig]);
+        add(K_RESTV_FLUXES, ig, mode_f, cells(ig)).grid.z = z;
         Launch &L = add(K_RESTRICT, ig, mode_f, cells(ig + 1), coarse_asm ? asm_bits(true) : 0);
-        L.grid.z = 3;                           // one thread per (coarse cell, equation)
+        L.grid.z = z;
     }
     // :230-233
     void prolong(int ig, int mode)
@@ -615,6 +628,7 @@ int create_impl(const mgfvm_config *cases, int ncases, const mgfvm_options *opt_
         cnt_off[c] = take(16 * sizeof(unsigned));
     }
     const size_t pool_bytes = align_up(off, 256);
+    x->pool_bytes = pool_bytes;
     cudaError_t me = cudaMalloc(&x->pool, pool_bytes);
     if (me != cudaSuccess)
         return mgfvm_fail(me == cudaErrorMemoryAllocation ? MGFVM_ENOMEM : MGFVM_ECUDA,
@@ -973,6 +987,142 @@ int mgfvm_time_op(mgfvm_ctx *x, int op, int level, int reps, double *ms_total, i
     return MGFVM_OK;
 }
 
+static bool tuning_valid(const mgfvm_tuning &t)
+{
+    for (int ig = 0; ig < MGFVM_MAX_LEVELS; ++ig) {
+        if (t.smooth_units[ig] < 0 || t.smooth_units[ig] > 64) return false;
+        if (t.smooth_threads[ig] != 0 && t.smooth_threads[ig] != SMOOTH_BLOCK && t.smooth_threads[ig] != SMOOTH_BLOCK / 2)
+            return false;
+        for (int v : {t.asm_slices[ig], t.restrict_slices[ig]})
+            if (v != 0 && v != 1 && v != 3) return false;
+    }
+    return true;
+}
+
+// Drop the captured graph and rebuild the V-cycle's launch list from x->tune.
+static void rebuild_schedule(mgfvm_ctx *x)
+{
+    if (x->gexec) cudaGraphExecDestroy(x->gexec);
+    if (x->graph) cudaGraphDestroy(x->graph);
+    x->gexec = nullptr;
+    x->graph = nullptr;
+    x->cyc.clear();
+    Builder b{x, &x->cyc};
+    b.cycle();
+}
+
+// Milliseconds per graph-replayed V-cycle (best of two runs of n), stop rule off.
+static int time_schedule(mgfvm_ctx *x, int n, double *ms)
+{
+    RC(build_graph(x));
+    CK(cudaGraphLaunch(x->gexec, x->stream));
+    double best = 1e300;
+    for (int rep = 0; rep < 2; ++rep) {
+        CK(cudaEventRecord(x->e0, x->stream));
+        for (int k = 0; k < n; ++k) CK(cudaGraphLaunch(x->gexec, x->stream));
+        CK(cudaEventRecord(x->e1, x->stream));
+        CK(cudaEventSynchronize(x->e1));
+        float t = 0;
+        CK(cudaEventElapsedTime(&t, x->e0, x->e1));
+        best = std::min(best, (double)t / n);
+    }
+    x->launches += (long long)(2 * n + 1) * (long long)x->cyc.size();
+    *ms = best;
+    return MGFVM_OK;
+}
+
+int mgfvm_get_tuning(mgfvm_ctx *x, mgfvm_tuning *t)
+{
+    RC(check_ctx(x));
+    if (!t) return mgfvm_fail(MGFVM_EINVAL, "null tuning");
+    *t = x->tune;
+    return MGFVM_OK;
+}
+
+int mgfvm_set_tuning(mgfvm_ctx *x, const mgfvm_tuning *t)
+{
+    RC(check_ctx(x));
+    if (!t || !tuning_valid(*t)) return mgfvm_fail(MGFVM_EINVAL, "tuning values outside the allowed sets");
+    x->tune = *t;
+    rebuild_schedule(x);
+    return MGFVM_OK;
+}
+
+int mgfvm_autotune(mgfvm_ctx *x, int cycles, mgfvm_tuning *chosen, double *ms_before, double *ms_after)
+{
+    RC(check_ctx(x));
+    if (cycles < 1) return mgfvm_fail(MGFVM_EINVAL, "cycles must be >= 1");
+    RC(pull(x));
+    const std::vector<CaseState> saved = x->hs;
+    char *backup = nullptr;
+    cudaError_t me = cudaMalloc(&backup, x->pool_bytes);
+    if (me != cudaSuccess)
+        return mgfvm_fail(me == cudaErrorMemoryAllocation ? MGFVM_ENOMEM : MGFVM_ECUDA,
+                          "autotune state backup of %zu bytes: %s", x->pool_bytes, cudaGetErrorString(me));
+    int rc = MGFVM_OK;
+    double t0 = 0.0, best = 0.0;
+    auto trial = [&](double *ms) -> int {
+        x->hs = saved;                  // histories and flags as before every trial
+        RC(push(x));
+        return time_schedule(x, cycles, ms);
+    };
+    do {
+        if (cudaMemcpyAsync(backup, x->pool, x->pool_bytes, cudaMemcpyDeviceToDevice, x->stream) != cudaSuccess) {
+            rc = mgfvm_fail(MGFVM_ECUDA, "autotune: state backup failed");
+            break;
+        }
+        if ((rc = set_controls(x, 0, 0.0)) != MGFVM_OK) break;
+        if ((rc = trial(&t0)) != MGFVM_OK) break;
+        best = t0;
+        Builder probe{x, nullptr};
+        // coordinate descent, level by level, one knob at a time
+        for (int ig = 0; ig < x->maxng && rc == MGFVM_OK; ++ig) {
+            std::vector<std::vector<int>> knobs;   // {kind, value0, value1}
+            int mx, my;
+            if (!probe.whole_level(ig, mx, my)) {
+                static const int opts[][2] = {{SMOOTH_BLOCK, 10}, {SMOOTH_BLOCK, 4}, {SMOOTH_BLOCK, 6}, {SMOOTH_BLOCK, 16},
+                                              {SMOOTH_BLOCK / 2, 4}, {SMOOTH_BLOCK / 2, 6}, {SMOOTH_BLOCK / 2, 10}};
+                for (auto &o : opts) knobs.push_back({0, o[0], o[1]});
+            }
+            knobs.push_back({1, 1, 0});
+            knobs.push_back({1, 3, 0});
+            if (ig + 1 < x->maxng) {
+                knobs.push_back({2, 1, 0});
+                knobs.push_back({2, 3, 0});
+            }
+            for (const auto &k : knobs) {
+                mgfvm_tuning keep = x->tune, cand = x->tune;
+                if (k[0] == 0) { cand.smooth_threads[ig] = k[1]; cand.smooth_units[ig] = k[2]; }
+                if (k[0] == 1) cand.asm_slices[ig] = k[1];
+                if (k[0] == 2) cand.restrict_slices[ig] = k[1];
+                if (memcmp(&cand, &keep, sizeof cand) == 0) continue;
+                x->tune = cand;
+                rebuild_schedule(x);
+                double t = 0.0;
+                if ((rc = trial(&t)) != MGFVM_OK) break;
+                if (t < best * 0.99) best = t;
+                else {
+                    x->tune = keep;
+                    rebuild_schedule(x);
+                }
+            }
+        }
+    } while (0);
+    // restore the batch exactly as it was
+    cudaError_t e = cudaMemcpyAsync(x->pool, backup, x->pool_bytes, cudaMemcpyDeviceToDevice, x->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(x->stream);
+    cudaFree(backup);
+    x->hs = saved;
+    const int rp = push(x);
+    if (rc != MGFVM_OK) return rc;
+    if (e != cudaSuccess) return mgfvm_fail(MGFVM_ECUDA, "autotune: state restore failed: %s", cudaGetErrorString(e));
+    if (rp != MGFVM_OK) return rp;
+    if (chosen) *chosen = x->tune;
+    if (ms_before) *ms_before = t0;
+    if (ms_after) *ms_after = best;
+    return MGFVM_OK;
+}
+
 int mgfvm_profile_cycle(mgfvm_ctx *x, double *ms, int *kernel, int *level, int cap, int *n_out)
 {
     RC(check_ctx(x));
@@ -1052,6 +1202,21 @@ int mgfvm_masserror_f64(const double *u, const double *v, const double *areax, c
     const void *p[] = {u, v, areax, areay, su, pp, err_out, partials};
     RC(check_raw(p, 8, npx, npy, npx - 1, npy - 1));
     CK(mg::raw_masserror(u, v, areax, areay, su, pp, npx, npy, err_out, partials, (cudaStream_t)stream));
+    return MGFVM_OK;
+}
+
+int mgfvm_check_division(int device, long long n, unsigned long long seed, long long *mismatches)
+{
+    if (n < 0 || !mismatches) return mgfvm_fail(MGFVM_EINVAL, "bad count or null output");
+    CK(cudaSetDevice(device));
+    unsigned long long *bad = nullptr, h = 0;
+    CK(cudaMalloc(&bad, sizeof *bad));
+    cudaError_t e = cudaMemset(bad, 0, sizeof *bad);
+    if (e == cudaSuccess) e = mg::raw_check_division(n, seed, bad, 0);
+    if (e == cudaSuccess) e = cudaMemcpy(&h, bad, sizeof h, cudaMemcpyDeviceToHost);
+    cudaFree(bad);
+    if (e != cudaSuccess) return mgfvm_fail(MGFVM_ECUDA, "division self-test: %s", cudaGetErrorString(e));
+    *mismatches = (long long)h;
     return MGFVM_OK;
 }
 

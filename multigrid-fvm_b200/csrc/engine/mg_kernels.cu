@@ -243,8 +243,8 @@ __global__ void __launch_bounds__(BLOCK) k_bound(const CaseDev *__restrict__ cs,
 // before it writes).  Every cell update is the reference's formula on the same
 // neighbour values, so the result is bit-identical to sweeping the whole level unit
 // by unit.
-template <int ISOLVE>
-__global__ void __launch_bounds__(SMOOTH_BLOCK) k_smooth(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode, int mask, int u0, int nu,
+template <int ISOLVE, int NT>
+__global__ void __launch_bounds__(NT, SMOOTH_BLOCK / NT) k_smooth(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode, int mask, int u0, int nu,
                                                          int dir, int tile)
 {
     extern __shared__ double sm[];
@@ -290,17 +290,29 @@ __global__ void __launch_bounds__(SMOOTH_BLOCK) k_smooth(const CaseDev *__restri
     const int jB = jA == jr ? jr + 1 : jr;                 // black cell
     const bool okA = own && (jA == jr || two), okB = own && (jB == jr || two);
     const int kA = (jA - ry0) * W + c, kB = (jB - ry0) * W + c;
+    // A domain cell is inside unit h's window while h <= H + its distance to the
+    // tile's nearest edge; -1 marks cells that are never updated.
+    const bool inx = i >= d.i0 && i <= dx1;
+    const int dxe = min(i - x0, x1 - i);
+    const int limA = okA && inx && jA >= d.j0 && jA <= dy1 ? H + min(dxe, min(jA - y0, y1 - jA)) : -1;
+    const int limB = okB && inx && jB >= d.j0 && jB <= dy1 ? H + min(dxe, min(jB - y0, y1 - jB)) : -1;
     double A[6] = {0, 0, 0, 0, 0, 0}, B[6] = {0, 0, 0, 0, 0, 0}, pA = 0.0, pB = 0.0;
+    const int gA = jA * npx + i, gB = jB * npx + i;
     if (okA) {
-        const size_t g = (size_t)jA * npx + i;
-        pA = src[g];
-        A[0] = gaw[g]; A[1] = gae[g]; A[2] = gas[g]; A[3] = gan[g]; A[4] = gap[g]; A[5] = gsu[g];
+        pA = src[gA];
+        A[0] = gaw[gA]; A[1] = gae[gA]; A[2] = gas[gA]; A[3] = gan[gA]; A[4] = gap[gA]; A[5] = gsu[gA];
     }
     if (okB) {
-        const size_t g = (size_t)jB * npx + i;
-        pB = src[g];
-        B[0] = gaw[g]; B[1] = gae[g]; B[2] = gas[g]; B[3] = gan[g]; B[4] = gap[g]; B[5] = gsu[g];
+        pB = src[gB];
+        B[0] = gaw[gB]; B[1] = gae[gB]; B[2] = gas[gB]; B[3] = gan[gB]; B[4] = gap[gB]; B[5] = gsu[gB];
     }
+    // written back: the tile, plus the boundary ring where the tile touches it
+    const bool outx = i >= (x0 == d.i0 ? x0 - 1 : x0) && i <= (x1 == dx1 ? x1 + 1 : x1);
+    const int oy0 = y0 == d.j0 ? y0 - 1 : y0, oy1 = y1 == dy1 ? y1 + 1 : y1;
+    const bool outA = okA && outx && jA >= oy0 && jA <= oy1, outB = okB && outx && jB >= oy0 && jB <= oy1;
+    const double eps = ISOLVE == MGFVM_JACOBI ? 1.0e-30 : 0.0;   // solver's (ap + 1e-30), solvergs' ap
+    const Recip RA = make_recip(ISOLVE == MGFVM_JACOBI ? A[4] + eps : A[4]);
+    const Recip RB = make_recip(ISOLVE == MGFVM_JACOBI ? B[4] + eps : B[4]);
     if (okA) {
         phi[kA] = pA;
         if (ISOLVE == MGFVM_JACOBI) phi2[kA] = pA;
@@ -311,37 +323,31 @@ __global__ void __launch_bounds__(SMOOTH_BLOCK) k_smooth(const CaseDev *__restri
     }
     __syncthreads();
     for (int h = 1; h <= nu; ++h) {
-        const int wx0 = max(x0 - H + h, d.i0), wx1 = min(x1 + H - h, dx1);
-        const int wy0 = max(y0 - H + h, d.j0), wy1 = min(y1 + H - h, dy1);
-        const bool inx = i >= wx0 && i <= wx1;
         if (ISOLVE == MGFVM_GAUSS_SEIDEL) {
             if (((u0 + h - 1) & 1) == 0) {
-                if (okA && inx && jA >= wy0 && jA <= wy1)
-                    phi[kA] = gs_value(A[0], A[1], A[2], A[3], A[4], A[5], phi[kA - 1], phi[kA + 1], phi[kA - W],
-                                       phi[kA + W]);
+                if (h <= limA)
+                    phi[kA] = gs_value_r(A[0], A[1], A[2], A[3], RA, A[5], phi[kA - 1], phi[kA + 1], phi[kA - W],
+                                         phi[kA + W]);
             } else {
-                if (okB && inx && jB >= wy0 && jB <= wy1)
-                    phi[kB] = gs_value(B[0], B[1], B[2], B[3], B[4], B[5], phi[kB - 1], phi[kB + 1], phi[kB - W],
-                                       phi[kB + W]);
+                if (h <= limB)
+                    phi[kB] = gs_value_r(B[0], B[1], B[2], B[3], RB, B[5], phi[kB - 1], phi[kB + 1], phi[kB - W],
+                                         phi[kB + W]);
             }
         } else {
             const double *cur = ((h - 1) & 1) ? phi2 : phi;
             double *nxt = ((h - 1) & 1) ? phi : phi2;
-            if (okA && inx && jA >= wy0 && jA <= wy1)
-                nxt[kA] = jacobi_value(A[0], A[1], A[2], A[3], A[4], A[5], cur[kA - 1], cur[kA + 1], cur[kA - W],
-                                       cur[kA + W], cur[kA]);
-            if (okB && inx && jB >= wy0 && jB <= wy1)
-                nxt[kB] = jacobi_value(B[0], B[1], B[2], B[3], B[4], B[5], cur[kB - 1], cur[kB + 1], cur[kB - W],
-                                       cur[kB + W], cur[kB]);
+            if (h <= limA)
+                nxt[kA] = jacobi_value_r(A[0], A[1], A[2], A[3], RA, A[5], cur[kA - 1], cur[kA + 1], cur[kA - W],
+                                         cur[kA + W], cur[kA]);
+            if (h <= limB)
+                nxt[kB] = jacobi_value_r(B[0], B[1], B[2], B[3], RB, B[5], cur[kB - 1], cur[kB + 1], cur[kB - W],
+                                         cur[kB + W], cur[kB]);
         }
         __syncthreads();
     }
     const double *res = (ISOLVE == MGFVM_JACOBI && (nu & 1)) ? phi2 : phi;
-    const int ox0 = x0 == d.i0 ? x0 - 1 : x0, ox1 = x1 == dx1 ? x1 + 1 : x1;
-    const int oy0 = y0 == d.j0 ? y0 - 1 : y0, oy1 = y1 == dy1 ? y1 + 1 : y1;
-    const bool outx = i >= ox0 && i <= ox1;
-    if (okA && outx && jA >= oy0 && jA <= oy1) dst[(size_t)jA * npx + i] = res[kA];
-    if (okB && outx && jB >= oy0 && jB <= oy1) dst[(size_t)jB * npx + i] = res[kB];
+    if (outA) dst[gA] = res[kA];
+    if (outB) dst[gB] = res[kB];
 }
 
 // After an odd number of smoothing launches the result sits in the ping-pong buffer.
@@ -733,10 +739,10 @@ __global__ void __launch_bounds__(TAIL_BLOCK, 1) k_tail(const CaseDev *__restric
 }
 
 // ------------------------------------------------------------- launcher
-int smooth_pairs_side(int units)
+int smooth_pairs_side(int units, int threads)
 {
     int s = 1;
-    while ((s + 1) * ((s + 2) / 2) <= SMOOTH_BLOCK) ++s;   // largest square region of <= SMOOTH_BLOCK pairs
+    while ((s + 1) * ((s + 2) / 2) <= threads) ++s;   // largest square region of <= `threads` pairs
     return s - 2 * units;
 }
 
@@ -760,10 +766,18 @@ cudaError_t launch_one(const Launch &X, const CaseDev *dc, CaseState *ds, const 
     case K_PFIX: k_pfix<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, X.a0); break;
     case K_BOUND: k_bound<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, X.a0); break;
     case K_SMOOTH:
-        if (S.isolve == MGFVM_JACOBI)
-            k_smooth<MGFVM_JACOBI><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
-        else
-            k_smooth<MGFVM_GAUSS_SEIDEL><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+        if (b > SMOOTH_BLOCK) return cudaErrorInvalidValue;
+        if (S.isolve == MGFVM_JACOBI) {
+            if (b <= SMOOTH_BLOCK / 2)
+                k_smooth<MGFVM_JACOBI, SMOOTH_BLOCK / 2><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+            else
+                k_smooth<MGFVM_JACOBI, SMOOTH_BLOCK><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+        } else {
+            if (b <= SMOOTH_BLOCK / 2)
+                k_smooth<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK / 2><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+            else
+                k_smooth<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+        }
         break;
     case K_COPY: k_copy<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, X.a0); break;
     case K_RESTV_FLUXES: k_restv_fluxes<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode); break;
@@ -885,6 +899,44 @@ cudaError_t raw_masserror(const double *u, const double *v, const double *ax, co
     const int nb = (int)raw_masserror_blocks(npx, npy);
     if (nb == 0) return cudaMemsetAsync(err_out, 0, sizeof(double), s);
     r_masserror<<<nb, BLOCK, 0, s>>>(u, v, ax, ay, su, pp, npx, npy, err_out, partials);
+    return cudaGetLastError();
+}
+
+// ----------------------------------------------- division self-test
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z)
+{
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// Operand k: even k draw raw 64-bit patterns (every exponent, subnormals, Inf, NaN,
+// signed zeros), odd k draw values with exponents in [-64, 63] like a smoother's.
+__device__ __forceinline__ double test_operand(unsigned long long seed, long long k, int which)
+{
+    const unsigned long long h = mix64(seed ^ mix64((unsigned long long)k * 2 + which));
+    if ((k & 1) == 0) return __longlong_as_double((long long)h);
+    const unsigned long long man = h & 0x000FFFFFFFFFFFFFull, sign = h & 0x8000000000000000ull;
+    const long long ex = 1023 + (long long)((h >> 52) & 127) - 64;
+    return __longlong_as_double((long long)(sign | ((unsigned long long)ex << 52) | man));
+}
+
+__global__ void r_check_division(long long n, unsigned long long seed, unsigned long long *bad)
+{
+    unsigned long long local = 0;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        const double a = test_operand(seed, k, 0), b = test_operand(seed, k, 1);
+        const double want = a / b, got = div_by(a, make_recip(b));
+        const bool same = __double_as_longlong(want) == __double_as_longlong(got) || (want != want && got != got);
+        local += same ? 0 : 1;
+    }
+    if (local) atomicAdd(bad, local);
+}
+
+cudaError_t raw_check_division(long long n, unsigned long long seed, unsigned long long *bad, cudaStream_t s)
+{
+    r_check_division<<<148 * 8, BLOCK, 0, s>>>(n, seed, bad);
     return cudaGetLastError();
 }
 

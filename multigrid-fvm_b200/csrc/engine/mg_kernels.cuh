@@ -35,11 +35,13 @@ struct Sched {
     int isolve, nswpm, nswpp;
 };
 
-// Tile smoother geometry: a CTA of at most SMOOTH_BLOCK threads, one vertical cell pair
-// per thread, covers a tile plus a halo of one cell per unit on every side.
+// Tile smoother geometry: a CTA of SMOOTH_BLOCK (one per SM) or SMOOTH_BLOCK/2 (two per
+// SM) threads, one vertical cell pair per thread, covers a tile plus a halo of one cell
+// per unit on every side.
 constexpr int SMOOTH_BLOCK = 1024;
 constexpr int MAX_UNITS = 10;   // default cap of half-sweeps (GS) or sweeps (Jacobi) per launch
-int smooth_pairs_side(int units);   // tile side whose region fits SMOOTH_BLOCK pairs
+constexpr int MIN_TILE = 8;     // smallest tile side a units cap may leave
+int smooth_pairs_side(int units, int threads);   // tile side whose region fits `threads` pairs
 
 cudaError_t launch_one(const Launch &L, const CaseDev *dcases, CaseState *dstate, const Sched &S,
                        cudaStream_t stream);
@@ -56,6 +58,7 @@ cudaError_t raw_masserror(const double *u, const double *v, const double *ax, co
                           double *su, double *pp, int npx, int npy, double *err_out,
                           double *partials, cudaStream_t s);
 size_t raw_masserror_blocks(int npx, int npy);
+cudaError_t raw_check_division(long long n, unsigned long long seed, unsigned long long *bad, cudaStream_t s);
 
 constexpr int BLOCK = 256;
 constexpr int TAIL_BLOCK = 512;

@@ -64,3 +64,15 @@ class Options(C.Structure):
     """struct mgfvm_options."""
     _fields_ = [("device", C.c_int), ("precision", C.c_int), ("tail_level", C.c_int),
                 ("use_graph", C.c_int), ("sync_every", C.c_int)]
+
+
+MAX_LEVELS = 16
+
+
+class Tuning(C.Structure):
+    """struct mgfvm_tuning: per-level schedule choices (0 = default)."""
+    _fields_ = [("smooth_units", C.c_int * MAX_LEVELS), ("smooth_threads", C.c_int * MAX_LEVELS),
+                ("asm_slices", C.c_int * MAX_LEVELS), ("restrict_slices", C.c_int * MAX_LEVELS)]
+
+    def as_dict(self):
+        return {k: list(getattr(self, k)) for k, _ in self._fields_}

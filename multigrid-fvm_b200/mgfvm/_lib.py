@@ -63,6 +63,9 @@ def lib() -> C.CDLL:
         "mgfvm_stream": (C.c_int, [_vp, C.POINTER(_vp)]),
         "mgfvm_time_op": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _dp, _ip]),
         "mgfvm_profile_cycle": (C.c_int, [_vp, _dp, _ip, _ip, C.c_int, _ip]),
+        "mgfvm_get_tuning": (C.c_int, [_vp, C.POINTER(_abi.Tuning)]),
+        "mgfvm_set_tuning": (C.c_int, [_vp, C.POINTER(_abi.Tuning)]),
+        "mgfvm_autotune": (C.c_int, [_vp, C.c_int, C.POINTER(_abi.Tuning), _dp, _dp]),
         "mgfvm_transfer_bytes": (C.c_int, [_vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
         "mgfvm_last_error": (C.c_char_p, []),
         "mgfvm_pattern_staggered": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
@@ -78,6 +81,7 @@ def lib() -> C.CDLL:
         "mgfvm_masserror_f64": (C.c_int, [_vp] * 6 + [C.c_int, C.c_int, _vp, _vp, _vp]),
         "mgfvm_masserror_scratch_doubles": (C.c_size_t, [C.c_int, C.c_int]),
         "mgfvm_masserror_f64_noalloc": (C.c_int, [_vp] * 6 + [C.c_int, C.c_int, _vp, _vp]),
+        "mgfvm_check_division": (C.c_int, [C.c_int, C.c_longlong, C.c_ulonglong, _vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -194,6 +194,33 @@ class Solver:
         return [(self.KERNELS[kid[k]], int(lvl[k]), float(ms[k])) for k in range(min(n.value, cap))]
 
     @property
+    def tuning(self) -> dict:
+        """Per-level schedule choices {smooth_units, smooth_threads, asm_slices,
+        restrict_slices} (lists of MAX_LEVELS ints, 0 = default)."""
+        t = _abi.Tuning()
+        check(self._lib.mgfvm_get_tuning(self._h, C.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, **per_level) -> None:
+        """Replace schedule choices, e.g. set_tuning(smooth_units={0: 4}, asm_slices={1: 1});
+        unspecified levels keep their values."""
+        t = _abi.Tuning()
+        check(self._lib.mgfvm_get_tuning(self._h, C.byref(t)))
+        for key, vals in per_level.items():
+            arr = getattr(t, key)
+            for lv, v in (vals.items() if isinstance(vals, dict) else enumerate(vals)):
+                arr[lv] = int(v)
+        check(self._lib.mgfvm_set_tuning(self._h, C.byref(t)))
+
+    def autotune(self, cycles: int = 5) -> Tuple[float, float, dict]:
+        """Time candidate schedules on this batch and keep the fastest; the batch's state
+        is unchanged.  Returns (ms per cycle before, after, chosen tuning)."""
+        t = _abi.Tuning()
+        a, b = C.c_double(), C.c_double()
+        check(self._lib.mgfvm_autotune(self._h, cycles, C.byref(t), C.byref(a), C.byref(b)))
+        return a.value, b.value, t.as_dict()
+
+    @property
     def transfer_bytes(self) -> Tuple[int, int]:
         """(host->device, device->host) bytes copied by this context so far."""
         a, b = C.c_longlong(), C.c_longlong()

@@ -176,3 +176,52 @@ def test_reference_stop_rule(oracle_built):
     cfg = configs.small(32, 3, convergence=1e9)
     s = Solver(cfg)
     assert int(s.solve(50)[0]) == 1
+
+
+TUNINGS = [
+    {"smooth_units": [1, 3, 2], "smooth_threads": [512, 1024, 512], "asm_slices": [1, 3, 1],
+     "restrict_slices": [3, 1, 3]},
+    {"smooth_units": [7, 5, 0], "smooth_threads": [1024, 512, 0], "asm_slices": [3, 1, 3],
+     "restrict_slices": [1, 3, 1]},
+    {"smooth_units": [16, 12, 20], "smooth_threads": [1024, 512, 1024]},
+]
+
+
+@pytest.mark.parametrize("name", ["c0_jacobi", "c0_gs", "obs64_gs", "obs64_odd_jacobi"])
+@pytest.mark.parametrize("k", range(len(TUNINGS)))
+def test_schedule_choices_bitexact(name, k, oracle_built):
+    """Every schedule choice (units per smoother launch, smoother CTA size, assembly and
+    restriction slices) gives the oracle's bits; the 64-cell cases smooth level 0 in
+    tiles."""
+    from mgfvm import configs
+    cfg = dict(small_cases(),
+               obs64_gs=configs.small(64, 3, isolve=2, ig_obs=3, sc_obs=0.2,
+                                      obstacles=[(2, 3, 2, 2), (5, 6, 4, 6), (1, 1, 7, 8)]),
+               obs64_odd_jacobi=configs.small(64, 3, isolve=1, nswpm=3, nswpp=9, ig_obs=3,
+                                              obstacles=[(3, 4, 3, 5)]))[name]
+    s, o = _pair(cfg)
+    s.set_tuning(**TUNINGS[k])
+    for n in (1, 3):
+        s.cycle(n)
+        o.cycle(n)
+        _compare(s, o, STATE, what=f"tuning {k} after +{n} cycles")
+    s.close()
+
+
+def test_autotune_keeps_state(oracle_built):
+    """The autotuner times candidates on the live batch and restores it: the next cycles
+    continue exactly where they would have."""
+    cfg = small_cases()["c0_gs"]
+    s, o = _pair(cfg)
+    s.cycle(2)
+    o.cycle(2)
+    before, after, chosen = s.autotune(2)
+    assert before > 0 and 0 < after <= before
+    assert set(chosen) == {"smooth_units", "smooth_threads", "asm_slices", "restrict_slices"}
+    _compare(s, o, STATE, what="after autotune")
+    s.cycle(3)
+    o.cycle(3)
+    _compare(s, o, STATE, what="after autotune +3 cycles")
+    es, _ = s.history(0)
+    assert len(es) == 5
+    np.testing.assert_allclose(es, o.history()[0], rtol=ERR_RTOL, atol=0)

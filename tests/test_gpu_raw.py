@@ -89,3 +89,15 @@ def test_raw_rejects_bad_extent():
     from mgfvm._abi import EINVAL
     rc = lib().mgfvm_rbgs_f64(*([C.c_void_p(0)] * 7), 10, 10, 20, 5, 2, None)
     assert rc == EINVAL
+
+
+def test_division_by_reciprocal_matches_ieee():
+    """The smoothers divide by a reciprocal taken once per cell plus two Markstein
+    correction steps; the result must carry the bits of the IEEE division on raw bit
+    patterns (every exponent, zeros, subnormals, Inf, NaN) and smoother-like values."""
+    from mgfvm._lib import lib
+    L = lib()
+    bad = C.c_longlong(-1)
+    for seed in (1, 2, 3):
+        assert L.mgfvm_check_division(0, 1 << 27, seed, C.byref(bad)) == 0
+        assert bad.value == 0
