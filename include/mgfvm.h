@@ -196,7 +196,8 @@ int mgfvm_solve(mgfvm_ctx *ctx, int max_cycles, double fp_tol, int *cycles_out);
 
 /* Per-cycle history of case `icase`: err[k] = level-0 sum |div| measured before the
  * cycle's p' correction (convergence_data, :717-724); delta[k] = the fixed-point
- * change defined above (0 for cycle 0 and when not tracked).  Either pointer may
+ * change defined above, tracked only by mgfvm_solve with fp_tol > 0 (0 for the
+ * first cycle of such a solve and for every cycle run otherwise).  Either pointer may
  * be NULL.  *n_out = cycles recorded (<= cap are copied). */
 int mgfvm_history(mgfvm_ctx *ctx, int icase, double *err, double *delta, int cap,
                   int *n_out);

@@ -215,15 +215,9 @@ struct Builder {
     // on the visit-start fluxes, so they are assembled together and smoothed in the
     // same launches; the scalar's outflow ghost moves with its equation.
     static int asm_bits(bool down) { return A_FLUX | A_U | A_V | A_SC | (down ? A_SC_OUTFLOW : 0); }
-    // Assembly and restriction run one thread per (cell, equation) — 3 slices — while a
-    // level's cells alone would not fill the GPU, one thread per cell otherwise.
-    int slices(int ig, int knob) const
-    {
-        if (knob == 1 || knob == 3) return knob;
-        int sms = 148;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, x->device);
-        return (long long)x->ncases * cells(ig) < (long long)sms * 2048 ? 3 : 1;
-    }
+    // Assembly and restriction run one thread per (cell, equation) — 3 slices, each
+    // with a third of the dependent loads — unless tuned to one thread per cell.
+    static int slices(int, int knob) { return knob == 1 ? 1 : 3; }
     void step(int ig, int mode, bool down, bool reduce, bool asm_done = false)
     {
         if (!asm_done) {

@@ -441,8 +441,35 @@ __global__ void __launch_bounds__(BLOCK) k_prol_apply(const CaseDev *__restrict_
 // rule, and prev <- current.  p sums are shifted by the previous cycle's means so a
 // uniform pressure drift does not cancel catastrophically.
 // The end-of-cycle work for level-0 cell index t of this block (see k_endcycle).
+// History entry and the reference's stop test (:247-248) when the fixed-point change is
+// not tracked: one thread per case.
+__device__ __forceinline__ void end_of_cycle_err_only(const CaseDev &C, CaseState &ST)
+{
+    const double err = ST.last_err;
+    const int k = ST.ncyc;
+    if (k < C.hist_cap) {
+        C.hist_err[k] = err;
+        C.hist_delta[k] = 0.0;
+    }
+    ST.ncyc = k + 1;
+    const bool finite = isfinite(err);
+    if (!finite) ST.status |= CASE_NONFINITE;
+    if (C.stop_enabled) {
+        if (!finite) ST.done = 1;
+        else if (err < C.convergence) { ST.done = 1; ST.status |= CASE_CONVERGED_REF; }
+    }
+    ST.have_prev = 0;
+}
+
+// The fixed-point change (four norms over level 0 and their block reduction) is
+// computed only while a solve with fp_tol > 0 runs; otherwise the cycle only records
+// its mass error.
 __device__ __forceinline__ void end_of_cycle(const CaseDev &C, CaseState &ST, int t, int nb)
 {
+    if (!(C.fp_tol > 0.0)) {
+        if (t == 0) end_of_cycle_err_only(C, ST);
+        return;
+    }
     const LevelDev &L = C.lv[0];
     const Dom d = dom_interior(L);
     const int n = d.wi * d.wj;
