@@ -3,14 +3,15 @@
 Workload (default, N=1): the obstacle-flow configuration — 256 x 256 cells, ngrid 5,
 red-black Gauss-Seidel, a seeded staggered lattice of blocks on a 16 x 16 base grid
 (porosity 0.75), both Reynolds numbers 10 and 100 solved together.  A step is one
-converged solve of those cases from the initial guess through the public API:
-reset (device init + rest_geom) and V-cycles until each case reaches the V-cycle
-fixed point (per-cycle relative change of u, v, sc and mean-free p below FP_TOL) or
-the reference's own mass-error test fires.  FP64 throughout, bit-identical to the
-reference's arithmetic.
+solve of those cases from the initial guess through the public API, as the reference
+program runs it: reset (device init + rest_geom) and V-cycles until the level-0 mass
+error falls below `convergence` or nvcycle (2000) cycles have run.  FP64 throughout,
+bit-identical to the reference's arithmetic.  The schedule (launch shapes only) is
+autotuned on the workload before timing.  The line also carries the V-cycle rate of a
+64-case batch of such cases against one case alone (`batched`).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload c1|c0|c2]
+                    [--workload c1|c0|c2] [--no-autotune] [--batch N]
 
 Multi-GPU: one process per GPU (torchrun); every rank solves its own copy of the
 workload (independent cases, no data-path collective: weak scaling); time is the max
@@ -74,8 +75,8 @@ def load_peaks():
 
 
 # DRAM bytes (read + write) per k_smooth launch of the p' smoothing on level 0, from one
-# ncu capture of `python bench.py --profile-cycles 1` (profiles/k_smooth_c1.md).
-ROOFLINE_TRAFFIC = {}
+# ncu capture of `python bench.py --profile-cycles 1` (profiles/k_smooth_obstacle256.md).
+ROOFLINE_TRAFFIC = {"c1": 7475712}
 
 
 def smoother_roofline(solver, cases, traffic=None, reps=20):
@@ -97,6 +98,30 @@ def smoother_roofline(solver, cases, traffic=None, reps=20):
             "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
             "per_launch_us": round(per_launch_ms * 1e3, 3), "launches_per_op": klaunch // reps,
             "algorithmic_bytes_per_launch": int(algo_bytes)}
+
+
+def batched_rate(nb, device, tune, cycles_per_solve, ncyc=40):
+    """V-cycle rate of `nb` obstacle-flow cases (256x256, ngrid 5, RBGS, Re alternating
+    10/100, seeded staggered lattices) in one context, against one case alone; solves/s
+    follow from the cycles one solve runs (the reference's stop rule does not fire on
+    these cases within nvcycle, so every solve runs nvcycle cycles)."""
+    from mgfvm import Solver, configs
+    out = {}
+    for label, n in (("one_case", 1), ("batch", nb)):
+        cases = [configs.c1(10.0 if k % 2 == 0 else 100.0, seed=k + 1) for k in range(n)]
+        with Solver(cases, device=device, sync_every=64) as s:
+            if tune:
+                s.autotune(3)
+            s.cycle(3)
+            s.cycle(ncyc)
+            ms = s.last_elapsed_ms / ncyc
+        out[label] = {"cases": n, "ms_per_cycle": round(ms, 4),
+                      "case_cycles_per_s": round(n / (ms / 1e3), 1),
+                      "solves_per_s": round(n / (ms / 1e3) / max(cycles_per_solve), 4)}
+    out["speedup_per_case"] = round(out["batch"]["case_cycles_per_s"] / out["one_case"]["case_cycles_per_s"], 2)
+    out["note"] = (f"{ncyc} graph-replayed V-cycles timed with CUDA events after 3 warm-up cycles; "
+                   f"solves/s = case-cycles/s / {max(cycles_per_solve)} cycles per solve")
+    return out
 
 
 # --------------------------------------------------------------- clocks
@@ -198,7 +223,7 @@ def run_reference_arm(a, rank, world):
         print(json.dumps({"impl": "reference", "unavailable": f"no converged cycle counts for {a.workload}"}))
         return
     procs = max(1, min(os.cpu_count() or 1, 64))
-    ncyc = {"c1": 8, "c0": 200}.get(a.workload, 8)
+    ncyc = {"c1": 30, "c0": 400}.get(a.workload, 20)
     vals = []
     for s in range(a.warmup + a.steps):
         v, kind, wall, tcyc = cpu_sample(cases, ctc, ncyc, procs)
@@ -229,6 +254,9 @@ def main():
     ap.add_argument("--workload", default="c1", choices=["c1", "c0", "c2"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tail", type=int, default=-1, help="first level of the one-CTA coarse kernel (-1 auto)")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the engine's default schedule")
+    ap.add_argument("--batch", type=int, default=64,
+                    help="cases of the batched obstacle-flow measurement (0: skip it)")
     ap.add_argument("--profile-cycles", type=int, default=0,
                     help="only run 3 warm-up V-cycles then this many V-cycles of the workload "
                          "(for ncu launch lists) and exit")
@@ -252,10 +280,16 @@ def main():
     cases, desc = workload(a.workload)
     n_cases = len(cases)
     solver = Solver(cases, device=local, sync_every=64, tail_level=a.tail)
+    tuned = None
+    if not a.no_autotune:
+        t_before, t_after, tuned = solver.autotune(5)
+        log(f"autotune: {t_before * 1e3:.1f} -> {t_after * 1e3:.1f} us per cycle")
     if a.profile_cycles:
         solver.cycle(3)
         n0 = solver.kernel_launches
+        torch.cuda.nvtx.range_push("profile")     # ncu --nvtx --nvtx-include profile/
         solver.cycle(a.profile_cycles)
+        torch.cuda.nvtx.range_pop()
         nprof = solver.kernel_launches - n0
         solver.cycle(20)
         log(f"20 cycles: {solver.last_elapsed_ms / 20:.3f} ms per cycle (tail {a.tail})")
@@ -322,6 +356,8 @@ def main():
         h2d = d2h = 0
         for _ in range(max(1, a.steps)):
             with Solver(cases, device=local) as s2:
+                if tuned:
+                    s2.set_tuning(**tuned)
                 s2.solve(max(c.nvcycle for c in cases), FP_TOL)
                 for k in range(n_cases):
                     for f in ("u", "v", "p", "sc"):
@@ -338,6 +374,11 @@ def main():
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             e2e["value"] = n_cases * max(1, a.steps) * world / float(t.item())
 
+    # ---- batched throughput: many obstacle-flow cases in one context
+    batched = None
+    if a.batch > 0 and a.workload == "c1":
+        batched = batched_rate(a.batch, local, not a.no_autotune, cycles_per_solve)
+
     # ---- parity spot check at full size: 3 cycles against the CPU oracle
     l2err = None
     cpu = None
@@ -351,7 +392,7 @@ def main():
             l2err = max(float(np.linalg.norm(s3.field(0, 0, f) - o.get(0, f)) /
                               max(np.linalg.norm(o.get(0, f)), 1e-300)) for f in ("u", "v", "p", "sc"))
         ctc = cycles_per_solve
-        v, kind, wall, tcyc = cpu_sample(cases, ctc, {"c1": 8, "c0": 200}.get(a.workload, 4),
+        v, kind, wall, tcyc = cpu_sample(cases, ctc, {"c1": 30, "c0": 400}.get(a.workload, 20),
                                          max(1, min(os.cpu_count() or 1, 64)))
         cpu = {"value": v, "unit": "solves/s", "cores": max(1, min(os.cpu_count() or 1, 64)), "kind": kind,
                "sample": f"V-cycles timed per host process ({wall:.1f} s wall), one case per process, "
@@ -371,6 +412,9 @@ def main():
             "cell_sweeps_per_s": cell_sweeps_per_s,
             "l2_rel_err_vs_oracle_3cycles": l2err,
             "roofline": roofline,
+            "batched": batched,
+            "schedule": {"autotuned": tuned is not None,
+                         "tuning": {k: v[:max(c.ngrid for c in cases)] for k, v in tuned.items()} if tuned else None},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": int(launches),
