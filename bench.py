@@ -115,13 +115,43 @@ def batched_rate(nb, device, tune, cycles_per_solve, ncyc=40):
             s.cycle(3)
             s.cycle(ncyc)
             ms = s.last_elapsed_ms / ncyc
-        out[label] = {"cases": n, "ms_per_cycle": round(ms, 4),
-                      "case_cycles_per_s": round(n / (ms / 1e3), 1),
-                      "solves_per_s": round(n / (ms / 1e3) / max(cycles_per_solve), 4)}
+            out[label] = {"cases": n, "ms_per_cycle": round(ms, 4),
+                          "case_cycles_per_s": round(n / (ms / 1e3), 1),
+                          "solves_per_s": round(n / (ms / 1e3) / max(cycles_per_solve), 4)}
+            if n > 1:   # level-0 fields of the batch exceed L2: the smoother against HBM
+                out[label]["smoother_roofline"] = smoother_roofline(s, cases, ROOFLINE_TRAFFIC.get(f"c1x{n}"))
     out["speedup_per_case"] = round(out["batch"]["case_cycles_per_s"] / out["one_case"]["case_cycles_per_s"], 2)
     out["note"] = (f"{ncyc} graph-replayed V-cycles timed with CUDA events after 3 warm-up cycles; "
                    f"solves/s = case-cycles/s / {max(cycles_per_solve)} cycles per solve")
     return out
+
+
+def mixed_solve(cases, device, ref_solver, tune):
+    """One solve of the workload with MGFVM_PREC_MIXED (FP32 correction smoothing
+    against FP64 residuals), timed like a bench step, and the relative L2 distance of
+    its final fields to the FP64 solve's (`ref_solver` holds the FP64 result; p
+    compared mean-free over the interior, its level being arbitrary)."""
+    import torch
+    from mgfvm import Solver
+    with Solver(cases, device=device, precision="mixed", sync_every=64) as s:
+        if tune:
+            s.autotune(3)
+        s.solve(20, FP_TOL)
+        s.reset()
+        torch.cuda.synchronize()
+        s.solve(max(c.nvcycle for c in cases), FP_TOL)
+        ms = s.last_elapsed_ms
+        err = 0.0
+        for k in range(len(cases)):
+            for f in ("u", "v", "sc"):
+                a, b = s.field(k, 0, f), ref_solver.field(k, 0, f)
+                err = max(err, float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)))
+            a, b = s.field(k, 0, "p")[1:-1, 1:-1], ref_solver.field(k, 0, "p")[1:-1, 1:-1]
+            a, b = a - a.mean(), b - b.mean()
+            err = max(err, float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)))
+    return {"value": round(len(cases) / (ms / 1e3), 4), "unit": "solves/s", "ms_per_step": round(ms, 3),
+            "rel_l2_vs_fp64_solve": err,
+            "form": "smoothers iterate an FP32 correction against FP64 residuals; the rest FP64"}
 
 
 # --------------------------------------------------------------- clocks
@@ -374,6 +404,11 @@ def main():
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             e2e["value"] = n_cases * max(1, a.steps) * world / float(t.item())
 
+    # ---- mixed precision: the same solve with FP32 correction smoothing
+    mixed = None
+    if world == 1:
+        mixed = mixed_solve(cases, local, solver, tuned is not None)
+
     # ---- batched throughput: many obstacle-flow cases in one context
     batched = None
     if a.batch > 0 and a.workload == "c1":
@@ -413,6 +448,7 @@ def main():
             "l2_rel_err_vs_oracle_3cycles": l2err,
             "roofline": roofline,
             "batched": batched,
+            "mixed": mixed,
             "schedule": {"autotuned": tuned is not None,
                          "tuning": {k: v[:max(c.ngrid for c in cases)] for k, v in tuned.items()} if tuned else None},
             "cpu_baseline": cpu,

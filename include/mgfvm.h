@@ -84,7 +84,10 @@ enum { MGFVM_JACOBI = 1, MGFVM_GAUSS_SEIDEL = 2 };
 /* Arithmetic of the V-cycle. */
 enum mgfvm_precision {
     MGFVM_PREC_FP64 = 0,   /* every array and every operation in FP64, as the reference */
-    MGFVM_PREC_MIXED = 1   /* FP32 smoothing/transfers, FP64 defect, norms and coarsest level */
+    MGFVM_PREC_MIXED = 1   /* the smoothers iterate an FP32 correction against an FP64
+                              residual taken at the start of every smoother launch; the
+                              coarsest level, assembly, transfers, defects and norms stay
+                              FP64, so fixed points are those of the FP64 equations      */
 };
 
 #define MGFVM_MAX_PORTS 10   /* inlet/outlet arrays of the reference hold 10 (:29, :38) */

@@ -124,6 +124,12 @@ struct Builder {
         return mx > 0 && mx * ((my + 1) / 2) <= SMOOTH_BLOCK;
     }
     static int round32(int n) { return std::max(32, (n + 31) / 32 * 32); }
+    int min_ngrid() const
+    {
+        int m = MAXLEV;
+        for (const mgfvm_config &c : x->cfg) m = std::min(m, c.ngrid);
+        return m;
+    }
     // `nsw` sweeps of the equations in `mask`.  A level that fits one CTA runs every
     // unit (half-sweep of red-black GS, sweep of Jacobi) in one in-place launch;
     // otherwise the units go in an even number of tile launches of at most the level's
@@ -135,13 +141,20 @@ struct Builder {
         if (units <= 0 || (isolve != MGFVM_JACOBI && isolve != MGFVM_GAUSS_SEIDEL)) return;
         const int neq = __builtin_popcount((unsigned)mask);
         const int bufs = isolve == MGFVM_JACOBI ? 2 : 1;
+        // mixed precision: FP32 correction smoothing on every level but the coarsest
+        const bool mixed = x->opt.precision == MGFVM_PREC_MIXED && ig < min_ngrid() - 1;
+        const int kern = mixed ? K_SMOOTH_MIXED : K_SMOOTH;
+        auto smem_for = [&](int cells) {
+            return mixed ? cells * (int)sizeof(double) + bufs * cells * (int)sizeof(float)
+                         : bufs * cells * (int)sizeof(double);
+        };
         int mx, my;
         if (whole_level(ig, mx, my)) {
-            Launch &L = add(K_SMOOTH, ig, mode, 0, mask, 0, units, 2);
+            Launch &L = add(kern, ig, mode, 0, mask, 0, units, 2);
             L.a4 = std::max(mx, my);
             L.grid = dim3(1, x->ncases, neq);
             L.block = round32(mx * ((my + 1) / 2));
-            L.smem = bufs * mx * my * (int)sizeof(double);
+            L.smem = smem_for(mx * my);
             return;
         }
         const int nt = x->tune.smooth_threads[ig] == SMOOTH_BLOCK / 2 ? SMOOTH_BLOCK / 2 : SMOOTH_BLOCK;
@@ -155,11 +168,11 @@ struct Builder {
         int u0 = 0;
         for (int c = 0; c < chunks; ++c) {
             const int nu = units / chunks + (c < units % chunks ? 1 : 0);
-            Launch &L = add(K_SMOOTH, ig, mode, 0, mask, u0, nu, c & 1);
+            Launch &L = add(kern, ig, mode, 0, mask, u0, nu, c & 1);
             L.a4 = tile;
             L.grid = dim3((unsigned)tiles(ig, tile), x->ncases, neq);
             L.block = std::min(nt, round32(side * ((side + 1) / 2)));
-            L.smem = bufs * side * side * (int)sizeof(double);
+            L.smem = smem_for(side * side);
             u0 += nu;
         }
         if (chunks & 1) {
@@ -550,8 +563,8 @@ int create_impl(const mgfvm_config *cases, int ncases, const mgfvm_options *opt_
     mgfvm_options opt;
     if (opt_in) opt = *opt_in; else mgfvm_options_default(&opt);
     if (opt.sync_every < 1) opt.sync_every = 1;
-    if (opt.precision != MGFVM_PREC_FP64)
-        return mgfvm_fail(MGFVM_EUNSUPPORTED, "precision %d not available in this build", opt.precision);
+    if (opt.precision != MGFVM_PREC_FP64 && opt.precision != MGFVM_PREC_MIXED)
+        return mgfvm_fail(MGFVM_EINVAL, "unknown precision %d", opt.precision);
     x->opt = opt;
     x->device = opt.device;
     x->ncases = ncases;

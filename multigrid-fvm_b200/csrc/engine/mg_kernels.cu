@@ -230,19 +230,76 @@ __global__ void __launch_bounds__(BLOCK) k_bound(const CaseDev *__restrict__ cs,
     bound_block(C, C.lv[ig], bits);
 }
 
+// Geometry of one smoother CTA (blockIdx.x picks a tile x tile block of equation e's
+// sweep domain): the tile, the region it stages (the tile plus a halo of `nu` cells,
+// clipped at the domain's boundary ring), and this thread's vertical pair of cells,
+// one of each colour (A red: i+j even, B black).
+struct PairTile {
+    Dom d;
+    int x0, y0, x1, y1, dx1, dy1, rx0, ry0, W, Hh, npairs;
+    int i, jA, jB, kA, kB, gA, gB;
+    int limA, limB;      // a domain cell is inside unit h's window while h <= lim (-1: never)
+    bool okA, okB;       // the cell lies in the staged region
+    bool outA, outB;     // written back: the tile, plus the boundary ring where it touches it
+};
+
+// 0: this CTA has work, 1: it has none, 2: the launch is too small for its region.
+__device__ __forceinline__ int pair_tile(const LevelDev &L, int e, int nu, int tile, PairTile &P)
+{
+    P.d = dom_eq(L, e);
+    const Dom &d = P.d;
+    if (d.wi <= 0 || d.wj <= 0) return 1;
+    const int tx_n = (d.wi + tile - 1) / tile, ty_n = (d.wj + tile - 1) / tile;
+    if ((int)blockIdx.x >= tx_n * ty_n) return 1;
+    const int tx = blockIdx.x % tx_n, ty = blockIdx.x / tx_n;
+    P.dx1 = d.i0 + d.wi - 1;
+    P.dy1 = d.j0 + d.wj - 1;
+    P.x0 = d.i0 + tx * tile;
+    P.y0 = d.j0 + ty * tile;
+    P.x1 = min(P.x0 + tile - 1, P.dx1);
+    P.y1 = min(P.y0 + tile - 1, P.dy1);
+    const int H = nu;
+    P.rx0 = max(P.x0 - H, d.i0 - 1);
+    P.ry0 = max(P.y0 - H, d.j0 - 1);
+    P.W = min(P.x1 + H, P.dx1 + 1) - P.rx0 + 1;
+    P.Hh = min(P.y1 + H, P.dy1 + 1) - P.ry0 + 1;
+    P.npairs = P.W * ((P.Hh + 1) >> 1);
+    if (P.npairs > (int)blockDim.x) return 2;
+    const int W = P.W, t = threadIdx.x;
+    const bool own = t < P.npairs;
+    const int c = own ? t % W : 0, r = own ? 2 * (t / W) : 0;
+    const int i = P.rx0 + c, jr = P.ry0 + r;
+    const bool two = own && r + 1 < P.Hh;
+    P.i = i;
+    P.jA = ((i + jr) & 1) == 0 ? jr : jr + 1;
+    P.jB = P.jA == jr ? jr + 1 : jr;
+    P.okA = own && (P.jA == jr || two);
+    P.okB = own && (P.jB == jr || two);
+    P.kA = (P.jA - P.ry0) * W + c;
+    P.kB = (P.jB - P.ry0) * W + c;
+    P.gA = P.jA * L.npx + i;
+    P.gB = P.jB * L.npx + i;
+    const bool inx = i >= d.i0 && i <= P.dx1;
+    const int dxe = min(i - P.x0, P.x1 - i);
+    P.limA = P.okA && inx && P.jA >= d.j0 && P.jA <= P.dy1 ? H + min(dxe, min(P.jA - P.y0, P.y1 - P.jA)) : -1;
+    P.limB = P.okB && inx && P.jB >= d.j0 && P.jB <= P.dy1 ? H + min(dxe, min(P.jB - P.y0, P.y1 - P.jB)) : -1;
+    const bool outx = i >= (P.x0 == d.i0 ? P.x0 - 1 : P.x0) && i <= (P.x1 == P.dx1 ? P.x1 + 1 : P.x1);
+    const int oy0 = P.y0 == d.j0 ? P.y0 - 1 : P.y0, oy1 = P.y1 == P.dy1 ? P.y1 + 1 : P.y1;
+    P.outA = P.okA && outx && P.jA >= oy0 && P.jA <= oy1;
+    P.outB = P.okB && outx && P.jB >= oy0 && P.jB <= oy1;
+    return 0;
+}
+
 // Temporal-blocked smoother.  blockIdx.z picks an equation of `mask`, blockIdx.x a
-// tile x tile block of its sweep domain.  The CTA stages the tile plus a halo of `nu`
-// cells (clipped at the domain's boundary ring): every thread owns one vertical pair
-// of cells, one of each colour, holds both cells' six coefficients in registers and
-// their field values in shared memory, so a half-sweep is one update per thread.  It
-// runs `nu` units — half-sweeps of red-black Gauss-Seidel (colour of global unit
-// u0+h-1: even = red, i+j even) or Jacobi sweeps — each on a window one cell narrower
-// on every cut side, then writes the tile (plus the boundary ring where the tile
-// touches it): dir 0 from the field to the equation's ping-pong buffer, dir 1 the
-// reverse, dir 2 in place (a single tile covering the domain: it reads everything
-// before it writes).  Every cell update is the reference's formula on the same
-// neighbour values, so the result is bit-identical to sweeping the whole level unit
-// by unit.
+// tile.  The CTA stages its region: every thread owns one vertical pair of cells,
+// holds both cells' six coefficients in registers and their field values in shared
+// memory, so a half-sweep is one update per thread.  It runs `nu` units — half-sweeps
+// of red-black Gauss-Seidel (colour of global unit u0+h-1: even = red) or Jacobi
+// sweeps — each on a window one cell narrower on every cut side, then writes the tile
+// back: dir 0 from the field to the equation's ping-pong buffer, dir 1 the reverse,
+// dir 2 in place (a single tile covering the domain: it reads everything before it
+// writes).  Every cell update is the reference's formula on the same neighbour values,
+// so the result is bit-identical to sweeping the whole level unit by unit.
 template <int ISOLVE, int NT>
 __global__ void __launch_bounds__(NT, SMOOTH_BLOCK / NT) k_smooth(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode, int mask, int u0, int nu,
                                                          int dir, int tile)
@@ -252,72 +309,43 @@ __global__ void __launch_bounds__(NT, SMOOTH_BLOCK / NT) k_smooth(const CaseDev 
     if (!case_active(C, st[blockIdx.y], ig, mode)) return;
     const int e = nth_eq(mask, blockIdx.z);
     const LevelDev &L = C.lv[ig];
-    const Dom d = dom_eq(L, e);
-    if (d.wi <= 0 || d.wj <= 0) return;
-    const int tx_n = (d.wi + tile - 1) / tile, ty_n = (d.wj + tile - 1) / tile;
-    if ((int)blockIdx.x >= tx_n * ty_n) return;
-    const int tx = blockIdx.x % tx_n, ty = blockIdx.x / tx_n;
-    const int dx1 = d.i0 + d.wi - 1, dy1 = d.j0 + d.wj - 1;
-    const int x0 = d.i0 + tx * tile, y0 = d.j0 + ty * tile;
-    const int x1 = min(x0 + tile - 1, dx1), y1 = min(y0 + tile - 1, dy1);
-    const int H = nu;
-    const int rx0 = max(x0 - H, d.i0 - 1), rx1 = min(x1 + H, dx1 + 1);
-    const int ry0 = max(y0 - H, d.j0 - 1), ry1 = min(y1 + H, dy1 + 1);
-    const int W = rx1 - rx0 + 1, Hh = ry1 - ry0 + 1;
-    const int npairs = W * ((Hh + 1) >> 1);
-    if (npairs > (int)blockDim.x) {     // the schedule sizes blocks to fit; never taken
+    PairTile P;
+    const int g = pair_tile(L, e, nu, tile, P);
+    if (g == 1) return;
+    if (g == 2) {     // the schedule sizes blocks to fit; never taken
         if (threadIdx.x == 0) atomicOr(&st[blockIdx.y].status, (int)CASE_BAD_LAUNCH);
         return;
     }
-    const int npx = L.npx;
+    const int W = P.W, kA = P.kA, kB = P.kB, limA = P.limA, limB = P.limB;
     const int fs = eq_field(e), ts = eq_tmp(e);
     const double *src = L.f[dir == 1 ? ts : fs];
     double *dst = L.f[dir == 0 ? ts : fs];
-    double *phi = sm, *phi2 = sm + W * Hh;
+    double *phi = sm, *phi2 = sm + W * P.Hh;
     const double *__restrict__ gaw = L.f[co_slot(e, CK_AW)];
     const double *__restrict__ gae = L.f[co_slot(e, CK_AE)];
     const double *__restrict__ gas = L.f[co_slot(e, CK_AS)];
     const double *__restrict__ gan = L.f[co_slot(e, CK_AN)];
     const double *__restrict__ gap = L.f[co_slot(e, CK_AP)];
     const double *__restrict__ gsu = L.f[co_slot(e, CK_SU)];
-
-    const int t = threadIdx.x;
-    const bool own = t < npairs;
-    const int c = own ? t % W : 0, r = own ? 2 * (t / W) : 0;
-    const int i = rx0 + c, jr = ry0 + r;                   // the pair (i, jr), (i, jr + 1)
-    const bool two = own && r + 1 < Hh;
-    const int jA = ((i + jr) & 1) == 0 ? jr : jr + 1;      // red cell
-    const int jB = jA == jr ? jr + 1 : jr;                 // black cell
-    const bool okA = own && (jA == jr || two), okB = own && (jB == jr || two);
-    const int kA = (jA - ry0) * W + c, kB = (jB - ry0) * W + c;
-    // A domain cell is inside unit h's window while h <= H + its distance to the
-    // tile's nearest edge; -1 marks cells that are never updated.
-    const bool inx = i >= d.i0 && i <= dx1;
-    const int dxe = min(i - x0, x1 - i);
-    const int limA = okA && inx && jA >= d.j0 && jA <= dy1 ? H + min(dxe, min(jA - y0, y1 - jA)) : -1;
-    const int limB = okB && inx && jB >= d.j0 && jB <= dy1 ? H + min(dxe, min(jB - y0, y1 - jB)) : -1;
     double A[6] = {0, 0, 0, 0, 0, 0}, B[6] = {0, 0, 0, 0, 0, 0}, pA = 0.0, pB = 0.0;
-    const int gA = jA * npx + i, gB = jB * npx + i;
-    if (okA) {
-        pA = src[gA];
-        A[0] = gaw[gA]; A[1] = gae[gA]; A[2] = gas[gA]; A[3] = gan[gA]; A[4] = gap[gA]; A[5] = gsu[gA];
+    if (P.okA) {
+        const int g0 = P.gA;
+        pA = src[g0];
+        A[0] = gaw[g0]; A[1] = gae[g0]; A[2] = gas[g0]; A[3] = gan[g0]; A[4] = gap[g0]; A[5] = gsu[g0];
     }
-    if (okB) {
-        pB = src[gB];
-        B[0] = gaw[gB]; B[1] = gae[gB]; B[2] = gas[gB]; B[3] = gan[gB]; B[4] = gap[gB]; B[5] = gsu[gB];
+    if (P.okB) {
+        const int g0 = P.gB;
+        pB = src[g0];
+        B[0] = gaw[g0]; B[1] = gae[g0]; B[2] = gas[g0]; B[3] = gan[g0]; B[4] = gap[g0]; B[5] = gsu[g0];
     }
-    // written back: the tile, plus the boundary ring where the tile touches it
-    const bool outx = i >= (x0 == d.i0 ? x0 - 1 : x0) && i <= (x1 == dx1 ? x1 + 1 : x1);
-    const int oy0 = y0 == d.j0 ? y0 - 1 : y0, oy1 = y1 == dy1 ? y1 + 1 : y1;
-    const bool outA = okA && outx && jA >= oy0 && jA <= oy1, outB = okB && outx && jB >= oy0 && jB <= oy1;
     const double eps = ISOLVE == MGFVM_JACOBI ? 1.0e-30 : 0.0;   // solver's (ap + 1e-30), solvergs' ap
     const Recip RA = make_recip(ISOLVE == MGFVM_JACOBI ? A[4] + eps : A[4]);
     const Recip RB = make_recip(ISOLVE == MGFVM_JACOBI ? B[4] + eps : B[4]);
-    if (okA) {
+    if (P.okA) {
         phi[kA] = pA;
         if (ISOLVE == MGFVM_JACOBI) phi2[kA] = pA;
     }
-    if (okB) {
+    if (P.okB) {
         phi[kB] = pB;
         if (ISOLVE == MGFVM_JACOBI) phi2[kB] = pB;
     }
@@ -346,8 +374,99 @@ __global__ void __launch_bounds__(NT, SMOOTH_BLOCK / NT) k_smooth(const CaseDev 
         __syncthreads();
     }
     const double *res = (ISOLVE == MGFVM_JACOBI && (nu & 1)) ? phi2 : phi;
-    if (outA) dst[gA] = res[kA];
-    if (outB) dst[gB] = res[kB];
+    if (P.outA) dst[P.gA] = res[kA];
+    if (P.outB) dst[P.gB] = res[kB];
+}
+
+// Mixed-precision variant (MGFVM_PREC_MIXED): the same tiles, units and windows, run
+// on the correction delta of A (phi + delta) = b in FP32.  The residual r = su +
+// sum a_nb phi_nb - ap phi_P is taken in FP64 from the staged field at the start of
+// every launch (so a smoothing call of several launches refreshes it in FP64); the
+// units then update delta_P = (sum a_nb delta_nb + r) / ap in FP32, dividing by a
+// reciprocal taken once, and the tile is written back as phi + delta.  A fixed point
+// of the V-cycle is therefore one of the FP64 equations: delta vanishes only where the
+// FP64 residual does.
+template <int ISOLVE, int NT>
+__global__ void __launch_bounds__(NT, SMOOTH_BLOCK / NT) k_smooth_mixed(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode, int mask,
+                                                               int u0, int nu, int dir, int tile)
+{
+    extern __shared__ double sm[];
+    const CaseDev &C = cs[blockIdx.y];
+    if (!case_active(C, st[blockIdx.y], ig, mode)) return;
+    const int e = nth_eq(mask, blockIdx.z);
+    const LevelDev &L = C.lv[ig];
+    PairTile P;
+    const int g = pair_tile(L, e, nu, tile, P);
+    if (g == 1) return;
+    if (g == 2) {
+        if (threadIdx.x == 0) atomicOr(&st[blockIdx.y].status, (int)CASE_BAD_LAUNCH);
+        return;
+    }
+    const int W = P.W, R = P.W * P.Hh, kA = P.kA, kB = P.kB, limA = P.limA, limB = P.limB;
+    const int fs = eq_field(e), ts = eq_tmp(e);
+    const double *src = L.f[dir == 1 ? ts : fs];
+    double *dst = L.f[dir == 0 ? ts : fs];
+    double *phi = sm;
+    float *del = reinterpret_cast<float *>(sm + R), *del2 = del + R;
+    const double *__restrict__ gaw = L.f[co_slot(e, CK_AW)];
+    const double *__restrict__ gae = L.f[co_slot(e, CK_AE)];
+    const double *__restrict__ gas = L.f[co_slot(e, CK_AS)];
+    const double *__restrict__ gan = L.f[co_slot(e, CK_AN)];
+    const double *__restrict__ gap = L.f[co_slot(e, CK_AP)];
+    const double *__restrict__ gsu = L.f[co_slot(e, CK_SU)];
+    double A[6] = {0, 0, 0, 0, 0, 0}, B[6] = {0, 0, 0, 0, 0, 0}, pA = 0.0, pB = 0.0;
+    if (P.okA) {
+        const int g0 = P.gA;
+        pA = src[g0];
+        A[0] = gaw[g0]; A[1] = gae[g0]; A[2] = gas[g0]; A[3] = gan[g0]; A[4] = gap[g0]; A[5] = gsu[g0];
+    }
+    if (P.okB) {
+        const int g0 = P.gB;
+        pB = src[g0];
+        B[0] = gaw[g0]; B[1] = gae[g0]; B[2] = gas[g0]; B[3] = gan[g0]; B[4] = gap[g0]; B[5] = gsu[g0];
+    }
+    const double eps = ISOLVE == MGFVM_JACOBI ? 1.0e-30 : 0.0;
+    if (P.okA) { phi[kA] = pA; del[kA] = 0.0f; if (ISOLVE == MGFVM_JACOBI) del2[kA] = 0.0f; }
+    if (P.okB) { phi[kB] = pB; del[kB] = 0.0f; if (ISOLVE == MGFVM_JACOBI) del2[kB] = 0.0f; }
+    __syncthreads();
+    // FP64 residuals of the cells this launch updates, then the FP32 operator
+    float fA[5] = {0, 0, 0, 0, 0}, fB[5] = {0, 0, 0, 0, 0}, rA = 0.0f, rB = 0.0f;
+    if (limA >= 1) {
+        const double apA = A[4] + eps;
+        const double nb = A[0] * phi[kA - 1] + A[1] * phi[kA + 1] + A[2] * phi[kA - W] + A[3] * phi[kA + W];
+        rA = (float)((nb + A[5]) - apA * pA);
+        fA[0] = (float)A[0]; fA[1] = (float)A[1]; fA[2] = (float)A[2]; fA[3] = (float)A[3];
+        fA[4] = (float)(1.0 / apA);
+    }
+    if (limB >= 1) {
+        const double apB = B[4] + eps;
+        const double nb = B[0] * phi[kB - 1] + B[1] * phi[kB + 1] + B[2] * phi[kB - W] + B[3] * phi[kB + W];
+        rB = (float)((nb + B[5]) - apB * pB);
+        fB[0] = (float)B[0]; fB[1] = (float)B[1]; fB[2] = (float)B[2]; fB[3] = (float)B[3];
+        fB[4] = (float)(1.0 / apB);
+    }
+    for (int h = 1; h <= nu; ++h) {
+        if (ISOLVE == MGFVM_GAUSS_SEIDEL) {
+            if (((u0 + h - 1) & 1) == 0) {
+                if (h <= limA)
+                    del[kA] = (fA[0] * del[kA - 1] + fA[1] * del[kA + 1] + fA[2] * del[kA - W] + fA[3] * del[kA + W] + rA) * fA[4];
+            } else {
+                if (h <= limB)
+                    del[kB] = (fB[0] * del[kB - 1] + fB[1] * del[kB + 1] + fB[2] * del[kB - W] + fB[3] * del[kB + W] + rB) * fB[4];
+            }
+        } else {
+            const float *cur = ((h - 1) & 1) ? del2 : del;
+            float *nxt = ((h - 1) & 1) ? del : del2;
+            if (h <= limA)
+                nxt[kA] = (fA[0] * cur[kA - 1] + fA[1] * cur[kA + 1] + fA[2] * cur[kA - W] + fA[3] * cur[kA + W] + rA) * fA[4];
+            if (h <= limB)
+                nxt[kB] = (fB[0] * cur[kB - 1] + fB[1] * cur[kB + 1] + fB[2] * cur[kB - W] + fB[3] * cur[kB + W] + rB) * fB[4];
+        }
+        __syncthreads();
+    }
+    const float *res = (ISOLVE == MGFVM_JACOBI && (nu & 1)) ? del2 : del;
+    if (P.outA) dst[P.gA] = limA >= 1 ? pA + (double)res[kA] : pA;
+    if (P.outB) dst[P.gB] = limB >= 1 ? pB + (double)res[kB] : pB;
 }
 
 // After an odd number of smoothing launches the result sits in the ping-pong buffer.
@@ -804,6 +923,20 @@ cudaError_t launch_one(const Launch &X, const CaseDev *dc, CaseState *ds, const 
                 k_smooth<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK / 2><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
             else
                 k_smooth<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+        }
+        break;
+    case K_SMOOTH_MIXED:
+        if (b > SMOOTH_BLOCK) return cudaErrorInvalidValue;
+        if (S.isolve == MGFVM_JACOBI) {
+            if (b <= SMOOTH_BLOCK / 2)
+                k_smooth_mixed<MGFVM_JACOBI, SMOOTH_BLOCK / 2><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+            else
+                k_smooth_mixed<MGFVM_JACOBI, SMOOTH_BLOCK><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+        } else {
+            if (b <= SMOOTH_BLOCK / 2)
+                k_smooth_mixed<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK / 2><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+            else
+                k_smooth_mixed<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
         }
         break;
     case K_COPY: k_copy<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, X.a0); break;

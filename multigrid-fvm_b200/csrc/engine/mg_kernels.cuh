@@ -18,7 +18,9 @@ enum KernelId {
     K_RESTV_FLUXES,  // restv + fine fluxes
     K_RESTRICT,      // restr{u,v,sc} + coarse fluxes
     K_PROL_CORR, K_PROL_APPLY,
-    K_TAIL, K_ENDCYCLE, K_PROL_APPLY_END, K_NKERNELS
+    K_TAIL, K_ENDCYCLE, K_PROL_APPLY_END,
+    K_SMOOTH_MIXED,  // as K_SMOOTH, FP32 correction smoothing with an FP64 residual
+    K_NKERNELS
 };
 
 struct Launch {
