@@ -144,7 +144,8 @@ typedef struct mgfvm_options {
 typedef struct mgfvm_tuning {
     int smooth_units[MGFVM_MAX_LEVELS];    /* smoother units (GS half-sweeps or Jacobi
                                               sweeps) per tile launch, >= 1             */
-    int smooth_threads[MGFVM_MAX_LEVELS];  /* smoother CTA: 1024 (one per SM) or 512   */
+    int smooth_threads[MGFVM_MAX_LEVELS];  /* smoother CTA: 1024 (one per SM), 512 (two)
+                                              or 256 threads (four)                     */
     int asm_slices[MGFVM_MAX_LEVELS];      /* assembly threads per cell: 1 or 3         */
     int restrict_slices[MGFVM_MAX_LEVELS]; /* restriction threads per cell: 1 or 3      */
 } mgfvm_tuning;

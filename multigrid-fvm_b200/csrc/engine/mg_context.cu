@@ -157,7 +157,8 @@ struct Builder {
             L.smem = smem_for(mx * my);
             return;
         }
-        const int nt = x->tune.smooth_threads[ig] == SMOOTH_BLOCK / 2 ? SMOOTH_BLOCK / 2 : SMOOTH_BLOCK;
+        const int tt = x->tune.smooth_threads[ig];
+        const int nt = tt == SMOOTH_BLOCK / 2 || tt == SMOOTH_BLOCK / 4 ? tt : SMOOTH_BLOCK;
         const int most = (smooth_pairs_side(0, nt) - MIN_TILE) / 2;   // units that leave a MIN_TILE tile
         const int cap = std::min(most, x->tune.smooth_units[ig] > 0 ? x->tune.smooth_units[ig] : MAX_UNITS);
         int chunks = (units + cap - 1) / cap;
@@ -998,7 +999,8 @@ static bool tuning_valid(const mgfvm_tuning &t)
 {
     for (int ig = 0; ig < MGFVM_MAX_LEVELS; ++ig) {
         if (t.smooth_units[ig] < 0 || t.smooth_units[ig] > 64) return false;
-        if (t.smooth_threads[ig] != 0 && t.smooth_threads[ig] != SMOOTH_BLOCK && t.smooth_threads[ig] != SMOOTH_BLOCK / 2)
+        if (t.smooth_threads[ig] != 0 && t.smooth_threads[ig] != SMOOTH_BLOCK && t.smooth_threads[ig] != SMOOTH_BLOCK / 2 &&
+            t.smooth_threads[ig] != SMOOTH_BLOCK / 4)
             return false;
         for (int v : {t.asm_slices[ig], t.restrict_slices[ig]})
             if (v != 0 && v != 1 && v != 3) return false;
@@ -1088,7 +1090,8 @@ int mgfvm_autotune(mgfvm_ctx *x, int cycles, mgfvm_tuning *chosen, double *ms_be
             int mx, my;
             if (!probe.whole_level(ig, mx, my)) {
                 static const int opts[][2] = {{SMOOTH_BLOCK, 10}, {SMOOTH_BLOCK, 4}, {SMOOTH_BLOCK, 6}, {SMOOTH_BLOCK, 16},
-                                              {SMOOTH_BLOCK / 2, 4}, {SMOOTH_BLOCK / 2, 6}, {SMOOTH_BLOCK / 2, 10}};
+                                              {SMOOTH_BLOCK / 2, 4}, {SMOOTH_BLOCK / 2, 6}, {SMOOTH_BLOCK / 2, 10},
+                                              {SMOOTH_BLOCK / 4, 3}, {SMOOTH_BLOCK / 4, 5}};
                 for (auto &o : opts) knobs.push_back({0, o[0], o[1]});
             }
             knobs.push_back({1, 1, 0});

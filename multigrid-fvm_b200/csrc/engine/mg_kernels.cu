@@ -914,12 +914,16 @@ cudaError_t launch_one(const Launch &X, const CaseDev *dc, CaseState *ds, const 
     case K_SMOOTH:
         if (b > SMOOTH_BLOCK) return cudaErrorInvalidValue;
         if (S.isolve == MGFVM_JACOBI) {
-            if (b <= SMOOTH_BLOCK / 2)
+            if (b <= SMOOTH_BLOCK / 4)
+                k_smooth<MGFVM_JACOBI, SMOOTH_BLOCK / 4><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+            else if (b <= SMOOTH_BLOCK / 2)
                 k_smooth<MGFVM_JACOBI, SMOOTH_BLOCK / 2><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
             else
                 k_smooth<MGFVM_JACOBI, SMOOTH_BLOCK><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
         } else {
-            if (b <= SMOOTH_BLOCK / 2)
+            if (b <= SMOOTH_BLOCK / 4)
+                k_smooth<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK / 4><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+            else if (b <= SMOOTH_BLOCK / 2)
                 k_smooth<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK / 2><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
             else
                 k_smooth<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
@@ -928,12 +932,16 @@ cudaError_t launch_one(const Launch &X, const CaseDev *dc, CaseState *ds, const 
     case K_SMOOTH_MIXED:
         if (b > SMOOTH_BLOCK) return cudaErrorInvalidValue;
         if (S.isolve == MGFVM_JACOBI) {
-            if (b <= SMOOTH_BLOCK / 2)
+            if (b <= SMOOTH_BLOCK / 4)
+                k_smooth_mixed<MGFVM_JACOBI, SMOOTH_BLOCK / 4><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+            else if (b <= SMOOTH_BLOCK / 2)
                 k_smooth_mixed<MGFVM_JACOBI, SMOOTH_BLOCK / 2><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
             else
                 k_smooth_mixed<MGFVM_JACOBI, SMOOTH_BLOCK><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
         } else {
-            if (b <= SMOOTH_BLOCK / 2)
+            if (b <= SMOOTH_BLOCK / 4)
+                k_smooth_mixed<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK / 4><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+            else if (b <= SMOOTH_BLOCK / 2)
                 k_smooth_mixed<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK / 2><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
             else
                 k_smooth_mixed<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);

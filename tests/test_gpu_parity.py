@@ -184,6 +184,7 @@ TUNINGS = [
     {"smooth_units": [7, 5, 0], "smooth_threads": [1024, 512, 0], "asm_slices": [3, 1, 3],
      "restrict_slices": [1, 3, 1]},
     {"smooth_units": [16, 12, 20], "smooth_threads": [1024, 512, 1024]},
+    {"smooth_units": [3, 7, 5], "smooth_threads": [256, 256, 256]},
 ]
 
 
