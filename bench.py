@@ -45,13 +45,19 @@ def log(*a):
 
 # --------------------------------------------------------------- workloads
 def workload(name):
+    """(cases, description, per-case inlet u profiles or None)."""
     from mgfvm import configs
     if name == "c1":
-        return configs.c1_pair(seed=1), "obstacle flow 256x256 ngrid 5 RBGS Re {10,100} (2 cases)"
+        return configs.c1_pair(seed=1), "obstacle flow 256x256 ngrid 5 RBGS Re {10,100} (2 cases)", None
     if name == "c0":
-        return [configs.c0(1)], "channel 64x64 ngrid 3 Jacobi Re 100"
+        return [configs.c0(1)], "channel 64x64 ngrid 3 Jacobi Re 100", None
     if name == "c2":
-        return configs.c2(64, seed=2), "64 mixed-size obstacle cases 64/128/256, coarsest 8x8"
+        return configs.c2(512, seed=2), "512 mixed-size obstacle cases 64/128/256, coarsest 8x8", None
+    if name == "c3":
+        return [configs.c3(seed=3)], "1024x1024 ngrid 7 quarter-pixel staggered lattice Re 200", None
+    if name == "c4":
+        cases, prof = configs.c4(64, seed=4)
+        return cases, "64 cases 256x256 ngrid 5 Re 100 random particles, per-face inlet u", prof
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -126,7 +132,7 @@ def batched_rate(nb, device, tune, cycles_per_solve, ncyc=40):
     return out
 
 
-def mixed_solve(cases, device, ref_solver, tune):
+def mixed_solve(cases, device, ref_solver, tune, profiles=None):
     """One solve of the workload with MGFVM_PREC_MIXED (FP32 correction smoothing
     against FP64 residuals), timed like a bench step, and the relative L2 distance of
     its final fields to the FP64 solve's (`ref_solver` holds the FP64 result; p
@@ -134,6 +140,8 @@ def mixed_solve(cases, device, ref_solver, tune):
     import torch
     from mgfvm import Solver
     with Solver(cases, device=device, precision="mixed", sync_every=64) as s:
+        for k, pr in enumerate(profiles or []):
+            s.set_inlet_profile(k, pr)
         if tune:
             s.autotune(3)
         s.solve(20, FP_TOL)
@@ -247,8 +255,8 @@ def cpu_sample(cases, cycles_to_converge, ncyc, procs):
 def run_reference_arm(a, rank, world):
     if rank != 0:
         return
-    cases, desc = workload(a.workload)
-    ctc = CYCLES_TO_CONVERGE[a.workload]
+    cases, desc, _ = workload(a.workload)
+    ctc = CYCLES_TO_CONVERGE.get(a.workload)
     if ctc is None:
         print(json.dumps({"impl": "reference", "unavailable": f"no converged cycle counts for {a.workload}"}))
         return
@@ -281,7 +289,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c1", choices=["c1", "c0", "c2"])
+    ap.add_argument("--workload", default="c1", choices=["c1", "c0", "c2", "c3", "c4"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tail", type=int, default=-1, help="first level of the one-CTA coarse kernel (-1 auto)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the engine's default schedule")
@@ -307,9 +315,11 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
 
     from mgfvm import Solver
-    cases, desc = workload(a.workload)
+    cases, desc, profiles = workload(a.workload)
     n_cases = len(cases)
     solver = Solver(cases, device=local, sync_every=64, tail_level=a.tail)
+    for k, pr in enumerate(profiles or []):
+        solver.set_inlet_profile(k, pr)
     tuned = None
     if not a.no_autotune:
         t_before, t_after, tuned = solver.autotune(5)
@@ -386,6 +396,8 @@ def main():
         h2d = d2h = 0
         for _ in range(max(1, a.steps)):
             with Solver(cases, device=local) as s2:
+                for k, pr in enumerate(profiles or []):
+                    s2.set_inlet_profile(k, pr)
                 if tuned:
                     s2.set_tuning(**tuned)
                 s2.solve(max(c.nvcycle for c in cases), FP_TOL)
@@ -407,7 +419,7 @@ def main():
     # ---- mixed precision: the same solve with FP32 correction smoothing
     mixed = None
     if world == 1:
-        mixed = mixed_solve(cases, local, solver, tuned is not None)
+        mixed = mixed_solve(cases, local, solver, tuned is not None, profiles)
 
     # ---- batched throughput: many obstacle-flow cases in one context
     batched = None
@@ -421,7 +433,10 @@ def main():
         sys.path.insert(0, os.path.join(REPO, "oracle"))
         import oracle
         with Solver(cases[:1], device=local) as s3:
-            o = oracle.OracleCase(cases[0])
+            pr0 = profiles[0] if profiles else None
+            if pr0 is not None:
+                s3.set_inlet_profile(0, pr0)
+            o = oracle.OracleCase(cases[0], pr0)
             s3.cycle(3)
             o.cycle(3)
             l2err = max(float(np.linalg.norm(s3.field(0, 0, f) - o.get(0, f)) /
