@@ -227,7 +227,8 @@ __device__ __forceinline__ void cell_asm(const LevelDev &L, const CaseDev &C, co
 
 // solve_pprime's assembly: masserror :1096-1125 then coefp :1018-1092 (with the
 // p' Dirichlet rows in the order x-, x+, y-, y+) at one interior cell; returns |div|.
-__device__ __forceinline__ double cell_mass_coefp(const LevelDev &L, const CaseDev &C, int i, int j)
+__device__ __forceinline__ double mass_coefp_values(const LevelDev &L, const CaseDev &C, int i, int j, Coef &k,
+                                                    double &su_out)
 {
     const int nx = L.npx, ny = L.npy, q = j * nx + i, s = q - nx;
     const double *ax = MGF(L, S_AREAX), *ay = MGF(L, S_AREAY);
@@ -236,8 +237,6 @@ __device__ __forceinline__ double cell_mass_coefp(const LevelDev &L, const CaseD
     const double axq = ax[q], ayq = ay[q];
     double div = axq * u[q] - axq * u[q - 1] + ayq * v[q] - ayq * v[s];
     double su = -div;
-    MGF(L, S_PP)[q] = 0.0;
-    Coef k;
     k.aw = ax[q - 1] * ax[q - 1] / apu[q - 1];
     k.ae = axq * axq / apu[q];
     k.as = ay[s] * ay[s] / apv[s];
@@ -248,8 +247,19 @@ __device__ __forceinline__ double cell_mass_coefp(const LevelDev &L, const CaseD
     if (C.ibc_xp == 2 && i == nx - 2) { k.ap = k.ap + diag; su = 0.0; }
     if (C.ibc_ym == 2 && j == 1) { k.ap = k.ap + diag; su = 0.0; }
     if (C.ibc_yp == 2 && j == ny - 2) { k.ap = k.ap + diag; su = 0.0; }
-    store_coef(L, EQ_PP, q, k, su);
+    su_out = su;
     return fabs(div);
+}
+
+__device__ __forceinline__ double cell_mass_coefp(const LevelDev &L, const CaseDev &C, int i, int j)
+{
+    Coef k;
+    double su;
+    const double ad = mass_coefp_values(L, C, i, j, k, su);
+    const int q = j * L.npx + i;
+    MGF(L, S_PP)[q] = 0.0;
+    store_coef(L, EQ_PP, q, k, su);
+    return ad;
 }
 
 // update :1127-1152 (the obstacle pressure copy :1153-1177 is a separate gather)

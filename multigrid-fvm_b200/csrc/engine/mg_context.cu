@@ -197,10 +197,7 @@ struct Builder {
     // pbound + outflow (bits as k_bound); skipped when no case has such a boundary
     void bound(int ig, int mode, int bits)
     {
-        bool need = false;
-        for (const CaseDev &C : x->hc)
-            need |= ((bits & 1) && (C.ibc_xm == 3 || C.ibc_ym == 3)) || ((bits & 6) && C.ibc_xp == 4);
-        if (!need) return;
+        if (!bound_needed(bits)) return;
         Launch &L = add(K_BOUND, ig, mode, 1, bits);
         L.grid = dim3(1, x->ncases);
     }
@@ -217,13 +214,35 @@ struct Builder {
         return true;
     }
     // returns the update's fuse bits (0: outflow still to do)
-    int solve_pp(int ig, int mode, bool reduce, int fuse)
+    // `bound_bits` != 0: pbound/outflow follow the obstacle pressure copy (k_bound bits);
+    // when both have work they run as one kernel, one CTA per case.
+    int solve_pp(int ig, int mode, bool reduce, int fuse, int bound_bits = 0)
     {
         add(K_MASS_COEFP, ig, mode, cells(ig), reduce ? 1 : 0);
         smooth(ig, mode, 1 << EQ_PP, x->sched.nswpp);
         add(K_UPDATE, ig, mode, cells(ig) + 2, fuse);
+        if (bound_bits && bound_needed(bound_bits) && pfix_needed(ig, mode)) {
+            Launch &L = add(K_PFIX_BOUND, ig, mode, 1, bound_bits);
+            L.grid = dim3(1, x->ncases);
+            L.block = PFIX_BOUND_BLOCK;
+            return fuse;
+        }
         pfix(ig, mode);
+        if (bound_bits) bound(ig, mode, bound_bits);
         return fuse;
+    }
+    bool pfix_needed(int ig, int mode) const
+    {
+        for (int c = 0; c < x->ncases; ++c)
+            if (mode_active(x->hc[c], ig, mode) && x->progs[c * MAXLEV + ig].ncopy > 0) return true;
+        return false;
+    }
+    bool bound_needed(int bits) const
+    {
+        bool need = false;
+        for (const CaseDev &C : x->hc)
+            need |= ((bits & 1) && (C.ibc_xm == 3 || C.ibc_ym == 3)) || ((bits & 6) && C.ibc_xp == 4);
+        return need;
     }
     // One SIMPLE step (down leg :201-207, up leg :235-244).  u, v and sc depend only
     // on the visit-start fluxes, so they are assembled together and smoothed in the
@@ -240,8 +259,7 @@ struct Builder {
         }
         smooth(ig, mode, (1 << EQ_U) | (1 << EQ_V) | (1 << EQ_SC), x->sched.nswpm);
         const int fuse = outflow_fusable(ig, mode) ? (down ? 1 : 3) : 0;
-        solve_pp(ig, mode, reduce, fuse);
-        if (!fuse) bound(ig, mode, down ? 3 : 7);
+        solve_pp(ig, mode, reduce, fuse, fuse ? 0 : (down ? 3 : 7));
     }
     // :211-220
     // `coarse_asm`: also run the coarse level's down-leg assembly (see k_restrict)

@@ -230,6 +230,28 @@ __global__ void __launch_bounds__(BLOCK) k_bound(const CaseDev *__restrict__ cs,
     bound_block(C, C.lv[ig], bits);
 }
 
+// update's obstacle pressure copy (:1153-1177, as k_pfix) followed by pbound/outflow
+// (as k_bound), one CTA per case: the copy may write the outlet columns that outflow
+// then reads, so the two run in this order with a block barrier between them.
+__global__ void __launch_bounds__(PFIX_BOUND_BLOCK) k_pfix_bound(const CaseDev *__restrict__ cs, CaseState *st, int ig,
+                                                                 int mode, int bits)
+{
+    const CaseDev &C = cs[blockIdx.y];
+    if (!case_active(C, st[blockIdx.y], ig, mode)) return;
+    const LevelDev &L = C.lv[ig];
+    double *p = MGF(L, S_P);
+    const int n = L.ncopy;
+    if (L.hazard) {
+        for (int k = threadIdx.x; k < n; k += blockDim.x) L.pbuf[k] = p[L.psrc[k]];
+        __syncthreads();
+        for (int k = threadIdx.x; k < n; k += blockDim.x) p[L.pdst[k]] = L.pbuf[k];
+    } else {
+        for (int k = threadIdx.x; k < n; k += blockDim.x) p[L.pdst[k]] = p[L.psrc[k]];
+    }
+    __syncthreads();
+    bound_block(C, L, bits);
+}
+
 // Geometry of one smoother CTA (blockIdx.x picks a tile x tile block of equation e's
 // sweep domain): the tile, the region it stages (the tile plus a halo of `nu` cells,
 // clipped at the domain's boundary ring), and this thread's vertical pair of cells,
@@ -897,6 +919,17 @@ cudaError_t configure_kernels()
     return cudaFuncSetAttribute(k_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, TAIL_SMEM_MAX);
 }
 
+template <int ISOLVE>
+static void launch_smooth(const Launch &X, dim3 g, int b, const CaseDev *dc, CaseState *ds, cudaStream_t st)
+{
+    if (b <= SMOOTH_BLOCK / 4)
+        k_smooth<ISOLVE, SMOOTH_BLOCK / 4><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+    else if (b <= SMOOTH_BLOCK / 2)
+        k_smooth<ISOLVE, SMOOTH_BLOCK / 2><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+    else
+        k_smooth<ISOLVE, SMOOTH_BLOCK><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+}
+
 cudaError_t launch_one(const Launch &X, const CaseDev *dc, CaseState *ds, const Sched &S, cudaStream_t st)
 {
     const dim3 g = X.grid;
@@ -913,21 +946,10 @@ cudaError_t launch_one(const Launch &X, const CaseDev *dc, CaseState *ds, const 
     case K_BOUND: k_bound<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, X.a0); break;
     case K_SMOOTH:
         if (b > SMOOTH_BLOCK) return cudaErrorInvalidValue;
-        if (S.isolve == MGFVM_JACOBI) {
-            if (b <= SMOOTH_BLOCK / 4)
-                k_smooth<MGFVM_JACOBI, SMOOTH_BLOCK / 4><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
-            else if (b <= SMOOTH_BLOCK / 2)
-                k_smooth<MGFVM_JACOBI, SMOOTH_BLOCK / 2><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
-            else
-                k_smooth<MGFVM_JACOBI, SMOOTH_BLOCK><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
-        } else {
-            if (b <= SMOOTH_BLOCK / 4)
-                k_smooth<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK / 4><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
-            else if (b <= SMOOTH_BLOCK / 2)
-                k_smooth<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK / 2><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
-            else
-                k_smooth<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
-        }
+        if (S.isolve == MGFVM_JACOBI)
+            launch_smooth<MGFVM_JACOBI>(X, g, b, dc, ds, st);
+        else
+            launch_smooth<MGFVM_GAUSS_SEIDEL>(X, g, b, dc, ds, st);
         break;
     case K_SMOOTH_MIXED:
         if (b > SMOOTH_BLOCK) return cudaErrorInvalidValue;
@@ -948,6 +970,7 @@ cudaError_t launch_one(const Launch &X, const CaseDev *dc, CaseState *ds, const 
         }
         break;
     case K_COPY: k_copy<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, X.a0); break;
+    case K_PFIX_BOUND: k_pfix_bound<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, X.a0); break;
     case K_RESTV_FLUXES: k_restv_fluxes<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode); break;
     case K_RESTRICT: k_restrict<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, (unsigned)X.a0); break;
     case K_PROL_CORR: k_prol_corr<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode); break;

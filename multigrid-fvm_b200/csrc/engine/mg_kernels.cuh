@@ -20,6 +20,7 @@ enum KernelId {
     K_PROL_CORR, K_PROL_APPLY,
     K_TAIL, K_ENDCYCLE, K_PROL_APPLY_END,
     K_SMOOTH_MIXED,  // as K_SMOOTH, FP32 correction smoothing with an FP64 residual
+    K_PFIX_BOUND,    // K_PFIX then K_BOUND (a0 = bits), one CTA per case
     K_NKERNELS
 };
 
@@ -63,6 +64,7 @@ size_t raw_masserror_blocks(int npx, int npy);
 cudaError_t raw_check_division(long long n, unsigned long long seed, unsigned long long *bad, cudaStream_t s);
 
 constexpr int BLOCK = 256;
+constexpr int PFIX_BOUND_BLOCK = 1024;
 constexpr int TAIL_BLOCK = 512;
 constexpr int TAIL_SMEM_MAX = 220 * 1024;   // dynamic shared memory of the coarse kernel (+ its static 256 B)
 
