@@ -9,7 +9,7 @@ import shutil
 import numpy as np
 import pytest
 
-from conftest import GOLDEN
+from conftest import GOLDEN, REPO
 
 
 def test_library_exports_every_declared_symbol():
@@ -133,3 +133,13 @@ def test_writers_byte_identical_to_reference(tmp_path, capfd, monkeypatch, oracl
     out = capfd.readouterr().out.splitlines()
     ref = open(os.path.join(d, "stdout.txt")).read().splitlines()
     assert out == ref[-4:]
+
+
+def test_sweep_driver_arguments(tmp_path):
+    """The batch driver checks its arguments and inputs before it needs a GPU."""
+    import subprocess
+    sweep = os.path.join(REPO, "multigrid-fvm_b200", "bin", "mgfvm_sweep")
+    r = subprocess.run([sweep, "--bogus"], cwd=tmp_path, capture_output=True, text=True, timeout=60)
+    assert r.returncode == 2 and "usage" in r.stderr
+    r = subprocess.run([sweep], cwd=tmp_path, capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1 and "pattern_*.txt" in r.stderr

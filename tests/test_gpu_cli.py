@@ -43,3 +43,31 @@ def test_cli_matches_reference_binary(tmp_path):
     assert csv_m[0] == csv_r[0] and len(csv_m) == len(csv_r)
     np.testing.assert_allclose([float(l.split(",")[1]) for l in csv_m[1:]],
                                [float(l.split(",")[1]) for l in csv_r[1:]], rtol=1e-6)
+
+
+SWEEP = os.path.join(REPO, "multigrid-fvm_b200", "bin", "mgfvm_sweep")
+
+
+def test_sweep_matches_one_run_per_pattern(tmp_path):
+    """The batch driver (run_patterns_and_save_vtk.sh's loop, all cases in one GPU
+    context) writes the same files as the drop-in solver run once per (Re, pattern)
+    in its own directory, as the shell loop runs the reference."""
+    from mgfvm import configs
+    base = configs.small(32, 3, isolve=2, ig_obs=3, sc_obs=0.0, nvcycle=40)
+    pats = {"1": [(2, 3, 2, 2), (5, 6, 4, 6)], "12": [(1, 1, 7, 8)], "3": []}
+    (tmp_path / "patterns").mkdir()
+    base.write(str(tmp_path))
+    for n, obs in pats.items():
+        (tmp_path / "patterns" / f"pattern_{n}.txt").write_text(base.replace(obstacles=obs).pattern_text())
+    res = subprocess.run([SWEEP, "--re", "10,20"], cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert res.returncode == 0, res.stdout + res.stderr
+    for re in ("10", "20"):
+        for n, obs in pats.items():
+            d = tmp_path / f"single_{re}_{n}"
+            base.replace(obstacles=obs, amuf=1.0 / float(re)).write(str(d))
+            r = subprocess.run([BIN], cwd=d, capture_output=True, text=True, timeout=120)
+            assert r.returncode == 0, r.stderr
+            out = tmp_path / "solution" / f"Re_{re}"
+            assert (out / "vtk_files" / f"vtk_{n}.vtk").read_text() == (d / "vtk_acc.vtk").read_text(), (re, n)
+            assert (out / "convergence_files" / f"convergence_{n}.csv").read_text() == \
+                (d / "convergence.csv").read_text(), (re, n)
