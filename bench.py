@@ -80,9 +80,10 @@ def load_peaks():
         return {}
 
 
-# DRAM bytes (read + write) per k_smooth launch of the p' smoothing on level 0, from one
-# ncu capture of `python bench.py --profile-cycles 1` (profiles/k_smooth_obstacle256.md).
-ROOFLINE_TRAFFIC = {"c1": 7475712}
+# DRAM bytes (read + write) per k_smooth launch of the p' smoothing on level 0, from ncu
+# captures (profiles/k_smooth_obstacle256.md): the 2-case workload of
+# `python bench.py --profile-cycles 1`, and the 64-case batch of the `batched` entry.
+ROOFLINE_TRAFFIC = {"c1": 7475712, "c1x64": 266211072}
 
 
 def smoother_roofline(solver, cases, traffic=None, reps=20):
@@ -391,10 +392,7 @@ def main():
     # ---- end to end through the public API with host buffers
     e2e = None
     if rank == 0 or True:
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        h2d = d2h = 0
-        for _ in range(max(1, a.steps)):
+        def e2e_step():
             with Solver(cases, device=local) as s2:
                 for k, pr in enumerate(profiles or []):
                     s2.set_inlet_profile(k, pr)
@@ -404,7 +402,14 @@ def main():
                 for k in range(n_cases):
                     for f in ("u", "v", "p", "sc"):
                         s2.field(k, 0, f)
-                b = s2.transfer_bytes
+                return s2.transfer_bytes
+
+        e2e_step()                           # untimed warm-up step
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        h2d = d2h = 0
+        for _ in range(max(1, a.steps)):
+            b = e2e_step()
             h2d += b[0]
             d2h += b[1]
         torch.cuda.synchronize()
