@@ -234,7 +234,9 @@ int mgfvm_last_elapsed_ms(mgfvm_ctx *ctx, double *ms);
 int mgfvm_stream(mgfvm_ctx *ctx, void **stream);
 
 /* Time `reps` back-to-back runs of single-step op `op` on `level` of every case with
- * CUDA events on the context stream (no host work between the events).
+ * CUDA events on the context stream: the op's launches are captured into a CUDA graph
+ * once and the graph is replayed `reps` times after one untimed replay, so no host
+ * launch overhead sits between the events.
  * *ms_total = elapsed milliseconds, *launches = kernels launched in that window. */
 int mgfvm_time_op(mgfvm_ctx *ctx, int op, int level, int reps, double *ms_total, int *launches);
 

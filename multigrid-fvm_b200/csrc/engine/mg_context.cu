@@ -1002,12 +1002,32 @@ int mgfvm_time_op(mgfvm_ctx *x, int op, int level, int reps, double *ms_total, i
     std::vector<Launch> v;
     Builder b{x, &v};
     b.op(op, level);
-    CK(cudaEventRecord(x->e0, x->stream));
-    for (int r = 0; r < reps; ++r) RC(run_list(x, v));
-    CK(cudaEventRecord(x->e1, x->stream));
-    CK(cudaEventSynchronize(x->e1));
+    // the op's launches are captured once into a graph and the graph is replayed, so
+    // the host's launch rate does not pace short kernels (as in a V-cycle)
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ge = nullptr;
+    CK(cudaStreamBeginCapture(x->stream, cudaStreamCaptureModeThreadLocal));
+    for (const Launch &L : v) {
+        cudaError_t e = launch_one(L, x->dc, x->ds, x->sched, x->stream);
+        if (e != cudaSuccess) {
+            cudaStreamEndCapture(x->stream, &g);
+            if (g) cudaGraphDestroy(g);
+            return mgfvm_fail(MGFVM_ECUDA, "time_op capture: %s", cudaGetErrorString(e));
+        }
+    }
+    CK(cudaStreamEndCapture(x->stream, &g));
+    cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
+    if (e == cudaSuccess) e = cudaGraphLaunch(ge, x->stream);          // warm the graph
+    if (e == cudaSuccess) e = cudaEventRecord(x->e0, x->stream);
+    for (int r = 0; r < reps && e == cudaSuccess; ++r) e = cudaGraphLaunch(ge, x->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(x->e1, x->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(x->e1);
     float ms = 0;
-    CK(cudaEventElapsedTime(&ms, x->e0, x->e1));
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, x->e0, x->e1);
+    if (ge) cudaGraphExecDestroy(ge);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return mgfvm_fail(MGFVM_ECUDA, "time_op: %s", cudaGetErrorString(e));
+    x->launches += (long long)v.size() * (reps + 1);
     if (ms_total) *ms_total = ms;
     if (launches) *launches = (int)v.size() * reps;
     return MGFVM_OK;
