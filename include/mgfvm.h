@@ -212,6 +212,13 @@ int mgfvm_level_dims(mgfvm_ctx *ctx, int icase, int level, int *npx, int *npy);
 /* Copy one array of one level of one case (npx*npy doubles) to or from the host. */
 int mgfvm_get_field(mgfvm_ctx *ctx, int icase, int level, int field, double *out);
 int mgfvm_set_field(mgfvm_ctx *ctx, int icase, int level, int field, const double *in);
+/* Zero-copy access: the device address of one array of one level of one case
+ * (npx*npy doubles, row-major ij = j*npx + i), owned by the context and valid until
+ * mgfvm_destroy.  Reads and writes through it must be ordered with the context's
+ * stream (mgfvm_stream).  For the coefficient fields (aw ... ap) the address is that
+ * of the equation most recently assembled on the level at the time of the call. */
+int mgfvm_field_device_ptr(mgfvm_ctx *ctx, int icase, int level, int field, double **ptr, int *npx,
+                           int *npy);
 /* The cell tag of one level (1 fluid, 0 obstacle; init :617-641), npx*npy ints. */
 int mgfvm_get_tag(mgfvm_ctx *ctx, int icase, int level, int *out);
 /* Obstacle index ranges of one level after the level mapping of :468-478.  Levels

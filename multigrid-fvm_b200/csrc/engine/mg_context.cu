@@ -920,6 +920,18 @@ int mgfvm_get_field(mgfvm_ctx *x, int icase, int level, int field, double *out)
     return MGFVM_OK;
 }
 
+int mgfvm_field_device_ptr(mgfvm_ctx *x, int icase, int level, int field, double **ptr, int *npx, int *npy)
+{
+    RC(check_ctx(x));
+    RC(check_case_level(x, icase, level));
+    if (field < 0 || field >= MGFVM_NFIELDS || !ptr) return mgfvm_fail(MGFVM_EINVAL, "bad field %d", field);
+    const LevelDev &L = x->hc[icase].lv[level];
+    *ptr = L.f[field_slot(field, x->last_eq[level])];
+    if (npx) *npx = L.npx;
+    if (npy) *npy = L.npy;
+    return MGFVM_OK;
+}
+
 int mgfvm_set_field(mgfvm_ctx *x, int icase, int level, int field, const double *in)
 {
     RC(check_ctx(x));

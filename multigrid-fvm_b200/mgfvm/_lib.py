@@ -82,6 +82,7 @@ def lib() -> C.CDLL:
         "mgfvm_masserror_scratch_doubles": (C.c_size_t, [C.c_int, C.c_int]),
         "mgfvm_masserror_f64_noalloc": (C.c_int, [_vp] * 6 + [C.c_int, C.c_int, _vp, _vp]),
         "mgfvm_check_division": (C.c_int, [C.c_int, C.c_longlong, C.c_ulonglong, _vp]),
+        "mgfvm_field_device_ptr": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p), _ip, _ip]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -67,6 +67,7 @@ class Solver:
         check(L.mgfvm_create(arr, len(self.cases), C.byref(opt), C.byref(h)))
         self._h = h
         self._lib = L
+        self.device = device
 
     # ------------------------------------------------------------ lifetime
     def close(self) -> None:
@@ -192,6 +193,22 @@ class Solver:
         check(self._lib.mgfvm_profile_cycle(self._h, ms.ctypes.data_as(_dp), kid.ctypes.data_as(_ip),
                                             lvl.ctypes.data_as(_ip), cap, C.byref(n)))
         return [(self.KERNELS[kid[k]], int(lvl[k]), float(ms[k])) for k in range(min(n.value, cap))]
+
+    def field_view(self, case: int, level: int, name: str):
+        """A torch float64 CUDA tensor (npy, npx) sharing the engine's memory of one
+        array (no copy).  Valid while the solver is open; order work on it with the
+        context stream (`stream`), e.g. by running torch work on
+        torch.cuda.ExternalStream(solver.stream)."""
+        import torch
+        ptr, nx, ny = C.c_void_p(), C.c_int(), C.c_int()
+        check(self._lib.mgfvm_field_device_ptr(self._h, case, level, _abi.FIELD[name], C.byref(ptr),
+                                                C.byref(nx), C.byref(ny)))
+
+        class _View:
+            __cuda_array_interface__ = {"shape": (ny.value, nx.value), "typestr": "<f8",
+                                        "data": (ptr.value, False), "version": 2, "strides": None}
+        t = torch.as_tensor(_View(), device=torch.device("cuda", self.device))
+        return t
 
     @property
     def tuning(self) -> dict:

@@ -101,3 +101,31 @@ def test_division_by_reciprocal_matches_ieee():
     for seed in (1, 2, 3):
         assert L.mgfvm_check_division(0, 1 << 27, seed, C.byref(bad)) == 0
         assert bad.value == 0
+
+
+def test_field_views_share_engine_memory(oracle_built):
+    """mgfvm_field_device_ptr / Solver.field_view: a torch tensor over the engine's own
+    array, no copy: it reads what the engine computed, and what is written through it
+    is what the next cycles start from."""
+    import torch
+    from mgfvm import Solver, configs
+    from oracle import OracleCase
+    cfg = configs.small(32, 3, isolve=2)
+    s = Solver(cfg)
+    s.cycle(2)
+    u = s.field_view(0, 0, "u")
+    assert u.shape == (34, 34) and u.dtype == torch.float64 and u.is_cuda
+    np.testing.assert_array_equal(u.cpu().numpy(), s.field(0, 0, "u"))
+    o = OracleCase(cfg)
+    o.cycle(2)
+    sc = o.get(0, "sc") * 0.5
+    o.set(0, "sc", sc)
+    stream = torch.cuda.ExternalStream(s.stream)
+    with torch.cuda.stream(stream):
+        s.field_view(0, 0, "sc").copy_(torch.from_numpy(sc).cuda())
+    stream.synchronize()
+    s.cycle(2)
+    o.cycle(2)
+    for f in ("u", "v", "p", "sc"):
+        assert_bitexact(s.field(0, 0, f), o.get(0, f), f"after writing sc through the view: {f}")
+    s.close()
