@@ -148,6 +148,8 @@ typedef struct mgfvm_tuning {
                                               or 256 threads (four)                     */
     int asm_slices[MGFVM_MAX_LEVELS];      /* assembly threads per cell: 1 or 3         */
     int restrict_slices[MGFVM_MAX_LEVELS]; /* restriction threads per cell: 1 or 3      */
+    int update_pfix[MGFVM_MAX_LEVELS];     /* obstacle pressure copy inside update where
+                                              legal: 0 or 2 yes, 1 no (own kernel)      */
 } mgfvm_tuning;
 
 typedef struct mgfvm_ctx mgfvm_ctx;

@@ -54,7 +54,12 @@ struct LevelDev {
     const int *pdst;
     const int *psrc;
     double *pbuf;
+    const int *pcode;   // the same copies done by k_update (mgfvm_obstacle_prog.fan), or nullptr
+    const int *pfan;
 };
+
+constexpr int PCODE_DST = 1 << 30;   // pcode bit: the copy writes this cell
+constexpr int PFAN_END = 1 << 30;    // pfan bit: last copy of its owner (PFAN_LAST of the host)
 
 // Stop-rule and status flags of one case.
 enum CaseStatus { CASE_RUNNING = 0, CASE_CONVERGED_REF = 1, CASE_CONVERGED_FP = 2,

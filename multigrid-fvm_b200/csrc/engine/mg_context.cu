@@ -34,6 +34,7 @@ using namespace mg;
         if (r_ != MGFVM_OK) return r_; \
     } while (0)
 
+static_assert(PFAN_LAST == mg::PFAN_END, "fan-list end marker differs between host and device");
 static const int TAIL_AUTO_CELLS = 0;   // automatic choice: grid kernels on every level (measured fastest)
 static const int HIST_INITIAL = 4096;
 
@@ -203,13 +204,25 @@ struct Builder {
     }
     // Can outflow run inside update on this level?  Not if pbound (periodic) or the
     // obstacle pressure copy sits between them on the outlet columns for any case.
-    bool outflow_fusable(int ig, int mode) const
+    bool outflow_fusable(int ig, int mode, bool pfix_in_update) const
     {
         for (int c = 0; c < x->ncases; ++c) {
             const CaseDev &C = x->hc[c];
             if (!mode_active(C, ig, mode)) continue;
             if (C.ibc_xm == 3 || C.ibc_ym == 3) return false;
-            if (x->progs[(size_t)c * MAXLEV + ig].touches_outlet) return false;
+            if (!pfix_in_update && x->progs[(size_t)c * MAXLEV + ig].touches_outlet) return false;
+        }
+        return true;
+    }
+    // Can update do the obstacle pressure copy itself?  Every active case's copy program
+    // on the level is empty or has no chained copies (fan lists built).
+    bool pfix_fusable(int ig, int mode) const
+    {
+        if (x->tune.update_pfix[ig] == 1) return false;
+        for (int c = 0; c < x->ncases; ++c) {
+            if (!mode_active(x->hc[c], ig, mode)) continue;
+            const LevelDev &L = x->hc[c].lv[ig];
+            if (L.ncopy > 0 && !L.pcode) return false;
         }
         return true;
     }
@@ -221,6 +234,10 @@ struct Builder {
         add(K_MASS_COEFP, ig, mode, cells(ig), reduce ? 1 : 0);
         smooth(ig, mode, 1 << EQ_PP, x->sched.nswpp);
         add(K_UPDATE, ig, mode, cells(ig) + 2, fuse);
+        if (fuse & 4) {                       // the copy ran inside update
+            if (bound_bits) bound(ig, mode, bound_bits);
+            return fuse;
+        }
         if (bound_bits && bound_needed(bound_bits) && pfix_needed(ig, mode)) {
             Launch &L = add(K_PFIX_BOUND, ig, mode, 1, bound_bits);
             L.grid = dim3(1, x->ncases);
@@ -258,8 +275,9 @@ struct Builder {
             L.grid.z = slices(ig, x->tune.asm_slices[ig]);
         }
         smooth(ig, mode, (1 << EQ_U) | (1 << EQ_V) | (1 << EQ_SC), x->sched.nswpm);
-        const int fuse = outflow_fusable(ig, mode) ? (down ? 1 : 3) : 0;
-        solve_pp(ig, mode, reduce, fuse, fuse ? 0 : (down ? 3 : 7));
+        const bool pfx = pfix_fusable(ig, mode);
+        const int fuse = outflow_fusable(ig, mode, pfx) ? (down ? 1 : 3) : 0;
+        solve_pp(ig, mode, reduce, fuse | (pfx ? 4 : 0), fuse ? 0 : (down ? 3 : 7));
     }
     // :211-220
     // `coarse_asm`: also run the coarse level's down-leg assembly (see k_restrict)
@@ -630,7 +648,7 @@ int create_impl(const mgfvm_config *cases, int ncases, const mgfvm_options *opt_
     std::vector<size_t> off_slots;
     size_t off = 0;
     auto take = [&](size_t bytes) { off = align_up(off, 256); size_t o = off; off += std::max<size_t>(bytes, 8); return o; };
-    struct Pend { int c, ig; size_t slot[NSLOTS]; size_t tag, seq, pdst, psrc, pbuf; };
+    struct Pend { int c, ig; size_t slot[NSLOTS]; size_t tag, seq, pdst, psrc, pbuf, pcode, pfan; };
     std::vector<Pend> pend;
     std::vector<size_t> part_off(ncases), cnt_off(ncases);
     for (int c = 0; c < ncases; ++c) {
@@ -647,6 +665,9 @@ int create_impl(const mgfvm_config *cases, int ncases, const mgfvm_options *opt_
             p.pdst = P.ncopy ? take(P.ncopy * sizeof(int)) : (size_t)-1;
             p.psrc = P.ncopy ? take(P.ncopy * sizeof(int)) : (size_t)-1;
             p.pbuf = P.ncopy ? take(P.ncopy * sizeof(double)) : (size_t)-1;
+            const bool fan = P.ncopy && P.fan;
+            p.pcode = fan ? take(n * sizeof(int)) : (size_t)-1;
+            p.pfan = fan ? take(2 * (size_t)P.ncopy * sizeof(int)) : (size_t)-1;
             pend.push_back(p);
         }
         const long long n0 = (long long)(npx_of(g, 0) - 2) * (npy_of(g, 0) - 2);
@@ -693,6 +714,7 @@ int create_impl(const mgfvm_config *cases, int ncases, const mgfvm_options *opt_
         L.ncopy = P.ncopy;
         L.hazard = P.hazard;
         L.seq = nullptr; L.pdst = nullptr; L.psrc = nullptr; L.pbuf = nullptr;
+        L.pcode = nullptr; L.pfan = nullptr;
         if (P.nseq) {
             const size_t n = (size_t)L.npx * L.npy;
             std::vector<unsigned> dense(n, 0u);
@@ -709,6 +731,22 @@ int create_impl(const mgfvm_config *cases, int ncases, const mgfvm_options *opt_
             x->h2d += 2LL * P.ncopy * (long long)sizeof(int);
             L.pdst = dd; L.psrc = ds;
             L.pbuf = (double *)(x->pool + p.pbuf);
+        }
+        if (p.pcode != (size_t)-1) {
+            // per cell: PCODE_DST when the copy writes it, 1 + its first fan entry when
+            // its update thread performs copies
+            const size_t n = (size_t)L.npx * L.npy;
+            std::vector<int> code(n, 0);
+            for (int k = 0; k < P.ncopy; ++k) {
+                code[P.fan[2 * k] & ~PFAN_LAST] |= PCODE_DST;
+                if (k == 0 || P.owners[k] != P.owners[k - 1]) code[P.owners[k]] |= k + 1;
+            }
+            int *dc = (int *)(x->pool + p.pcode), *df = (int *)(x->pool + p.pfan);
+            CK(cudaMemcpy(dc, code.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(df, P.fan, 2 * (size_t)P.ncopy * sizeof(int), cudaMemcpyHostToDevice));
+            x->h2d += (long long)(n + 2 * (size_t)P.ncopy) * (long long)sizeof(int);
+            L.pcode = dc;
+            L.pfan = df;
         }
     }
 
@@ -1054,6 +1092,7 @@ static bool tuning_valid(const mgfvm_tuning &t)
             return false;
         for (int v : {t.asm_slices[ig], t.restrict_slices[ig]})
             if (v != 0 && v != 1 && v != 3) return false;
+        if (t.update_pfix[ig] < 0 || t.update_pfix[ig] > 2) return false;
     }
     return true;
 }

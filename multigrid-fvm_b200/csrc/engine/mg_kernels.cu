@@ -134,11 +134,17 @@ __global__ void __launch_bounds__(BLOCK) k_asm(const CaseDev *__restrict__ cs, C
     else cell_asm(L, C, FluxArrays(L), i, j, w);
 }
 
-// update :1127-1152; with `fuse` (bit 1) also outflow :1211-1228 of u, v, p (bit 2:
-// and sc), legal when nothing between them in the reference (pbound, the obstacle
-// pressure copy) touches the outlet columns: the cell at i = npx-3 writes its new u
-// to both its face and the outlet face, the cell at i = npx-2 its new v and p to the
-// ghost column, and two extra threads copy the ghosts of the boundary rows.
+// update :1127-1152; with `fuse` bit 1 also outflow :1211-1228 of u, v, p (bit 2: and
+// sc), with bit 4 also update's obstacle pressure copy (:1153-1177).  The copy gives
+// every destination the post-update pressure of its source; each is written by one
+// thread, the one updating the source (or, for a source on the boundary ring, the
+// nearest interior cell, which reads it before writing anything), and destinations
+// skip their own pressure write, so no thread reads a pressure another has changed.
+// Outflow is fused when nothing between update and outflow in the reference (pbound,
+// or the copy when it is not fused here) touches the outlet columns: the cell at
+// i = npx-3 writes its new u to its face and the outlet face, the cell at i = npx-2 its
+// new v and p to the ghost column (its copy's owner the copied p), and two extra
+// threads copy the ghosts of the boundary rows.
 __global__ void __launch_bounds__(BLOCK) k_update(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode,
                                                   int fuse)
 {
@@ -155,13 +161,24 @@ __global__ void __launch_bounds__(BLOCK) k_update(const CaseDev *__restrict__ cs
         const double un = u[q] + MGF(L, S_AREAX)[q] * (ppq - pp[q + 1]) / MGF(L, S_APU)[q];
         const double vn = v[q] + MGF(L, S_AREAY)[q] * (ppq - pp[q + nx]) / MGF(L, S_APV)[q];
         const double pn = p[q] + C.relxp * (ppq - ppref);
+        const int code = ((fuse & 4) && L.pcode) ? L.pcode[q] : 0;
+        if (code & ~PCODE_DST) {
+            for (int k = (code & ~PCODE_DST) - 1;; ++k) {
+                const int e = L.pfan[2 * k], src = L.pfan[2 * k + 1], dq = e & ~PFAN_END;
+                const double val = src < 0 ? pn : p[src];
+                p[dq] = val;
+                if (out && dq % nx == nx - 2) p[dq + 1] = val;
+                if (e & PFAN_END) break;
+            }
+        }
+        const bool dst = (code & PCODE_DST) != 0;
         if (!out || i != nx - 2) u[q] = un;
         v[q] = vn;
-        p[q] = pn;
+        if (!dst) p[q] = pn;
         if (out && i == nx - 3) u[q + 1] = un;
         if (out && i == nx - 2) {
             v[q + 1] = vn;
-            p[q + 1] = pn;
+            if (!dst) p[q + 1] = pn;
             if (fuse & 2) MGF(L, S_SC)[q + 1] = MGF(L, S_SC)[q];
         }
     } else if (out && t < n + 2) {

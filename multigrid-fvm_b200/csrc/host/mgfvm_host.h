@@ -32,7 +32,17 @@ typedef struct mgfvm_obstacle_prog {
     unsigned *codes;
     int max_adds;      /* longest sequence seen */
     int touches_outlet; /* a copy reads or writes column npx-2 or npx-1 (the outflow's columns) */
+    /* The same copies grouped by the interior cell whose update thread performs them
+     * (the source itself when it is interior, else the nearest interior cell):
+     * owners[k] in increasing order, fan[2k] = destination | PFAN_LAST on the last copy
+     * of an owner, fan[2k+1] = source index when it lies on the boundary ring (the
+     * owner reads its value) or -1 (the owner's own updated pressure).  Built only when
+     * hazard == 0. */
+    int *owners;
+    int *fan;
 } mgfvm_obstacle_prog;
+
+#define PFAN_LAST (1 << 30)
 
 int mgfvm_build_obstacle_prog(const mgfvm_config *c, int ig, mgfvm_obstacle_prog *out);
 void mgfvm_free_obstacle_prog(mgfvm_obstacle_prog *p);

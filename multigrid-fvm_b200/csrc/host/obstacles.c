@@ -110,6 +110,34 @@ int mgfvm_build_obstacle_prog(const mgfvm_config *c, int ig, mgfvm_obstacle_prog
     out->touches_outlet = outlet;
     out->ncopy = m;
     out->hazard = hazard;
+    if (!hazard && m > 0) {
+        /* group the copies by owner: the source when interior, else the interior cell
+         * next to it (sources are at most one cell outside an interior obstacle) */
+        int *tri = (int *)malloc(sizeof(int) * 3 * (size_t)m);
+        out->owners = (int *)malloc(sizeof(int) * (size_t)m);
+        out->fan = (int *)malloc(sizeof(int) * 2 * (size_t)m);
+        if (!tri || !out->owners || !out->fan) {
+            free(tri); free(pairs); free(origin); free(written); free(seq);
+            mgfvm_free_obstacle_prog(out);
+            return mgfvm_fail(MGFVM_ENOMEM, "obstacle program: out of host memory");
+        }
+        for (int k = 0; k < m; ++k) {
+            const int s0 = out->src[k], si = s0 % nx, sj = s0 / nx;
+            const int oi = si < 1 ? 1 : (si > nx - 2 ? nx - 2 : si);
+            const int oj = sj < 1 ? 1 : (sj > ny - 2 ? ny - 2 : sj);
+            tri[3 * k] = oj * nx + oi;
+            tri[3 * k + 1] = out->dst[k];
+            tri[3 * k + 2] = (oi == si && oj == sj) ? -1 : s0;
+        }
+        qsort(tri, (size_t)m, 3 * sizeof(int), cmp_pair);   /* by owner */
+        for (int k = 0; k < m; ++k) {
+            out->owners[k] = tri[3 * k];
+            const int last = k == m - 1 || tri[3 * (k + 1)] != tri[3 * k];
+            out->fan[2 * k] = tri[3 * k + 1] | (last ? PFAN_LAST : 0);
+            out->fan[2 * k + 1] = tri[3 * k + 2];
+        }
+        free(tri);
+    }
     m = 0;
     for (size_t q = 0; q < n; ++q)
         if (seq[q]) { out->cells[m] = (int)q; out->codes[m] = seq[q]; ++m; }
@@ -122,6 +150,6 @@ int mgfvm_build_obstacle_prog(const mgfvm_config *c, int ig, mgfvm_obstacle_prog
 void mgfvm_free_obstacle_prog(mgfvm_obstacle_prog *p)
 {
     if (!p) return;
-    free(p->dst); free(p->src); free(p->cells); free(p->codes);
+    free(p->dst); free(p->src); free(p->cells); free(p->codes); free(p->owners); free(p->fan);
     memset(p, 0, sizeof *p);
 }
