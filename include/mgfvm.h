@@ -150,6 +150,10 @@ typedef struct mgfvm_tuning {
     int restrict_slices[MGFVM_MAX_LEVELS]; /* restriction threads per cell: 1 or 3      */
     int update_pfix[MGFVM_MAX_LEVELS];     /* obstacle pressure copy inside update where
                                               legal: 0 or 2 yes, 1 no (own kernel)      */
+    int odd_chunks[MGFVM_MAX_LEVELS];      /* an odd number of tile-smoother launches may
+                                              leave the result in the ping-pong buffers
+                                              for the next kernel to take: 0 or 2 yes,
+                                              1 no (even launch counts only)            */
 } mgfvm_tuning;
 
 typedef struct mgfvm_ctx mgfvm_ctx;

@@ -227,12 +227,12 @@ __device__ __forceinline__ void cell_asm(const LevelDev &L, const CaseDev &C, co
 
 // solve_pprime's assembly: masserror :1096-1125 then coefp :1018-1092 (with the
 // p' Dirichlet rows in the order x-, x+, y-, y+) at one interior cell; returns |div|.
+// u, v: the velocity arrays to read (the fields, or the smoother's buffers holding them)
 __device__ __forceinline__ double mass_coefp_values(const LevelDev &L, const CaseDev &C, int i, int j, Coef &k,
-                                                    double &su_out)
+                                                    double &su_out, const double *u, const double *v)
 {
     const int nx = L.npx, ny = L.npy, q = j * nx + i, s = q - nx;
     const double *ax = MGF(L, S_AREAX), *ay = MGF(L, S_AREAY);
-    const double *u = MGF(L, S_U), *v = MGF(L, S_V);
     const double *apu = MGF(L, S_APU), *apv = MGF(L, S_APV);
     const double axq = ax[q], ayq = ay[q];
     double div = axq * u[q] - axq * u[q - 1] + ayq * v[q] - ayq * v[s];
@@ -251,11 +251,21 @@ __device__ __forceinline__ double mass_coefp_values(const LevelDev &L, const Cas
     return fabs(div);
 }
 
-__device__ __forceinline__ double cell_mass_coefp(const LevelDev &L, const CaseDev &C, int i, int j)
+// `from_tmp`: the u, v, sc smoothing left its results in the ping-pong buffers; they
+// are read from there and this cell's values are copied back to the fields.
+__device__ __forceinline__ double cell_mass_coefp(const LevelDev &L, const CaseDev &C, int i, int j,
+                                                  bool from_tmp = false)
 {
     Coef k;
     double su;
-    const double ad = mass_coefp_values(L, C, i, j, k, su);
+    const double *u = MGF(L, from_tmp ? S_TMP0 : S_U), *v = MGF(L, from_tmp ? S_TMP1 : S_V);
+    const double ad = mass_coefp_values(L, C, i, j, k, su, u, v);
+    if (from_tmp) {
+        const int q = j * L.npx + i;
+        if (i <= L.npx - 3) MGF(L, S_U)[q] = u[q];
+        if (j <= L.npy - 3) MGF(L, S_V)[q] = v[q];
+        MGF(L, S_SC)[q] = MGF(L, S_TMP2)[q];
+    }
     const int q = j * L.npx + i;
     MGF(L, S_PP)[q] = 0.0;
     store_coef(L, EQ_PP, q, k, su);

@@ -135,11 +135,13 @@ struct Builder {
     // unit (half-sweep of red-black GS, sweep of Jacobi) in one in-place launch;
     // otherwise the units go in an even number of tile launches of at most the level's
     // cap each, alternating field -> buffer -> field (a single launch copies back).
-    void smooth(int ig, int mode, int mask, int nsw)
+    // `tmp_ok`: the next kernel can take the result from the ping-pong buffers, so an
+    // odd number of tile launches needs no copy back.  Returns whether it is left there.
+    bool smooth(int ig, int mode, int mask, int nsw, bool tmp_ok = false)
     {
         const int isolve = x->sched.isolve;
         const int units = isolve == MGFVM_GAUSS_SEIDEL ? 2 * nsw : nsw;
-        if (units <= 0 || (isolve != MGFVM_JACOBI && isolve != MGFVM_GAUSS_SEIDEL)) return;
+        if (units <= 0 || (isolve != MGFVM_JACOBI && isolve != MGFVM_GAUSS_SEIDEL)) return false;
         const int neq = __builtin_popcount((unsigned)mask);
         const int bufs = isolve == MGFVM_JACOBI ? 2 : 1;
         // mixed precision: FP32 correction smoothing on every level but the coarsest
@@ -156,14 +158,14 @@ struct Builder {
             L.grid = dim3(1, x->ncases, neq);
             L.block = round32(mx * ((my + 1) / 2));
             L.smem = smem_for(mx * my);
-            return;
+            return false;
         }
         const int tt = x->tune.smooth_threads[ig];
         const int nt = tt == SMOOTH_BLOCK / 2 || tt == SMOOTH_BLOCK / 4 ? tt : SMOOTH_BLOCK;
         const int most = (smooth_pairs_side(0, nt) - MIN_TILE) / 2;   // units that leave a MIN_TILE tile
         const int cap = std::min(most, x->tune.smooth_units[ig] > 0 ? x->tune.smooth_units[ig] : MAX_UNITS);
         int chunks = (units + cap - 1) / cap;
-        if ((chunks & 1) && units >= chunks + 1) ++chunks;
+        if ((chunks & 1) && units >= chunks + 1 && !tmp_ok) ++chunks;
         const int hmax = (units + chunks - 1) / chunks;
         const int tile = smooth_pairs_side(hmax, nt);
         const int side = tile + 2 * hmax;
@@ -178,9 +180,11 @@ struct Builder {
             u0 += nu;
         }
         if (chunks & 1) {
+            if (tmp_ok) return true;
             Launch &L = add(K_COPY, ig, mode, cells(ig), mask);
             L.grid.z = neq;
         }
+        return false;
     }
     void pfix(int ig, int mode)
     {
@@ -229,10 +233,12 @@ struct Builder {
     // returns the update's fuse bits (0: outflow still to do)
     // `bound_bits` != 0: pbound/outflow follow the obstacle pressure copy (k_bound bits);
     // when both have work they run as one kernel, one CTA per case.
-    int solve_pp(int ig, int mode, bool reduce, int fuse, int bound_bits = 0)
+    // `uvsc_in_tmp`: the preceding u, v, sc smoothing left its results in the buffers
+    int solve_pp(int ig, int mode, bool reduce, int fuse, int bound_bits = 0, bool uvsc_in_tmp = false)
     {
-        add(K_MASS_COEFP, ig, mode, cells(ig), reduce ? 1 : 0);
-        smooth(ig, mode, 1 << EQ_PP, x->sched.nswpp);
+        add(K_MASS_COEFP, ig, mode, cells(ig), reduce ? 1 : 0, uvsc_in_tmp ? 1 : 0);
+        const bool chain = mode != M_OP && x->tune.odd_chunks[ig] != 1;
+        if (smooth(ig, mode, 1 << EQ_PP, x->sched.nswpp, chain)) fuse |= 8;
         add(K_UPDATE, ig, mode, cells(ig) + 2, fuse);
         if (fuse & 4) {                       // the copy ran inside update
             if (bound_bits) bound(ig, mode, bound_bits);
@@ -274,10 +280,11 @@ struct Builder {
             Launch &L = add(K_ASM, ig, mode, cells(ig), asm_bits(down), 1);
             L.grid.z = slices(ig, x->tune.asm_slices[ig]);
         }
-        smooth(ig, mode, (1 << EQ_U) | (1 << EQ_V) | (1 << EQ_SC), x->sched.nswpm);
+        const bool in_tmp = smooth(ig, mode, (1 << EQ_U) | (1 << EQ_V) | (1 << EQ_SC), x->sched.nswpm,
+                                   x->tune.odd_chunks[ig] != 1);
         const bool pfx = pfix_fusable(ig, mode);
         const int fuse = outflow_fusable(ig, mode, pfx) ? (down ? 1 : 3) : 0;
-        solve_pp(ig, mode, reduce, fuse | (pfx ? 4 : 0), fuse ? 0 : (down ? 3 : 7));
+        solve_pp(ig, mode, reduce, fuse | (pfx ? 4 : 0), fuse ? 0 : (down ? 3 : 7), in_tmp);
     }
     // :211-220
     // `coarse_asm`: also run the coarse level's down-leg assembly (see k_restrict)
@@ -1093,6 +1100,7 @@ static bool tuning_valid(const mgfvm_tuning &t)
         for (int v : {t.asm_slices[ig], t.restrict_slices[ig]})
             if (v != 0 && v != 1 && v != 3) return false;
         if (t.update_pfix[ig] < 0 || t.update_pfix[ig] > 2) return false;
+        if (t.odd_chunks[ig] < 0 || t.odd_chunks[ig] > 2) return false;
     }
     return true;
 }

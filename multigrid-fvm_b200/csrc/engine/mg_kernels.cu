@@ -135,7 +135,8 @@ __global__ void __launch_bounds__(BLOCK) k_asm(const CaseDev *__restrict__ cs, C
 }
 
 // update :1127-1152; with `fuse` bit 1 also outflow :1211-1228 of u, v, p (bit 2: and
-// sc), with bit 4 also update's obstacle pressure copy (:1153-1177).  The copy gives
+// sc), with bit 4 also update's obstacle pressure copy (:1153-1177); bit 8: p' is in its
+// ping-pong buffer (an odd number of smoother launches), read from there and copied back.  The copy gives
 // every destination the post-update pressure of its source; each is written by one
 // thread, the one updating the source (or, for a source on the boundary ring, the
 // nearest interior cell, which reads it before writing anything), and destinations
@@ -156,11 +157,12 @@ __global__ void __launch_bounds__(BLOCK) k_update(const CaseDev *__restrict__ cs
     if (cell_at(d, t, i, j)) {
         const int q = j * nx + i;
         double *u = MGF(L, S_U), *v = MGF(L, S_V), *p = MGF(L, S_P);
-        const double *pp = MGF(L, S_PP);
+        const double *pp = MGF(L, (fuse & 8) ? S_TMP0 : S_PP);
         const double ppref = 0.0, ppq = pp[q];
         const double un = u[q] + MGF(L, S_AREAX)[q] * (ppq - pp[q + 1]) / MGF(L, S_APU)[q];
         const double vn = v[q] + MGF(L, S_AREAY)[q] * (ppq - pp[q + nx]) / MGF(L, S_APV)[q];
         const double pn = p[q] + C.relxp * (ppq - ppref);
+        if (fuse & 8) MGF(L, S_PP)[q] = ppq;
         const int code = ((fuse & 4) && L.pcode) ? L.pcode[q] : 0;
         if (code & ~PCODE_DST) {
             for (int k = (code & ~PCODE_DST) - 1;; ++k) {
@@ -188,7 +190,10 @@ __global__ void __launch_bounds__(BLOCK) k_update(const CaseDev *__restrict__ cs
 }
 
 // masserror + coefp; with `reduce`, sum|div| of this level lands in C.last_err.
-__global__ void __launch_bounds__(BLOCK) k_mass_coefp(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode, int reduce)
+// `from_tmp`: u, v, sc are in their ping-pong buffers (an odd number of smoother
+// launches); read from there and copied back.
+__global__ void __launch_bounds__(BLOCK) k_mass_coefp(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode, int reduce,
+                                                      int from_tmp)
 {
     CASE_PROLOGUE(mode);
     const Dom d = dom_interior(L);
@@ -196,7 +201,7 @@ __global__ void __launch_bounds__(BLOCK) k_mass_coefp(const CaseDev *__restrict_
     if ((int)blockIdx.x >= nb) return;
     double a[1] = {0.0};
     int i, j;
-    if (cell_at(d, t, i, j)) a[0] = cell_mass_coefp(L, C, i, j);
+    if (cell_at(d, t, i, j)) a[0] = cell_mass_coefp(L, C, i, j, from_tmp != 0);
     if (!reduce) return;
     block_sum<1>(a);
     if (publish_partials<1>(C.partials, &C.counters[0], a, nb)) {
@@ -957,7 +962,7 @@ cudaError_t launch_one(const Launch &X, const CaseDev *dc, CaseState *ds, const 
         if (X.a1) k_asm<1><<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, (unsigned)X.a0);
         else k_asm<0><<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, (unsigned)X.a0);
         break;
-    case K_MASS_COEFP: k_mass_coefp<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, X.a0); break;
+    case K_MASS_COEFP: k_mass_coefp<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1); break;
     case K_UPDATE: k_update<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, X.a0); break;
     case K_PFIX: k_pfix<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, X.a0); break;
     case K_BOUND: k_bound<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, X.a0); break;
