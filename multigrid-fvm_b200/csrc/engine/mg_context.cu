@@ -236,10 +236,22 @@ struct Builder {
     // `uvsc_in_tmp`: the preceding u, v, sc smoothing left its results in the buffers
     int solve_pp(int ig, int mode, bool reduce, int fuse, int bound_bits = 0, bool uvsc_in_tmp = false)
     {
-        add(K_MASS_COEFP, ig, mode, cells(ig), reduce ? 1 : 0, uvsc_in_tmp ? 1 : 0);
-        const bool chain = mode != M_OP && x->tune.odd_chunks[ig] != 1;
-        if (smooth(ig, mode, 1 << EQ_PP, x->sched.nswpp, chain)) fuse |= 8;
-        add(K_UPDATE, ig, mode, cells(ig) + 2, fuse);
+        int mx, my;
+        const bool mixed = x->opt.precision == MGFVM_PREC_MIXED && ig < min_ngrid() - 1;
+        const int units = x->sched.isolve == MGFVM_GAUSS_SEIDEL ? 2 * x->sched.nswpp : x->sched.nswpp;
+        if (mode != M_OP && !mixed && !uvsc_in_tmp && units > 0 && x->tune.pp_level[ig] != 1 &&
+            (x->sched.isolve == MGFVM_JACOBI || x->sched.isolve == MGFVM_GAUSS_SEIDEL) && whole_level(ig, mx, my)) {
+            // the level fits one CTA per case: masserror + coefp, smoothing and update in one kernel
+            Launch &L = add(K_PP_LEVEL, ig, mode, 0, units, reduce ? 1 : 0, fuse);
+            L.grid = dim3(1, x->ncases);
+            L.block = round32(mx * ((my + 1) / 2));
+            L.smem = (x->sched.isolve == MGFVM_JACOBI ? 2 : 1) * mx * my * (int)sizeof(double);
+        } else {
+            add(K_MASS_COEFP, ig, mode, cells(ig), reduce ? 1 : 0, uvsc_in_tmp ? 1 : 0);
+            const bool chain = mode != M_OP && x->tune.odd_chunks[ig] != 1;
+            if (smooth(ig, mode, 1 << EQ_PP, x->sched.nswpp, chain)) fuse |= 8;
+            add(K_UPDATE, ig, mode, cells(ig) + 2, fuse);
+        }
         if (fuse & 4) {                       // the copy ran inside update
             if (bound_bits) bound(ig, mode, bound_bits);
             return fuse;
@@ -1101,6 +1113,7 @@ static bool tuning_valid(const mgfvm_tuning &t)
             if (v != 0 && v != 1 && v != 3) return false;
         if (t.update_pfix[ig] < 0 || t.update_pfix[ig] > 2) return false;
         if (t.odd_chunks[ig] < 0 || t.odd_chunks[ig] > 2) return false;
+        if (t.pp_level[ig] < 0 || t.pp_level[ig] > 2) return false;
     }
     return true;
 }

@@ -146,6 +146,39 @@ __global__ void __launch_bounds__(BLOCK) k_asm(const CaseDev *__restrict__ cs, C
 // i = npx-3 writes its new u to its face and the outlet face, the cell at i = npx-2 its
 // new v and p to the ghost column (its copy's owner the copied p), and two extra
 // threads copy the ghosts of the boundary rows.
+// One interior cell of update (+ the fusions above): ppq, ppe, ppn = p' at the cell and
+// its east and north neighbours.
+__device__ __forceinline__ void update_cell(const LevelDev &L, const CaseDev &C, int i, int j, double ppq, double ppe,
+                                            double ppn, bool out, int fuse)
+{
+    const int nx = L.npx, q = j * nx + i;
+    double *u = MGF(L, S_U), *v = MGF(L, S_V), *p = MGF(L, S_P);
+    const double ppref = 0.0;
+    const double un = u[q] + MGF(L, S_AREAX)[q] * (ppq - ppe) / MGF(L, S_APU)[q];
+    const double vn = v[q] + MGF(L, S_AREAY)[q] * (ppq - ppn) / MGF(L, S_APV)[q];
+    const double pn = p[q] + C.relxp * (ppq - ppref);
+    const int code = ((fuse & 4) && L.pcode) ? L.pcode[q] : 0;
+    if (code & ~PCODE_DST) {
+        for (int k = (code & ~PCODE_DST) - 1;; ++k) {
+            const int e = L.pfan[2 * k], src = L.pfan[2 * k + 1], dq = e & ~PFAN_END;
+            const double val = src < 0 ? pn : p[src];
+            p[dq] = val;
+            if (out && dq % nx == nx - 2) p[dq + 1] = val;
+            if (e & PFAN_END) break;
+        }
+    }
+    const bool dst = (code & PCODE_DST) != 0;
+    if (!out || i != nx - 2) u[q] = un;
+    v[q] = vn;
+    if (!dst) p[q] = pn;
+    if (out && i == nx - 3) u[q + 1] = un;
+    if (out && i == nx - 2) {
+        v[q + 1] = vn;
+        if (!dst) p[q + 1] = pn;
+        if (fuse & 2) MGF(L, S_SC)[q + 1] = MGF(L, S_SC)[q];
+    }
+}
+
 __global__ void __launch_bounds__(BLOCK) k_update(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode,
                                                   int fuse)
 {
@@ -156,33 +189,10 @@ __global__ void __launch_bounds__(BLOCK) k_update(const CaseDev *__restrict__ cs
     int i, j;
     if (cell_at(d, t, i, j)) {
         const int q = j * nx + i;
-        double *u = MGF(L, S_U), *v = MGF(L, S_V), *p = MGF(L, S_P);
         const double *pp = MGF(L, (fuse & 8) ? S_TMP0 : S_PP);
-        const double ppref = 0.0, ppq = pp[q];
-        const double un = u[q] + MGF(L, S_AREAX)[q] * (ppq - pp[q + 1]) / MGF(L, S_APU)[q];
-        const double vn = v[q] + MGF(L, S_AREAY)[q] * (ppq - pp[q + nx]) / MGF(L, S_APV)[q];
-        const double pn = p[q] + C.relxp * (ppq - ppref);
+        const double ppq = pp[q];
         if (fuse & 8) MGF(L, S_PP)[q] = ppq;
-        const int code = ((fuse & 4) && L.pcode) ? L.pcode[q] : 0;
-        if (code & ~PCODE_DST) {
-            for (int k = (code & ~PCODE_DST) - 1;; ++k) {
-                const int e = L.pfan[2 * k], src = L.pfan[2 * k + 1], dq = e & ~PFAN_END;
-                const double val = src < 0 ? pn : p[src];
-                p[dq] = val;
-                if (out && dq % nx == nx - 2) p[dq + 1] = val;
-                if (e & PFAN_END) break;
-            }
-        }
-        const bool dst = (code & PCODE_DST) != 0;
-        if (!out || i != nx - 2) u[q] = un;
-        v[q] = vn;
-        if (!dst) p[q] = pn;
-        if (out && i == nx - 3) u[q + 1] = un;
-        if (out && i == nx - 2) {
-            v[q + 1] = vn;
-            if (!dst) p[q + 1] = pn;
-            if (fuse & 2) MGF(L, S_SC)[q + 1] = MGF(L, S_SC)[q];
-        }
+        update_cell(L, C, i, j, ppq, pp[q + 1], pp[q + nx], out, fuse);
     } else if (out && t < n + 2) {
         const int jb = t == n ? 0 : L.npy - 1;
         row_outflow(L, jb, (fuse & 2) != 0);
@@ -420,6 +430,108 @@ __global__ void __launch_bounds__(NT, SMOOTH_BLOCK / NT) k_smooth(const CaseDev 
     const double *res = (ISOLVE == MGFVM_JACOBI && (nu & 1)) ? phi2 : phi;
     if (P.outA) dst[P.gA] = res[kA];
     if (P.outB) dst[P.gB] = res[kB];
+}
+
+// solve_pprime and update on a level that one CTA per case holds (at most SMOOTH_BLOCK
+// vertical cell pairs): masserror + coefp for every interior cell (:1096-1125,
+// :1018-1092), all `nu` p' units in shared memory (as k_smooth with one tile), then
+// update (:1127-1152) with k_update's fusions (`fuse` bits 1, 2, 4) reading p' from
+// shared memory, and the final p' written to the field.  The p' coefficients stay in
+// registers (nothing else reads them).  With `reduce` the level's sum |div| (a block
+// tree) becomes the case's mass error.  Same bits as the separate kernels.
+template <int ISOLVE>
+__global__ void __launch_bounds__(SMOOTH_BLOCK, 1) k_pp_level(const CaseDev *__restrict__ cs, CaseState *st, int ig,
+                                                              int mode, int nu, int reduce, int fuse)
+{
+    extern __shared__ double sm[];
+    const CaseDev &C = cs[blockIdx.y];
+    CaseState &ST = st[blockIdx.y];
+    if (!case_active(C, ST, ig, mode)) return;
+    const LevelDev &L = C.lv[ig];
+    PairTile P;
+    const int g = pair_tile(L, EQ_PP, nu, max(L.npx, L.npy), P);
+    if (g == 1) return;
+    if (g == 2) {
+        if (threadIdx.x == 0) atomicOr(&ST.status, (int)CASE_BAD_LAUNCH);
+        return;
+    }
+    const int W = P.W, kA = P.kA, kB = P.kB, limA = P.limA, limB = P.limB;
+    double *phi = sm, *phi2 = sm + W * P.Hh;
+    const double *u = MGF(L, S_U), *v = MGF(L, S_V);
+    double *pp = MGF(L, S_PP);
+    double A[6] = {0, 0, 0, 0, 0, 0}, B[6] = {0, 0, 0, 0, 0, 0}, pA = 0.0, pB = 0.0, divs = 0.0;
+    {
+        Coef k;
+        double su;
+        if (P.okA) {
+            if (limA >= 0) {
+                divs += mass_coefp_values(L, C, P.i, P.jA, k, su, u, v);
+                A[0] = k.aw; A[1] = k.ae; A[2] = k.as; A[3] = k.an; A[4] = k.ap; A[5] = su;
+            } else {
+                pA = pp[P.gA];      // boundary ring: masserror leaves it
+            }
+        }
+        if (P.okB) {
+            if (limB >= 0) {
+                divs += mass_coefp_values(L, C, P.i, P.jB, k, su, u, v);
+                B[0] = k.aw; B[1] = k.ae; B[2] = k.as; B[3] = k.an; B[4] = k.ap; B[5] = su;
+            } else {
+                pB = pp[P.gB];
+            }
+        }
+    }
+    const double eps = ISOLVE == MGFVM_JACOBI ? 1.0e-30 : 0.0;
+    const Recip RA = make_recip(ISOLVE == MGFVM_JACOBI ? A[4] + eps : A[4]);
+    const Recip RB = make_recip(ISOLVE == MGFVM_JACOBI ? B[4] + eps : B[4]);
+    if (P.okA) {
+        phi[kA] = pA;
+        if (ISOLVE == MGFVM_JACOBI) phi2[kA] = pA;
+    }
+    if (P.okB) {
+        phi[kB] = pB;
+        if (ISOLVE == MGFVM_JACOBI) phi2[kB] = pB;
+    }
+    __syncthreads();
+    for (int h = 1; h <= nu; ++h) {
+        if (ISOLVE == MGFVM_GAUSS_SEIDEL) {
+            if (((h - 1) & 1) == 0) {
+                if (h <= limA)
+                    phi[kA] = gs_value_r(A[0], A[1], A[2], A[3], RA, A[5], phi[kA - 1], phi[kA + 1], phi[kA - W],
+                                         phi[kA + W]);
+            } else {
+                if (h <= limB)
+                    phi[kB] = gs_value_r(B[0], B[1], B[2], B[3], RB, B[5], phi[kB - 1], phi[kB + 1], phi[kB - W],
+                                         phi[kB + W]);
+            }
+        } else {
+            const double *cur = ((h - 1) & 1) ? phi2 : phi;
+            double *nxt = ((h - 1) & 1) ? phi : phi2;
+            if (h <= limA)
+                nxt[kA] = jacobi_value_r(A[0], A[1], A[2], A[3], RA, A[5], cur[kA - 1], cur[kA + 1], cur[kA - W],
+                                         cur[kA + W], cur[kA]);
+            if (h <= limB)
+                nxt[kB] = jacobi_value_r(B[0], B[1], B[2], B[3], RB, B[5], cur[kB - 1], cur[kB + 1], cur[kB - W],
+                                         cur[kB + W], cur[kB]);
+        }
+        __syncthreads();
+    }
+    const double *res = (ISOLVE == MGFVM_JACOBI && (nu & 1)) ? phi2 : phi;
+    const bool out = (fuse & 1) && C.ibc_xp == 4;
+    // the region is the padded level (W = npx), so shared and global indices coincide
+    if (limA >= 0) {
+        pp[P.gA] = res[kA];
+        update_cell(L, C, P.i, P.jA, res[kA], res[kA + 1], res[kA + W], out, fuse);
+    }
+    if (limB >= 0) {
+        pp[P.gB] = res[kB];
+        update_cell(L, C, P.i, P.jB, res[kB], res[kB + 1], res[kB + W], out, fuse);
+    }
+    if (out && threadIdx.x < 2) row_outflow(L, threadIdx.x == 0 ? 0 : L.npy - 1, (fuse & 2) != 0);
+    if (reduce) {
+        double a[1] = {divs};
+        block_sum<1>(a);
+        if (threadIdx.x == 0) ST.last_err = a[0];
+    }
 }
 
 // Mixed-precision variant (MGFVM_PREC_MIXED): the same tiles, units and windows, run
@@ -992,6 +1104,13 @@ cudaError_t launch_one(const Launch &X, const CaseDev *dc, CaseState *ds, const 
         }
         break;
     case K_COPY: k_copy<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, X.a0); break;
+    case K_PP_LEVEL:
+        if (b > SMOOTH_BLOCK) return cudaErrorInvalidValue;
+        if (S.isolve == MGFVM_JACOBI)
+            k_pp_level<MGFVM_JACOBI><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2);
+        else
+            k_pp_level<MGFVM_GAUSS_SEIDEL><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2);
+        break;
     case K_PFIX_BOUND: k_pfix_bound<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, X.a0); break;
     case K_RESTV_FLUXES: k_restv_fluxes<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode); break;
     case K_RESTRICT: k_restrict<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, (unsigned)X.a0); break;

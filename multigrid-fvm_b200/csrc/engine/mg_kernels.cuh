@@ -21,6 +21,8 @@ enum KernelId {
     K_TAIL, K_ENDCYCLE, K_PROL_APPLY_END,
     K_SMOOTH_MIXED,  // as K_SMOOTH, FP32 correction smoothing with an FP64 residual
     K_PFIX_BOUND,    // K_PFIX then K_BOUND (a0 = bits), one CTA per case
+    K_PP_LEVEL,      // masserror+coefp, p' smoothing, update on a one-CTA level: a0 = units,
+                     // a1 = reduce, a2 = update fuse bits
     K_NKERNELS
 };
 
