@@ -143,3 +143,41 @@ def test_sweep_driver_arguments(tmp_path):
     assert r.returncode == 2 and "usage" in r.stderr
     r = subprocess.run([sweep], cwd=tmp_path, capture_output=True, text=True, timeout=60)
     assert r.returncode == 1 and "pattern_*.txt" in r.stderr
+
+
+def _read_pattern(path):
+    lines = open(path).read().split("\n")
+    n = int(lines[0])
+    return [tuple(int(v) for v in l.split()) for l in lines[1:1 + n]]
+
+
+def _read_pgm(path):
+    tok = open(path).read().split()
+    assert tok[0] == "P2" and tok[3] == "255"
+    w, h = int(tok[1]), int(tok[2])
+    return np.array([int(v) for v in tok[4:]], dtype=np.int32).reshape(h, w)
+
+
+def test_pattern_generator_tool(tmp_path):
+    """bin/mgfvm_patterns writes the reference generators' directory layout and file
+    formats, with the seeded library generators' patterns."""
+    import subprocess
+    from mgfvm import patterns
+    tool = os.path.join(REPO, "multigrid-fvm_b200", "bin", "mgfvm_patterns")
+    r = subprocess.run([tool, "staggered", "16", "3", "1", "1", "2", "7"], cwd=tmp_path, capture_output=True,
+                       text=True, timeout=60)
+    assert r.returncode == 0, r.stderr
+    d = tmp_path / "n16_por_75.0_sx1_sy1_scale1x"
+    for v in (1, 2, 3, 4):
+        g = patterns.staggered_grid(16, "full", 1, 1, variant=v, seed=7)
+        assert _read_pattern(d / f"pattern_{v}.txt") == patterns.pixels(g)
+        assert np.array_equal(_read_pgm(d / f"pattern_{v}.pgm"), np.where(g == 1, 0, 255))
+    r = subprocess.run([tool, "random", "20", "0.3", "2", "50", "30", "20", "5"], cwd=tmp_path,
+                       capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, r.stderr
+    d = tmp_path / "n_20" / "p_0.30"
+    for p in (1, 2):
+        g, rects = patterns.random_grid(20, 0.3, (50.0, 30.0, 20.0), seed=5 + p - 1)
+        assert _read_pattern(d / f"pattern_{p}.txt") == rects
+        assert np.array_equal(_read_pgm(d / f"pattern_{p}.pgm"), np.where(g == 1, 0, 255))
+    assert subprocess.run([tool, "bogus"], cwd=tmp_path, capture_output=True, timeout=60).returncode == 2
