@@ -228,3 +228,37 @@ def test_autotune_keeps_state(oracle_built):
     es, _ = s.history(0)
     assert len(es) == 5
     np.testing.assert_allclose(es, o.history()[0], rtol=ERR_RTOL, atol=0)
+
+
+@pytest.mark.parametrize("kw", [dict(n=32, ngrid=1, isolve=2), dict(n=32, ngrid=1, isolve=1),
+                                dict(n=8, ngrid=2, isolve=2), dict(n=16, ngrid=4, isolve=1)])
+def test_edge_sizes_bitexact(kw, oracle_built):
+    """One level (no multigrid), a tiny grid, and a coarsest level of 2 x 2 cells."""
+    from mgfvm import configs
+    n, ng, iso = kw["n"], kw["ngrid"], kw["isolve"]
+    cfg = configs.small(n, ng, isolve=iso)
+    s, o = _pair(cfg)
+    for c in (1, 4):
+        s.cycle(c)
+        o.cycle(c)
+        _compare(s, o, STATE, what=f"n={n} ngrid={ng} after +{c} cycles")
+    s.close()
+
+
+def test_zero_cycles_and_mixed_depth_batch(oracle_built):
+    """solve(0) runs nothing; a batch whose cases have different level counts, where
+    the shallow case stops early under the reference rule, keeps the deep one going."""
+    from mgfvm import Solver, configs
+    from oracle import OracleCase
+    deep = configs.small(32, 3, isolve=2)
+    shallow = configs.small(16, 2, isolve=2, convergence=1e30)   # stops after one cycle
+    s = Solver([deep, shallow])
+    assert list(s.solve(0, 0.0)) == [0, 0]
+    ran = s.solve(5, 0.0)
+    assert list(ran) == [5, 1]
+    od, osh = OracleCase(deep), OracleCase(shallow)
+    od.cycle(5)
+    osh.cycle(1)
+    _compare(s, od, STATE, case=0, what="deep case")
+    _compare(s, osh, STATE, case=1, what="shallow case")
+    s.close()
