@@ -236,22 +236,15 @@ struct Builder {
     // `uvsc_in_tmp`: the preceding u, v, sc smoothing left its results in the buffers
     int solve_pp(int ig, int mode, bool reduce, int fuse, int bound_bits = 0, bool uvsc_in_tmp = false)
     {
-        int mx, my;
-        const bool mixed = x->opt.precision == MGFVM_PREC_MIXED && ig < min_ngrid() - 1;
-        const int units = x->sched.isolve == MGFVM_GAUSS_SEIDEL ? 2 * x->sched.nswpp : x->sched.nswpp;
-        if (mode != M_OP && !mixed && !uvsc_in_tmp && units > 0 && x->tune.pp_level[ig] != 1 &&
-            (x->sched.isolve == MGFVM_JACOBI || x->sched.isolve == MGFVM_GAUSS_SEIDEL) && whole_level(ig, mx, my)) {
-            // the level fits one CTA per case: masserror + coefp, smoothing and update in one kernel
-            Launch &L = add(K_PP_LEVEL, ig, mode, 0, units, reduce ? 1 : 0, fuse);
-            L.grid = dim3(1, x->ncases);
-            L.block = round32(mx * ((my + 1) / 2));
-            L.smem = (x->sched.isolve == MGFVM_JACOBI ? 2 : 1) * mx * my * (int)sizeof(double);
-        } else {
-            add(K_MASS_COEFP, ig, mode, cells(ig), reduce ? 1 : 0, uvsc_in_tmp ? 1 : 0);
-            const bool chain = mode != M_OP && x->tune.odd_chunks[ig] != 1;
-            if (smooth(ig, mode, 1 << EQ_PP, x->sched.nswpp, chain)) fuse |= 8;
-            add(K_UPDATE, ig, mode, cells(ig) + 2, fuse);
-        }
+        add(K_MASS_COEFP, ig, mode, cells(ig), reduce ? 1 : 0, uvsc_in_tmp ? 1 : 0);
+        const bool chain = mode != M_OP && x->tune.odd_chunks[ig] != 1;
+        if (smooth(ig, mode, 1 << EQ_PP, x->sched.nswpp, chain)) fuse |= 8;
+        add(K_UPDATE, ig, mode, cells(ig) + 2, fuse);
+        return after_update(ig, mode, fuse, bound_bits);
+    }
+    // the obstacle pressure copy (unless update did it: fuse bit 4) and pbound/outflow
+    int after_update(int ig, int mode, int fuse, int bound_bits)
+    {
         if (fuse & 4) {                       // the copy ran inside update
             if (bound_bits) bound(ig, mode, bound_bits);
             return fuse;
@@ -288,6 +281,27 @@ struct Builder {
     static int slices(int, int knob) { return knob == 1 ? 1 : 3; }
     void step(int ig, int mode, bool down, bool reduce, bool asm_done = false)
     {
+        int mx, my;
+        const bool mixed = x->opt.precision == MGFVM_PREC_MIXED && ig < min_ngrid() - 1;
+        const int isolve = x->sched.isolve;
+        const int ppu = isolve == MGFVM_GAUSS_SEIDEL ? 2 * x->sched.nswpp : x->sched.nswpp;
+        const int mu = isolve == MGFVM_GAUSS_SEIDEL ? 2 * x->sched.nswpm : x->sched.nswpm;
+        if (mode != M_OP && !mixed && ppu > 0 && x->tune.pp_level[ig] != 1 &&
+            (isolve == MGFVM_JACOBI || isolve == MGFVM_GAUSS_SEIDEL) && whole_level(ig, mx, my)) {
+            // the whole visit (assembly, u/v/sc smoothing, p' and update) in one launch
+            const bool pfx = pfix_fusable(ig, mode);
+            const int fuse = outflow_fusable(ig, mode, pfx) ? (down ? 1 : 3) : 0;
+            const int what = asm_done ? 0 : (int)asm_bits(down);
+            const bool visit = what != 0 || mu > 0;
+            Launch &L = add(visit ? K_LEVEL_VISIT : K_PP_LEVEL, ig, mode, 0, ppu, reduce ? 1 : 0,
+                            fuse | (pfx ? 4 : 0), what);
+            L.a4 = std::max(mu, 0);
+            L.grid = dim3(visit ? 3 : 1, x->ncases);
+            L.block = round32(mx * ((my + 1) / 2));
+            L.smem = (isolve == MGFVM_JACOBI ? 2 : 1) * mx * my * (int)sizeof(double);
+            after_update(ig, mode, fuse | (pfx ? 4 : 0), fuse ? 0 : (down ? 3 : 7));
+            return;
+        }
         if (!asm_done) {
             Launch &L = add(K_ASM, ig, mode, cells(ig), asm_bits(down), 1);
             L.grid.z = slices(ig, x->tune.asm_slices[ig]);

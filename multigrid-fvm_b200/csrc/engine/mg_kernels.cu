@@ -298,14 +298,15 @@ struct PairTile {
 };
 
 // 0: this CTA has work, 1: it has none, 2: the launch is too small for its region.
-__device__ __forceinline__ int pair_tile(const LevelDev &L, int e, int nu, int tile, PairTile &P)
+// `bx` picks the tile (blockIdx.x in the tiled smoothers).
+__device__ __forceinline__ int pair_tile(const LevelDev &L, int e, int nu, int tile, PairTile &P, int bx)
 {
     P.d = dom_eq(L, e);
     const Dom &d = P.d;
     if (d.wi <= 0 || d.wj <= 0) return 1;
     const int tx_n = (d.wi + tile - 1) / tile, ty_n = (d.wj + tile - 1) / tile;
-    if ((int)blockIdx.x >= tx_n * ty_n) return 1;
-    const int tx = blockIdx.x % tx_n, ty = blockIdx.x / tx_n;
+    if (bx >= tx_n * ty_n) return 1;
+    const int tx = bx % tx_n, ty = bx / tx_n;
     P.dx1 = d.i0 + d.wi - 1;
     P.dy1 = d.j0 + d.wj - 1;
     P.x0 = d.i0 + tx * tile;
@@ -364,7 +365,7 @@ __global__ void __launch_bounds__(NT, SMOOTH_BLOCK / NT) k_smooth(const CaseDev 
     const int e = nth_eq(mask, blockIdx.z);
     const LevelDev &L = C.lv[ig];
     PairTile P;
-    const int g = pair_tile(L, e, nu, tile, P);
+    const int g = pair_tile(L, e, nu, tile, P, blockIdx.x);
     if (g == 1) return;
     if (g == 2) {     // the schedule sizes blocks to fit; never taken
         if (threadIdx.x == 0) atomicOr(&st[blockIdx.y].status, (int)CASE_BAD_LAUNCH);
@@ -432,6 +433,62 @@ __global__ void __launch_bounds__(NT, SMOOTH_BLOCK / NT) k_smooth(const CaseDev 
     if (P.outB) dst[P.gB] = res[kB];
 }
 
+// All `mu` units of equation e on a level that one CTA holds, in place (k_smooth with
+// one tile covering the domain).  Returns pair_tile's verdict (uniform over the CTA).
+template <int ISOLVE>
+__device__ __forceinline__ int level_smooth_eq(const LevelDev &L, int e, int mu, double *sm)
+{
+    PairTile P;
+    const int g = pair_tile(L, e, mu, max(L.npx, L.npy), P, 0);
+    if (g != 0) return g;
+    const int W = P.W, kA = P.kA, kB = P.kB, limA = P.limA, limB = P.limB;
+    double *phi = sm, *phi2 = sm + W * P.Hh, *fld = MGF(L, eq_field(e));
+    double A[6] = {0, 0, 0, 0, 0, 0}, B[6] = {0, 0, 0, 0, 0, 0};
+    if (P.okA) {
+        const double pa = fld[P.gA];
+        for (int a = 0; a < 6; ++a) A[a] = MGF(L, co_slot(e, a))[P.gA];
+        phi[kA] = pa;
+        if (ISOLVE == MGFVM_JACOBI) phi2[kA] = pa;
+    }
+    if (P.okB) {
+        const double pb = fld[P.gB];
+        for (int a = 0; a < 6; ++a) B[a] = MGF(L, co_slot(e, a))[P.gB];
+        phi[kB] = pb;
+        if (ISOLVE == MGFVM_JACOBI) phi2[kB] = pb;
+    }
+    const double eps = ISOLVE == MGFVM_JACOBI ? 1.0e-30 : 0.0;
+    const Recip RA = make_recip(ISOLVE == MGFVM_JACOBI ? A[4] + eps : A[4]);
+    const Recip RB = make_recip(ISOLVE == MGFVM_JACOBI ? B[4] + eps : B[4]);
+    __syncthreads();
+    for (int h = 1; h <= mu; ++h) {
+        if (ISOLVE == MGFVM_GAUSS_SEIDEL) {
+            if (((h - 1) & 1) == 0) {
+                if (h <= limA)
+                    phi[kA] = gs_value_r(A[0], A[1], A[2], A[3], RA, A[5], phi[kA - 1], phi[kA + 1], phi[kA - W],
+                                         phi[kA + W]);
+            } else {
+                if (h <= limB)
+                    phi[kB] = gs_value_r(B[0], B[1], B[2], B[3], RB, B[5], phi[kB - 1], phi[kB + 1], phi[kB - W],
+                                         phi[kB + W]);
+            }
+        } else {
+            const double *cur = ((h - 1) & 1) ? phi2 : phi;
+            double *nxt = ((h - 1) & 1) ? phi : phi2;
+            if (h <= limA)
+                nxt[kA] = jacobi_value_r(A[0], A[1], A[2], A[3], RA, A[5], cur[kA - 1], cur[kA + 1], cur[kA - W],
+                                         cur[kA + W], cur[kA]);
+            if (h <= limB)
+                nxt[kB] = jacobi_value_r(B[0], B[1], B[2], B[3], RB, B[5], cur[kB - 1], cur[kB + 1], cur[kB - W],
+                                         cur[kB + W], cur[kB]);
+        }
+        __syncthreads();
+    }
+    const double *res = (ISOLVE == MGFVM_JACOBI && (mu & 1)) ? phi2 : phi;
+    if (limA >= 0) fld[P.gA] = res[kA];
+    if (limB >= 0) fld[P.gB] = res[kB];
+    return 0;
+}
+
 // solve_pprime and update on a level that one CTA per case holds (at most SMOOTH_BLOCK
 // vertical cell pairs): masserror + coefp for every interior cell (:1096-1125,
 // :1018-1092), all `nu` p' units in shared memory (as k_smooth with one tile), then
@@ -440,16 +497,11 @@ __global__ void __launch_bounds__(NT, SMOOTH_BLOCK / NT) k_smooth(const CaseDev 
 // registers (nothing else reads them).  With `reduce` the level's sum |div| (a block
 // tree) becomes the case's mass error.  Same bits as the separate kernels.
 template <int ISOLVE>
-__global__ void __launch_bounds__(SMOOTH_BLOCK, 1) k_pp_level(const CaseDev *__restrict__ cs, CaseState *st, int ig,
-                                                              int mode, int nu, int reduce, int fuse)
+__device__ __forceinline__ void pp_level_body(const CaseDev &C, CaseState &ST, const LevelDev &L, int nu, int reduce,
+                                              int fuse, double *sm)
 {
-    extern __shared__ double sm[];
-    const CaseDev &C = cs[blockIdx.y];
-    CaseState &ST = st[blockIdx.y];
-    if (!case_active(C, ST, ig, mode)) return;
-    const LevelDev &L = C.lv[ig];
     PairTile P;
-    const int g = pair_tile(L, EQ_PP, nu, max(L.npx, L.npy), P);
+    const int g = pair_tile(L, EQ_PP, nu, max(L.npx, L.npy), P, 0);
     if (g == 1) return;
     if (g == 2) {
         if (threadIdx.x == 0) atomicOr(&ST.status, (int)CASE_BAD_LAUNCH);
@@ -534,6 +586,58 @@ __global__ void __launch_bounds__(SMOOTH_BLOCK, 1) k_pp_level(const CaseDev *__r
     }
 }
 
+template <int ISOLVE>
+__global__ void __launch_bounds__(SMOOTH_BLOCK, 1) k_pp_level(const CaseDev *__restrict__ cs, CaseState *st, int ig,
+                                                              int mode, int nu, int reduce, int fuse)
+{
+    extern __shared__ double sm[];
+    const CaseDev &C = cs[blockIdx.y];
+    CaseState &ST = st[blockIdx.y];
+    if (!case_active(C, ST, ig, mode)) return;
+    pp_level_body<ISOLVE>(C, ST, C.lv[ig], nu, reduce, fuse, sm);
+}
+
+// Every thread of the cluster arrives; memory written before it (global included) is
+// visible to every thread of the cluster after it.
+__device__ __forceinline__ void cluster_barrier()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// A whole visit to a level that one CTA per case holds, as one launch of a cluster of
+// three CTAs per case (cluster rank r = blockIdx.x: u, v, sc).  CTA r runs its part of
+// the level's assembly `what` (the slices of k_asm with three slices: fluxes + u, v,
+// sc + outflow ghost) over every cell, then — once the whole cluster has assembled, as
+// the smoothers read nothing the other parts write — `mu` units of its equation in
+// place; after a second cluster barrier CTA 0 runs solve_pprime and update
+// (pp_level_body).  No thread leaves before the barriers: the case's activity is the
+// same for the three CTAs and only guards the work.
+template <int ISOLVE>
+__global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(SMOOTH_BLOCK, 1)
+    k_level_visit(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode, int nu, int reduce, int fuse,
+                  int what, int mu)
+{
+    extern __shared__ double sm[];
+    const CaseDev &C = cs[blockIdx.y];
+    CaseState &ST = st[blockIdx.y];
+    const bool active = case_active(C, ST, ig, mode);
+    const LevelDev &L = C.lv[ig];
+    const int r = blockIdx.x;
+    if (what) {
+        if (active) {
+            const unsigned w = asm_slice((unsigned)what, r, 3);
+            const int n = L.npx * L.npy;
+            for (int q = threadIdx.x; q < n; q += blockDim.x) cell_asm(L, C, FluxLive(L), q % L.npx, q / L.npx, w);
+        }
+        cluster_barrier();
+    }
+    if (active && mu > 0 && level_smooth_eq<ISOLVE>(L, r == 0 ? EQ_U : r == 1 ? EQ_V : EQ_SC, mu, sm) == 2 &&
+        threadIdx.x == 0)
+        atomicOr(&ST.status, (int)CASE_BAD_LAUNCH);   // the schedule sizes blocks to fit; never taken
+    cluster_barrier();
+    if (active && r == 0) pp_level_body<ISOLVE>(C, ST, L, nu, reduce, fuse, sm);
+}
+
 // Mixed-precision variant (MGFVM_PREC_MIXED): the same tiles, units and windows, run
 // on the correction delta of A (phi + delta) = b in FP32.  The residual r = su +
 // sum a_nb phi_nb - ap phi_P is taken in FP64 from the staged field at the start of
@@ -552,7 +656,7 @@ __global__ void __launch_bounds__(NT, SMOOTH_BLOCK / NT) k_smooth_mixed(const Ca
     const int e = nth_eq(mask, blockIdx.z);
     const LevelDev &L = C.lv[ig];
     PairTile P;
-    const int g = pair_tile(L, e, nu, tile, P);
+    const int g = pair_tile(L, e, nu, tile, P, blockIdx.x);
     if (g == 1) return;
     if (g == 2) {
         if (threadIdx.x == 0) atomicOr(&st[blockIdx.y].status, (int)CASE_BAD_LAUNCH);
@@ -1110,6 +1214,14 @@ cudaError_t launch_one(const Launch &X, const CaseDev *dc, CaseState *ds, const 
             k_pp_level<MGFVM_JACOBI><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2);
         else
             k_pp_level<MGFVM_GAUSS_SEIDEL><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2);
+        break;
+    case K_LEVEL_VISIT:
+        if (b > SMOOTH_BLOCK || g.x != 3) return cudaErrorInvalidValue;
+        if (S.isolve == MGFVM_JACOBI)
+            k_level_visit<MGFVM_JACOBI><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+        else
+            k_level_visit<MGFVM_GAUSS_SEIDEL><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3,
+                                                                     X.a4);
         break;
     case K_PFIX_BOUND: k_pfix_bound<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, X.a0); break;
     case K_RESTV_FLUXES: k_restv_fluxes<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode); break;

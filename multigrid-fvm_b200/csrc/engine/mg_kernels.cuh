@@ -23,6 +23,8 @@ enum KernelId {
     K_PFIX_BOUND,    // K_PFIX then K_BOUND (a0 = bits), one CTA per case
     K_PP_LEVEL,      // masserror+coefp, p' smoothing, update on a one-CTA level: a0 = units,
                      // a1 = reduce, a2 = update fuse bits
+    K_LEVEL_VISIT,   // a whole one-CTA level visit, a cluster of 3 CTAs per case: K_PP_LEVEL's
+                     // a0-a2, a3 = assembly bits (0: done), a4 = u/v/sc units
     K_NKERNELS
 };
 

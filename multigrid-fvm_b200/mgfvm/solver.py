@@ -180,7 +180,8 @@ class Solver:
         return ms.value, n.value
 
     KERNELS = ["fluxes", "asm", "mass_coefp", "update", "pfix", "bound", "smooth", "copy", "restv_fluxes",
-               "restrict", "prol_corr", "prol_apply", "tail", "endcycle", "prol_apply_end", "smooth_mixed", "pfix_bound", "pp_level"]
+               "restrict", "prol_corr", "prol_apply", "tail", "endcycle", "prol_apply_end", "smooth_mixed", "pfix_bound", "pp_level",
+               "level_visit"]
 
     def profile_cycle(self):
         """One directly-launched V-cycle with an event after every kernel: a list of
