@@ -154,9 +154,10 @@ typedef struct mgfvm_tuning {
                                               leave the result in the ping-pong buffers
                                               for the next kernel to take: 0 or 2 yes,
                                               1 no (even launch counts only)            */
-    int pp_level[MGFVM_MAX_LEVELS];        /* on a level one CTA per case holds: p'
-                                              assembly, smoothing and update in one
-                                              kernel: 0 or 2 yes, 1 no                  */
+    int pp_level[MGFVM_MAX_LEVELS];        /* on a level one CTA per case holds: the
+                                              whole visit (assembly, u/v/sc smoothing,
+                                              p', update) in one launch: 0 or 2 yes,
+                                              1 no                                      */
 } mgfvm_tuning;
 
 typedef struct mgfvm_ctx mgfvm_ctx;
