@@ -136,6 +136,9 @@ typedef struct mgfvm_options {
     int use_graph;     /* replay V-cycles from a captured CUDA graph (1) or launch
                           every kernel directly (0)                                   */
     int sync_every;    /* cycles between host reads of the stop flags in mgfvm_solve */
+    int tangent;       /* 1: every case also carries the derivative of its state along
+                          one parameter direction (mgfvm_set_direction); FP64 only, and
+                          the whole V-cycle runs in the one-CTA-per-case kernel       */
 } mgfvm_options;
 
 /* Per-level schedule choices (index = level; 0 = the engine's default).  Every choice
@@ -275,6 +278,44 @@ int mgfvm_set_tuning(mgfvm_ctx *ctx, const mgfvm_tuning *t);
  * under the initial and the chosen schedule (either may be NULL); `chosen` may be
  * NULL.  No counterpart in the reference. */
 int mgfvm_autotune(mgfvm_ctx *ctx, int cycles, mgfvm_tuning *chosen, double *ms_before, double *ms_after);
+
+/* ------------------------------------------------------------ derivatives
+ * Forward-mode (tangent-linear) derivatives of the V-cycle iteration.  In a context
+ * created with mgfvm_options.tangent = 1, every value of every case is paired with
+ * its derivative along the case's parameter direction; each V-cycle advances both
+ * with the reference's operations (same value bits as a plain context), so after n
+ * cycles the derivative arrays hold d(state after n cycles)/d(parameter) exactly,
+ * the quantity a central finite difference of the reference's n cycles
+ * approximates.  A batch of cases with the same inputs and different directions
+ * gives a whole gradient in one run.  No counterpart in the reference.
+ *
+ * Directions: the level-0 inlet velocity u at face row index+1 of the x- boundary
+ * (index in [0, nfy), the per-face inlet profile of mgfvm_set_inlet_profile), the
+ * viscosity amuf, the Prandtl-type number prsc (scalar diffusivity amuf/prsc). */
+enum mgfvm_direction { MGFVM_DIR_NONE = 0, MGFVM_DIR_INLET = 1, MGFVM_DIR_AMUF = 2, MGFVM_DIR_PRSC = 3 };
+
+/* Set case `icase`'s direction and return it to its initial state with the
+ * derivative seeded (zero state derivative; the inlet face's own value, the coarse
+ * faces rest_geom averages from it, or the derivatives of amu and amusc). */
+int mgfvm_set_direction(mgfvm_ctx *ctx, int icase, int kind, int index);
+
+/* Derivative array of a field (npx*npy, as mgfvm_get_field); zeros for arrays no
+ * parameter changes (face areas, obstacle sources). */
+int mgfvm_get_tangent(mgfvm_ctx *ctx, int icase, int level, int field, double *out);
+
+/* Objective of the level-0 state: J = mean_j p(1, j) - mean_j p(npx-2, j) +
+ * mean_j sc(npx-1, j) over the interior rows j = 1 .. npy-2 (uniform dy, so the
+ * dy-weighted means are plain means): the inlet-to-outlet pressure drop plus the
+ * mean outlet scalar.  *dJ (tangent contexts; may be NULL) = its derivative along
+ * the case's direction.  Either pointer may be NULL. */
+int mgfvm_objective(mgfvm_ctx *ctx, int icase, double *J, double *dJ);
+
+/* Whole gradient of J after `ncycles` V-cycles from the initial state of `cfg` with
+ * the given per-face inlet profile (may be empty): creates a tangent context of
+ * nfy + 2 cases (every inlet face, amuf, prsc) on `device`, runs it and releases it.
+ * dJ_dinlet receives nfy values; any output may be NULL. */
+int mgfvm_gradient(const mgfvm_config *cfg, const double *inlet_u, int n_inlet, int ncycles, int device,
+                   double *J, double *dJ_dinlet, double *dJ_damuf, double *dJ_dprsc);
 
 /* Bytes this context copied host->device and device->host since it was created. */
 int mgfvm_transfer_bytes(mgfvm_ctx *ctx, long long *h2d, long long *d2h);

@@ -16,6 +16,7 @@
 
 #include "mg_init.cuh"
 #include "mg_kernels.cuh"
+#include "mg_tangent.cuh"
 #include "mgfvm_host.h"
 
 using namespace mg;
@@ -72,6 +73,12 @@ struct mgfvm_ctx {
     long long h2d = 0, d2h = 0;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     double last_ms = 0.0;
+    // tangent contexts (opt.tangent): derivative storage and each case's direction
+    char *tpool = nullptr;
+    std::vector<size_t> tcase_off, tcase_bytes;   // per case: its part of tpool
+    std::vector<CaseTan> ht;
+    CaseTan *dt = nullptr;
+    std::vector<int> dir_kind, dir_index;
 };
 
 static inline int npx_of(const mgfvm_config &c, int ig) { return c.nfx / (1 << ig) + 2; }
@@ -350,8 +357,8 @@ struct Builder {
                                                          (long long)sizeof(double));
             }
             Launch L{};
-            L.kernel = K_TAIL; L.grid = dim3(x->ncases); L.block = TAIL_BLOCK;
-            L.smem = (int)std::min<long long>(need, TAIL_SMEM_MAX);
+            L.kernel = x->opt.tangent ? K_TAIL_TAN : K_TAIL; L.grid = dim3(x->ncases); L.block = TAIL_BLOCK;
+            L.smem = x->opt.tangent ? 0 : (int)std::min<long long>(need, TAIL_SMEM_MAX);
             out->push_back(L);
         }
         for (int ig = x->maxng - 1; ig > 0; --ig) {
@@ -455,7 +462,7 @@ int field_slot(int f, int eq)
 int run_list(mgfvm_ctx *x, const std::vector<Launch> &v)
 {
     for (const Launch &L : v) {
-        cudaError_t e = launch_one(L, x->dc, x->ds, x->sched, x->stream);
+        cudaError_t e = launch_one(L, x->dc, x->ds, x->dt, x->sched, x->stream);
         if (e != cudaSuccess)
             return mgfvm_fail(MGFVM_ECUDA, "kernel %d at level %d failed to launch: %s", L.kernel, L.ig,
                               cudaGetErrorString(e));
@@ -508,7 +515,7 @@ int build_graph(mgfvm_ctx *x)
     if (x->gexec) return MGFVM_OK;
     CK(cudaStreamBeginCapture(x->stream, cudaStreamCaptureModeThreadLocal));
     for (const Launch &L : x->cyc) {
-        cudaError_t e = launch_one(L, x->dc, x->ds, x->sched, x->stream);
+        cudaError_t e = launch_one(L, x->dc, x->ds, x->dt, x->sched, x->stream);
         if (e != cudaSuccess) {
             cudaGraph_t g;
             cudaStreamEndCapture(x->stream, &g);
@@ -545,6 +552,84 @@ int set_controls(mgfvm_ctx *x, int stop, double fp_tol)
     return push(x);
 }
 
+// Derivative storage of a tangent context: every slot tangent_slot() admits, on every
+// level of every case, plus each pressure-copy buffer; zero until seeded.
+int alloc_tangent(mgfvm_ctx *x)
+{
+    size_t off = 0;
+    auto take = [&](size_t bytes) { off = align_up(off, 256); size_t o = off; off += std::max<size_t>(bytes, 8); return o; };
+    std::vector<std::vector<size_t>> offs(x->ncases);
+    x->tcase_off.assign(x->ncases, 0);
+    x->tcase_bytes.assign(x->ncases, 0);
+    for (int c = 0; c < x->ncases; ++c) {
+        const mgfvm_config &g = x->cfg[c];
+        x->tcase_off[c] = align_up(off, 256);
+        for (int ig = 0; ig < g.ngrid; ++ig) {
+            const size_t n = (size_t)npx_of(g, ig) * npy_of(g, ig);
+            for (int s = 0; s < NSLOTS; ++s) offs[c].push_back(tangent_slot(s) ? take(n * sizeof(double)) : (size_t)-1);
+            const int nc = x->progs[(size_t)c * MAXLEV + ig].ncopy;
+            offs[c].push_back(take((size_t)std::max(nc, 1) * sizeof(double)));
+        }
+        x->tcase_bytes[c] = align_up(off, 256) - x->tcase_off[c];
+    }
+    const size_t bytes = align_up(off, 256);
+    cudaError_t me = cudaMalloc(&x->tpool, bytes);
+    if (me != cudaSuccess)
+        return mgfvm_fail(me == cudaErrorMemoryAllocation ? MGFVM_ENOMEM : MGFVM_ECUDA,
+                          "derivative storage of %zu bytes: %s", bytes, cudaGetErrorString(me));
+    CK(cudaMemset(x->tpool, 0, bytes));
+    x->ht.assign(x->ncases, CaseTan{});
+    for (int c = 0; c < x->ncases; ++c) {
+        size_t k = 0;
+        for (int ig = 0; ig < x->cfg[c].ngrid; ++ig) {
+            LevelTan &D = x->ht[c].lv[ig];
+            for (int s = 0; s < NSLOTS; ++s, ++k) D.t[s] = offs[c][k] == (size_t)-1 ? nullptr : (double *)(x->tpool + offs[c][k]);
+            D.pbuf_t = (double *)(x->tpool + offs[c][k++]);
+        }
+    }
+    x->dir_kind.assign(x->ncases, MGFVM_DIR_NONE);
+    x->dir_index.assign(x->ncases, 0);
+    CK(cudaMalloc(&x->dt, sizeof(CaseTan) * x->ncases));
+    CK(cudaMemcpy(x->dt, x->ht.data(), sizeof(CaseTan) * x->ncases, cudaMemcpyHostToDevice));
+    x->h2d += (long long)sizeof(CaseTan) * x->ncases;
+    return MGFVM_OK;
+}
+
+// Zero case c's derivatives and seed its direction: the level-0 inlet face (i = 0,
+// row index + 1) with the coarse faces that rest_geom averages from it (rest_geom
+// :1391-1473, as k_rest_geom), or the derivative of every level's amu and amusc =
+// amuf / prsc (coefsc :867) with respect to amuf or prsc.
+int seed_tangent(mgfvm_ctx *x, int c)
+{
+    CK(cudaMemsetAsync(x->tpool + x->tcase_off[c], 0, x->tcase_bytes[c], x->stream));
+    const mgfvm_config &g = x->cfg[c];
+    const int kind = x->dir_kind[c], idx = x->dir_index[c];
+    for (int ig = 0; ig < g.ngrid; ++ig) {
+        LevelTan &D = x->ht[c].lv[ig];
+        D.amu_t = kind == MGFVM_DIR_AMUF ? 1.0 : 0.0;
+        D.amusc_t = kind == MGFVM_DIR_AMUF ? 1.0 / g.prsc : kind == MGFVM_DIR_PRSC ? -g.amuf / (g.prsc * g.prsc) : 0.0;
+    }
+    if (kind == MGFVM_DIR_INLET) {
+        std::vector<double> col(npy_of(g, 0), 0.0);
+        col[idx + 1] = 1.0;
+        for (int ig = 0; ig < g.ngrid; ++ig) {
+            const int npx = npx_of(g, ig), npy = npy_of(g, ig);
+            if (ig > 0) {
+                std::vector<double> cc(npy, 0.0);
+                for (int jc = 1; jc <= npy - 2; ++jc) cc[jc] = 0.5 * (col[2 * jc] + col[2 * jc - 1]);
+                col.swap(cc);
+            }
+            CK(cudaMemcpy2DAsync(x->ht[c].lv[ig].t[S_U], sizeof(double) * npx, col.data(), sizeof(double),
+                                 sizeof(double), npy, cudaMemcpyHostToDevice, x->stream));
+            x->h2d += (long long)(sizeof(double) * npy);
+        }
+    }
+    CK(cudaMemcpyAsync(x->dt + c, &x->ht[c], sizeof(CaseTan), cudaMemcpyHostToDevice, x->stream));
+    x->h2d += (long long)sizeof(CaseTan);
+    CK(cudaStreamSynchronize(x->stream));
+    return MGFVM_OK;
+}
+
 int init_state(mgfvm_ctx *x, int only_case)
 {
     for (int c = 0; c < x->ncases; ++c) {
@@ -566,6 +651,9 @@ int init_state(mgfvm_ctx *x, int only_case)
     if (e != cudaSuccess) return mgfvm_fail(MGFVM_ECUDA, "init kernels: %s", cudaGetErrorString(e));
     x->launches += 3LL * x->maxng + 1 + (x->maxng - 1);
     CK(cudaStreamSynchronize(x->stream));
+    if (x->opt.tangent)
+        for (int c = 0; c < x->ncases; ++c)
+            if (only_case < 0 || c == only_case) RC(seed_tangent(x, c));
     return MGFVM_OK;
 }
 
@@ -599,6 +687,8 @@ void destroy_all(mgfvm_ctx *x)
     if (x->gexec) cudaGraphExecDestroy(x->gexec);
     if (x->graph) cudaGraphDestroy(x->graph);
     if (x->pool) cudaFree(x->pool);
+    if (x->tpool) cudaFree(x->tpool);
+    if (x->dt) cudaFree(x->dt);
     if (x->hist) cudaFree(x->hist);
     if (x->dprofile) cudaFree(x->dprofile);
     if (x->dobs) cudaFree(x->dobs);
@@ -635,6 +725,8 @@ int create_impl(const mgfvm_config *cases, int ncases, const mgfvm_options *opt_
     if (opt.sync_every < 1) opt.sync_every = 1;
     if (opt.precision != MGFVM_PREC_FP64 && opt.precision != MGFVM_PREC_MIXED)
         return mgfvm_fail(MGFVM_EINVAL, "unknown precision %d", opt.precision);
+    if (opt.tangent && opt.precision != MGFVM_PREC_FP64)
+        return mgfvm_fail(MGFVM_EINVAL, "derivatives are taken of the FP64 V-cycle only");
     x->opt = opt;
     x->device = opt.device;
     x->ncases = ncases;
@@ -723,7 +815,8 @@ int create_impl(const mgfvm_config *cases, int ncases, const mgfvm_options *opt_
         C.ibc_xm = g.ibc_xm; C.ibc_xp = g.ibc_xp; C.ibc_ym = g.ibc_ym; C.ibc_yp = g.ibc_yp;
         C.ngrid = g.ngrid;
         int tail = g.ngrid;
-        if (opt.tail_level >= 0) tail = std::min(opt.tail_level, g.ngrid);
+        if (opt.tangent) tail = 0;     // the tangent V-cycle runs in the one-CTA kernel
+        else if (opt.tail_level >= 0) tail = std::min(opt.tail_level, g.ngrid);
         else
             for (int ig = 0; ig < g.ngrid; ++ig)
                 if (npx_of(g, ig) * npy_of(g, ig) <= TAIL_AUTO_CELLS) { tail = ig; break; }
@@ -823,6 +916,7 @@ int create_impl(const mgfvm_config *cases, int ncases, const mgfvm_options *opt_
     RC(ensure_hist(x, HIST_INITIAL));
     for (int ig = 0; ig < MAXLEV; ++ig) x->last_eq[ig] = EQ_SC;
     CK(configure_kernels());
+    if (opt.tangent) RC(alloc_tangent(x));
     RC(init_state(x, -1));
     Builder b{x, &x->cyc};
     b.cycle();
@@ -1006,6 +1100,7 @@ int mgfvm_field_device_ptr(mgfvm_ctx *x, int icase, int level, int field, double
 int mgfvm_set_field(mgfvm_ctx *x, int icase, int level, int field, const double *in)
 {
     RC(check_ctx(x));
+    if (x->opt.tangent) return mgfvm_fail(MGFVM_EINVAL, "%s: not available in a tangent context (it would change the state without its derivatives)", __func__);
     RC(check_case_level(x, icase, level));
     if (field < 0 || field >= MGFVM_NFIELDS || !in) return mgfvm_fail(MGFVM_EINVAL, "bad field %d", field);
     CK(cudaStreamSynchronize(x->stream));
@@ -1039,6 +1134,7 @@ int mgfvm_get_obstacle_ranges(mgfvm_ctx *x, int icase, int level, int *out)
 int mgfvm_op(mgfvm_ctx *x, int op, int level)
 {
     RC(check_ctx(x));
+    if (x->opt.tangent) return mgfvm_fail(MGFVM_EINVAL, "%s: not available in a tangent context (it would change the state without its derivatives)", __func__);
     if (op < 0 || op >= MGFVM_NOPS) return mgfvm_fail(MGFVM_EINVAL, "unknown op %d", op);
     if (level < 0 || level >= x->maxng) return mgfvm_fail(MGFVM_EINVAL, "level %d out of range", level);
     if ((op == MGFVM_OP_RESTRICT || op == MGFVM_OP_PROLONG) && level + 1 >= x->maxng)
@@ -1077,6 +1173,7 @@ int mgfvm_stream(mgfvm_ctx *x, void **stream)
 int mgfvm_time_op(mgfvm_ctx *x, int op, int level, int reps, double *ms_total, int *launches)
 {
     RC(check_ctx(x));
+    if (x->opt.tangent) return mgfvm_fail(MGFVM_EINVAL, "%s: not available in a tangent context (it would change the state without its derivatives)", __func__);
     if (op < 0 || op >= MGFVM_NOPS || reps < 1) return mgfvm_fail(MGFVM_EINVAL, "bad op %d or reps %d", op, reps);
     if (level < 0 || level >= x->maxng) return mgfvm_fail(MGFVM_EINVAL, "level %d out of range", level);
     if ((op == MGFVM_OP_RESTRICT || op == MGFVM_OP_PROLONG) && level + 1 >= x->maxng)
@@ -1091,7 +1188,7 @@ int mgfvm_time_op(mgfvm_ctx *x, int op, int level, int reps, double *ms_total, i
     cudaGraphExec_t ge = nullptr;
     CK(cudaStreamBeginCapture(x->stream, cudaStreamCaptureModeThreadLocal));
     for (const Launch &L : v) {
-        cudaError_t e = launch_one(L, x->dc, x->ds, x->sched, x->stream);
+        cudaError_t e = launch_one(L, x->dc, x->ds, x->dt, x->sched, x->stream);
         if (e != cudaSuccess) {
             cudaStreamEndCapture(x->stream, &g);
             if (g) cudaGraphDestroy(g);
@@ -1184,6 +1281,7 @@ int mgfvm_set_tuning(mgfvm_ctx *x, const mgfvm_tuning *t)
 int mgfvm_autotune(mgfvm_ctx *x, int cycles, mgfvm_tuning *chosen, double *ms_before, double *ms_after)
 {
     RC(check_ctx(x));
+    if (x->opt.tangent) return mgfvm_fail(MGFVM_EINVAL, "%s: not available in a tangent context (it would change the state without its derivatives)", __func__);
     if (cycles < 1) return mgfvm_fail(MGFVM_EINVAL, "cycles must be >= 1");
     RC(pull(x));
     const std::vector<CaseState> saved = x->hs;
@@ -1268,7 +1366,7 @@ int mgfvm_profile_cycle(mgfvm_ctx *x, double *ms, int *kernel, int *level, int c
     for (auto &e : ev) CK(cudaEventCreate(&e));
     CK(cudaEventRecord(ev[0], x->stream));
     for (int k = 0; k < n; ++k) {
-        cudaError_t e = launch_one(x->cyc[k], x->dc, x->ds, x->sched, x->stream);
+        cudaError_t e = launch_one(x->cyc[k], x->dc, x->ds, x->dt, x->sched, x->stream);
         if (e != cudaSuccess) return mgfvm_fail(MGFVM_ECUDA, "profile launch %d: %s", k, cudaGetErrorString(e));
         CK(cudaEventRecord(ev[k + 1], x->stream));
     }
@@ -1352,6 +1450,109 @@ int mgfvm_check_division(int device, long long n, unsigned long long seed, long 
     if (e != cudaSuccess) return mgfvm_fail(MGFVM_ECUDA, "division self-test: %s", cudaGetErrorString(e));
     *mismatches = (long long)h;
     return MGFVM_OK;
+}
+
+// ------------------------------------------------------------ derivatives
+int mgfvm_set_direction(mgfvm_ctx *x, int icase, int kind, int index)
+{
+    RC(check_ctx(x));
+    if (!x->opt.tangent) return mgfvm_fail(MGFVM_EINVAL, "not a tangent context (mgfvm_options.tangent)");
+    if (icase < 0 || icase >= x->ncases) return mgfvm_fail(MGFVM_EINVAL, "case %d out of range", icase);
+    if (kind < MGFVM_DIR_NONE || kind > MGFVM_DIR_PRSC) return mgfvm_fail(MGFVM_EINVAL, "unknown direction %d", kind);
+    if (kind == MGFVM_DIR_INLET && (index < 0 || index >= x->cfg[icase].nfy))
+        return mgfvm_fail(MGFVM_EINVAL, "inlet face %d outside [0, %d)", index, x->cfg[icase].nfy);
+    RC(pull(x));
+    x->dir_kind[icase] = kind;
+    x->dir_index[icase] = kind == MGFVM_DIR_INLET ? index : 0;
+    return init_state(x, icase);
+}
+
+int mgfvm_get_tangent(mgfvm_ctx *x, int icase, int level, int field, double *out)
+{
+    RC(check_ctx(x));
+    if (!x->opt.tangent) return mgfvm_fail(MGFVM_EINVAL, "not a tangent context (mgfvm_options.tangent)");
+    RC(check_case_level(x, icase, level));
+    if (field < 0 || field >= MGFVM_NFIELDS || !out) return mgfvm_fail(MGFVM_EINVAL, "bad field %d", field);
+    CK(cudaStreamSynchronize(x->stream));
+    const LevelDev &L = x->hc[icase].lv[level];
+    const double *t = x->ht[icase].lv[level].t[field_slot(field, x->last_eq[level])];
+    const size_t n = (size_t)L.npx * L.npy;
+    if (!t) {
+        std::fill(out, out + n, 0.0);   // geometry and obstacle sources do not depend on the parameters
+        return MGFVM_OK;
+    }
+    CK(cudaMemcpy(out, t, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    x->d2h += (long long)(sizeof(double) * n);
+    return MGFVM_OK;
+}
+
+// J of the level-0 state (and its derivative from the tangent fields): row means over
+// the interior rows j = 1 .. npy-2, summed in row order.
+static void objective_of(const double *p, const double *sc, int npx, int npy, double *J)
+{
+    double sin = 0.0, sout = 0.0, ssc = 0.0;
+    for (int j = 1; j <= npy - 2; ++j) {
+        sin += p[(size_t)j * npx + 1];
+        sout += p[(size_t)j * npx + npx - 2];
+        ssc += sc[(size_t)j * npx + npx - 1];
+    }
+    const double ny = (double)(npy - 2);
+    *J = (sin / ny - sout / ny) + ssc / ny;
+}
+
+int mgfvm_objective(mgfvm_ctx *x, int icase, double *J, double *dJ)
+{
+    RC(check_ctx(x));
+    RC(check_case_level(x, icase, 0));
+    if (dJ && !x->opt.tangent) return mgfvm_fail(MGFVM_EINVAL, "dJ needs a tangent context (mgfvm_options.tangent)");
+    const LevelDev &L = x->hc[icase].lv[0];
+    const size_t n = (size_t)L.npx * L.npy;
+    std::vector<double> p(n), sc(n);
+    if (J) {
+        RC(mgfvm_get_field(x, icase, 0, MGFVM_F_P, p.data()));
+        RC(mgfvm_get_field(x, icase, 0, MGFVM_F_SC, sc.data()));
+        objective_of(p.data(), sc.data(), L.npx, L.npy, J);
+    }
+    if (dJ) {
+        RC(mgfvm_get_tangent(x, icase, 0, MGFVM_F_P, p.data()));
+        RC(mgfvm_get_tangent(x, icase, 0, MGFVM_F_SC, sc.data()));
+        objective_of(p.data(), sc.data(), L.npx, L.npy, dJ);
+    }
+    return MGFVM_OK;
+}
+
+int mgfvm_gradient(const mgfvm_config *cfg, const double *inlet_u, int n_inlet, int ncycles, int device,
+                   double *J, double *dJ_dinlet, double *dJ_damuf, double *dJ_dprsc)
+{
+    mgfvm_clear_error();
+    if (!cfg || ncycles < 0 || n_inlet < 0 || (n_inlet > 0 && !inlet_u))
+        return mgfvm_fail(MGFVM_EINVAL, "bad gradient arguments");
+    const int nf = cfg->nfy, ncase = nf + 2;
+    std::vector<mgfvm_config> cases(ncase, *cfg);
+    mgfvm_options opt;
+    mgfvm_options_default(&opt);
+    opt.device = device;
+    opt.tangent = 1;
+    mgfvm_ctx *x = nullptr;
+    RC(mgfvm_create(cases.data(), ncase, &opt, &x));
+    int rc = MGFVM_OK;
+    do {
+        for (int c = 0; c < ncase; ++c) {
+            x->profile[c].assign(inlet_u, inlet_u + n_inlet);
+            x->dir_kind[c] = c < nf ? MGFVM_DIR_INLET : c == nf ? MGFVM_DIR_AMUF : MGFVM_DIR_PRSC;
+            x->dir_index[c] = c < nf ? c : 0;
+        }
+        if ((rc = upload_profiles(x)) != MGFVM_OK) break;
+        if ((rc = init_state(x, -1)) != MGFVM_OK) break;
+        if ((rc = mgfvm_cycle(x, ncycles)) != MGFVM_OK) break;
+        if (J && (rc = mgfvm_objective(x, 0, J, nullptr)) != MGFVM_OK) break;
+        for (int c = 0; c < ncase && rc == MGFVM_OK; ++c) {
+            double *dst = c < nf ? (dJ_dinlet ? dJ_dinlet + c : nullptr) : c == nf ? dJ_damuf : dJ_dprsc;
+            if (dst) rc = mgfvm_objective(x, c, nullptr, dst);
+        }
+    } while (0);
+    mgfvm_destroy(x);
+    return rc;
 }
 
 }  // extern "C"

@@ -17,6 +17,9 @@
 // All reductions are two-level and fixed-order, so results are reproducible.
 #include "mg_cells.cuh"
 #include "mg_kernels.cuh"
+#include "mg_tangent.cuh"
+
+#include <type_traits>
 
 namespace mg {
 
@@ -239,20 +242,26 @@ __global__ void __launch_bounds__(BLOCK) k_pfix(const CaseDev *__restrict__ cs, 
 
 // pbound :1179-1210 then outflow :1211-1228 (bits: 1 periodic, 2 outflow of u, v, p,
 // 4 the scalar ghost too) — one block per case.
-__device__ __forceinline__ void bound_block(const CaseDev &C, const LevelDev &L, int bits)
+template <class IO>
+__device__ __forceinline__ void bound_block_io(const CaseDev &C, const IO &io, int bits)
 {
+    const LevelDev &L = io.L;
     if ((bits & 1) && C.ibc_xm == 3) {
-        for (int j = 1 + threadIdx.x; j < L.npy - 1; j += blockDim.x) row_periodic_x(L, j);
+        for (int j = 1 + threadIdx.x; j < L.npy - 1; j += blockDim.x) row_periodic_x_io(io, j);
         __syncthreads();
     }
     if ((bits & 1) && C.ibc_ym == 3) {
-        if (threadIdx.x == 0) line_periodic_y(L);
+        if (threadIdx.x == 0) line_periodic_y_io(io);
         __syncthreads();
     }
     if ((bits & 2) && C.ibc_xp == 4) {
-        for (int j = threadIdx.x; j < L.npy; j += blockDim.x) row_outflow(L, j, (bits & 4) != 0);
+        for (int j = threadIdx.x; j < L.npy; j += blockDim.x) row_outflow_io(io, j, (bits & 4) != 0);
         __syncthreads();
     }
+}
+__device__ __forceinline__ void bound_block(const CaseDev &C, const LevelDev &L, int bits)
+{
+    bound_block_io(C, Prim{L}, bits);
 }
 
 __global__ void __launch_bounds__(BLOCK) k_bound(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode, int bits)
@@ -509,7 +518,6 @@ __device__ __forceinline__ void pp_level_body(const CaseDev &C, CaseState &ST, c
     }
     const int W = P.W, kA = P.kA, kB = P.kB, limA = P.limA, limB = P.limB;
     double *phi = sm, *phi2 = sm + W * P.Hh;
-    const double *u = MGF(L, S_U), *v = MGF(L, S_V);
     double *pp = MGF(L, S_PP);
     double A[6] = {0, 0, 0, 0, 0, 0}, B[6] = {0, 0, 0, 0, 0, 0}, pA = 0.0, pB = 0.0, divs = 0.0;
     {
@@ -517,7 +525,7 @@ __device__ __forceinline__ void pp_level_body(const CaseDev &C, CaseState &ST, c
         double su;
         if (P.okA) {
             if (limA >= 0) {
-                divs += mass_coefp_values(L, C, P.i, P.jA, k, su, u, v);
+                divs += mass_coefp_values(L, C, P.i, P.jA, k, su, S_U, S_V);
                 A[0] = k.aw; A[1] = k.ae; A[2] = k.as; A[3] = k.an; A[4] = k.ap; A[5] = su;
             } else {
                 pA = pp[P.gA];      // boundary ring: masserror leaves it
@@ -525,7 +533,7 @@ __device__ __forceinline__ void pp_level_body(const CaseDev &C, CaseState &ST, c
         }
         if (P.okB) {
             if (limB >= 0) {
-                divs += mass_coefp_values(L, C, P.i, P.jB, k, su, u, v);
+                divs += mass_coefp_values(L, C, P.i, P.jB, k, su, S_U, S_V);
                 B[0] = k.aw; B[1] = k.ae; B[2] = k.as; B[3] = k.an; B[4] = k.ap; B[5] = su;
             } else {
                 pB = pp[P.gB];
@@ -741,27 +749,39 @@ __global__ void __launch_bounds__(BLOCK) k_copy(const CaseDev *__restrict__ cs, 
 
 // restv :1354-1389 on coarse level ig+1, fluxes(fine) :216 and the fine residuals of
 // restr{u,v,sc}, one thread per (fine cell, slice `which` of 3)
+template <class IO>
+__device__ __forceinline__ void cell_restv_fluxes_io(const IO &F, const IO &K, const CaseDev &C, int i, int j,
+                                                     int which, int nwhich)
+{
+    if (which == 0) {
+        if (i <= F.L.npx - 2 && j <= F.L.npy - 2) cell_fluxes_io(F, j * F.L.npx + i);
+        if (((i | j) & 1) == 0) {
+            const int ic = i >> 1, jc = j >> 1;
+            if (ic >= 1 && jc >= 1 && ic <= K.L.npx - 2 && jc <= K.L.npy - 2) cell_restv_io(F, K, ic, jc);
+        }
+    }
+    for (int w = which; w < 3; w += nwhich) cell_fine_residuals_io(F, C, i, j, w);
+}
 __device__ __forceinline__ void cell_restv_fluxes(const LevelDev &F, const LevelDev &K, const CaseDev &C, int i,
                                                   int j, int which, int nwhich)
 {
-    if (which == 0) {
-        if (i <= F.npx - 2 && j <= F.npy - 2) cell_fluxes(F, j * F.npx + i);
-        if (((i | j) & 1) == 0) {
-            const int ic = i >> 1, jc = j >> 1;
-            if (ic >= 1 && jc >= 1 && ic <= K.npx - 2 && jc <= K.npy - 2) cell_restv(F, K, ic, jc);
-        }
-    }
-    for (int w = which; w < 3; w += nwhich) cell_fine_residuals(F, C, i, j, w);
+    cell_restv_fluxes_io(Prim{F}, Prim{K}, C, i, j, which, nwhich);
 }
 
 // restru/restrv/restrsc :1474-1740 and fluxes(coarse) :215, one thread per
 // (coarse cell, slice `which` of 3)
+template <class IO>
+__device__ __forceinline__ void cell_restrict_fluxes_io(const IO &F, const IO &K, const CaseDev &C, int ic, int jc,
+                                                        int which, int nwhich)
+{
+    if (which == 0 && ic <= K.L.npx - 2 && jc <= K.L.npy - 2) cell_fluxes_io(K, jc * K.L.npx + ic);
+    if (ic >= 1 && jc >= 1 && ic <= K.L.npx - 2 && jc <= K.L.npy - 2)
+        for (int w = which; w < 3; w += nwhich) cell_restrict_io(F, K, C, ic, jc, w);
+}
 __device__ __forceinline__ void cell_restrict_fluxes(const LevelDev &F, const LevelDev &K, const CaseDev &C,
                                                      int ic, int jc, int which, int nwhich)
 {
-    if (which == 0 && ic <= K.npx - 2 && jc <= K.npy - 2) cell_fluxes(K, jc * K.npx + ic);
-    if (ic >= 1 && jc >= 1 && ic <= K.npx - 2 && jc <= K.npy - 2)
-        for (int w = which; w < 3; w += nwhich) cell_restrict(F, K, C, ic, jc, w);
+    cell_restrict_fluxes_io(Prim{F}, Prim{K}, C, ic, jc, which, nwhich);
 }
 
 __global__ void __launch_bounds__(BLOCK) k_restv_fluxes(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode)
@@ -946,34 +966,35 @@ __device__ __forceinline__ void for_cells(const Dom &d, F f)
 
 // Smooth the equations of `mask` on one level, in place in global memory, every
 // equation's unit h in the same phase.
-__device__ void tail_smooth_global(const LevelDev &L, const int *eqs, int ne, int nsw, int isolve)
+template <class IO>
+__device__ void tail_smooth_global(const IO &io, const int *eqs, int ne, int nsw, int isolve)
 {
+    const LevelDev &L = io.L;
     if (isolve == MGFVM_JACOBI) {
         for (int k = 0; k < ne; ++k) {
             const int e = eqs[k];
             const Dom d = dom_eq(L, e);
             const Dom x = {d.i0 - 1, d.j0 - 1, d.wi + 2, d.wj + 2};
-            double *phi = MGF(L, eq_field(e)), *tmp = MGF(L, eq_tmp(e));
+            const int phi = eq_field(e), tmp = eq_tmp(e);
             for_cells(x, [&](int i, int j) {
                 if (i == x.i0 || i == x.i0 + x.wi - 1 || j == x.j0 || j == x.j0 + x.wj - 1)
-                    tmp[j * L.npx + i] = phi[j * L.npx + i];
+                    io.st(tmp, j * L.npx + i, io.ld(phi, j * L.npx + i));
             });
         }
         for (int it = 0; it < nsw; ++it) {
             for (int k = 0; k < ne; ++k) {
                 const int e = eqs[k];
-                double *phi = MGF(L, eq_field(e)), *tmp = MGF(L, eq_tmp(e));
-                const double *cur = (it & 1) ? tmp : phi;
-                double *nxt = (it & 1) ? phi : tmp;
-                for_cells(dom_eq(L, e), [&](int i, int j) { cell_jacobi(L, e, cur, nxt, j * L.npx + i); });
+                const int phi = eq_field(e), tmp = eq_tmp(e);
+                const int cur = (it & 1) ? tmp : phi, nxt = (it & 1) ? phi : tmp;
+                for_cells(dom_eq(L, e), [&](int i, int j) { cell_jacobi_io(io, e, cur, nxt, j * L.npx + i); });
             }
             __syncthreads();
         }
         if (nsw & 1) {
             for (int k = 0; k < ne; ++k) {
                 const int e = eqs[k];
-                double *phi = MGF(L, eq_field(e)), *tmp = MGF(L, eq_tmp(e));
-                for_cells(dom_eq(L, e), [&](int i, int j) { phi[j * L.npx + i] = tmp[j * L.npx + i]; });
+                const int phi = eq_field(e), tmp = eq_tmp(e);
+                for_cells(dom_eq(L, e), [&](int i, int j) { io.st(phi, j * L.npx + i, io.ld(tmp, j * L.npx + i)); });
             }
             __syncthreads();
         }
@@ -983,12 +1004,12 @@ __device__ void tail_smooth_global(const LevelDev &L, const int *eqs, int ne, in
             for (int k = 0; k < ne; ++k) {
                 const int e = eqs[k];
                 const Dom d = dom_eq(L, e);
-                double *phi = MGF(L, eq_field(e));
+                const int phi = eq_field(e);
                 const int wr = (d.wi + 1) >> 1, n = wr * d.wj;
                 for (int t = threadIdx.x; t < n; t += blockDim.x) {
                     const int j = d.j0 + t / wr;
                     const int i = d.i0 + (((d.i0 + j) & 1) != colour ? 1 : 0) + 2 * (t % wr);
-                    if (i <= d.i0 + d.wi - 1) cell_gs(L, e, phi, j * L.npx + i);
+                    if (i <= d.i0 + d.wi - 1) cell_gs_io(io, e, phi, j * L.npx + i);
                 }
             }
             __syncthreads();
@@ -1012,7 +1033,7 @@ __device__ void tail_smooth(const LevelDev &L, int mask, int nsw, int isolve, do
         int g = 0;
         while (k + g < ne && (long long)(g + 1) * per * n <= sm_doubles) ++g;
         if (g == 0) {
-            tail_smooth_global(L, eqs + k, 1, nsw, isolve);
+            tail_smooth_global(Prim{L}, eqs + k, 1, nsw, isolve);
             ++k;
             continue;
         }
@@ -1074,55 +1095,93 @@ __device__ void tail_smooth(const LevelDev &L, int mask, int nsw, int isolve, do
     }
 }
 
-// One SIMPLE step on level ig (down leg :201-207, up leg :235-244).
-__device__ void tail_step(const CaseDev &C, CaseState &ST, int ig, bool down, const Sched &S, double *sm, int smd)
+// The levels of one case as seen by the one-CTA kernel (TanCase: mg_tangent.cuh).
+struct PrimCase {
+    const CaseDev &C;
+    __device__ __forceinline__ Prim io(int ig) const { return Prim{C.lv[ig]}; }
+};
+
+// update's obstacle pressure copy (:1153-1177) by one CTA
+template <class IO>
+__device__ __forceinline__ void pfix_block_io(const IO &io)
 {
-    const LevelDev &L = C.lv[ig];
-    const FluxLive fl(L);
-    const unsigned what = A_FLUX | A_U | A_V | A_SC | (down ? A_SC_OUTFLOW : 0u);
-    for_cells(dom_all(L), [&](int i, int j) { cell_asm(L, C, fl, i, j, what); });
+    const LevelDev &L = io.L;
+    if (L.ncopy <= 0) return;
+    if (L.hazard) {
+        for (int t = threadIdx.x; t < L.ncopy; t += blockDim.x) io.set_pb(t, io.ld(S_P, L.psrc[t]));
+        __syncthreads();
+        for (int t = threadIdx.x; t < L.ncopy; t += blockDim.x) io.st(S_P, L.pdst[t], io.pb(t));
+    } else {
+        for (int t = threadIdx.x; t < L.ncopy; t += blockDim.x) io.st(S_P, L.pdst[t], io.ld(S_P, L.psrc[t]));
+    }
     __syncthreads();
-    tail_smooth(L, (1 << EQ_U) | (1 << EQ_V) | (1 << EQ_SC), S.nswpm, S.isolve, sm, smd);
+}
+
+// One SIMPLE step on level ig (down leg :201-207, up leg :235-244).  The plain run
+// stages each level's smoothing in shared memory where it fits (tail_smooth); the
+// tangent run smooths in global memory.
+template <class X>
+__device__ void tail_step(const X &cx, CaseState &ST, int ig, bool down, const Sched &S, double *sm, int smd)
+{
+    const CaseDev &C = cx.C;
+    const auto io = cx.io(ig);
+    using IO = decltype(io);
+    constexpr bool plain = std::is_same<typename std::remove_cv<IO>::type, Prim>::value;
+    const LevelDev &L = io.L;
+    const FluxLiveT<typename std::remove_cv<IO>::type> fl{io};
+    const unsigned what = A_FLUX | A_U | A_V | A_SC | (down ? A_SC_OUTFLOW : 0u);
+    for_cells(dom_all(L), [&](int i, int j) { cell_asm_io(io, C, fl, i, j, what); });
+    __syncthreads();
+    const int uvsc[3] = {EQ_U, EQ_V, EQ_SC}, pp[1] = {EQ_PP};
+    if constexpr (plain) tail_smooth(L, (1 << EQ_U) | (1 << EQ_V) | (1 << EQ_SC), S.nswpm, S.isolve, sm, smd);
+    else tail_smooth_global(io, uvsc, 3, S.nswpm, S.isolve);
     double acc[1] = {0.0};
-    for_cells(dom_interior(L), [&](int i, int j) { acc[0] += cell_mass_coefp(L, C, i, j); });
+    for_cells(dom_interior(L), [&](int i, int j) { acc[0] += val(cell_mass_coefp_io(io, C, i, j)); });
     if (ig == 0 && down) {
         block_sum<1>(acc);
         if (threadIdx.x == 0) ST.last_err = acc[0];
     }
     __syncthreads();
-    tail_smooth(L, 1 << EQ_PP, S.nswpp, S.isolve, sm, smd);
-    for_cells(dom_interior(L), [&](int i, int j) { cell_update(L, C, j * L.npx + i); });
+    if constexpr (plain) tail_smooth(L, 1 << EQ_PP, S.nswpp, S.isolve, sm, smd);
+    else tail_smooth_global(io, pp, 1, S.nswpp, S.isolve);
+    for_cells(dom_interior(L), [&](int i, int j) { cell_update_io(io, C, j * L.npx + i); });
     __syncthreads();
-    if (L.ncopy > 0) {
-        double *p = MGF(L, S_P);
-        if (L.hazard) {
-            for (int t = threadIdx.x; t < L.ncopy; t += blockDim.x) L.pbuf[t] = p[L.psrc[t]];
-            __syncthreads();
-            for (int t = threadIdx.x; t < L.ncopy; t += blockDim.x) p[L.pdst[t]] = L.pbuf[t];
-        } else {
-            for (int t = threadIdx.x; t < L.ncopy; t += blockDim.x) p[L.pdst[t]] = p[L.psrc[t]];
-        }
-        __syncthreads();
+    pfix_block_io(io);
+    bound_block_io(C, io, down ? 3 : 7);
+}
+
+template <class X>
+__device__ void tail_restrict(const X &cx, int ig)
+{
+    const auto F = cx.io(ig), K = cx.io(ig + 1);
+    for_cells(dom_all(F.L), [&](int i, int j) { cell_restv_fluxes_io(F, K, cx.C, i, j, 0, 1); });
+    __syncthreads();
+    for_cells(dom_all(K.L), [&](int i, int j) { cell_restrict_fluxes_io(F, K, cx.C, i, j, 0, 1); });
+    __syncthreads();
+}
+
+template <class X>
+__device__ void tail_prolong(const X &cx, int ig)
+{
+    const auto F = cx.io(ig), K = cx.io(ig + 1);
+    for_cells(dom_interior(K.L), [&](int i, int j) { cell_prol_corr_io(F, K, i, j); });
+    __syncthreads();
+    for_cells(dom_interior(F.L), [&](int i, int j) { cell_prol_apply_io(F, K, i, j); });
+    __syncthreads();
+}
+
+template <class X>
+__device__ void tail_cycle(const X &cx, CaseState &ST, const Sched &S, double *sm, int smd)
+{
+    const CaseDev &C = cx.C;
+    for (int ig = C.tail; ig < C.ngrid; ++ig) {
+        tail_step(cx, ST, ig, true, S, sm, smd);
+        if (ig != C.ngrid - 1) tail_restrict(cx, ig);
     }
-    bound_block(C, L, down ? 3 : 7);
-}
-
-__device__ void tail_restrict(const CaseDev &C, int ig)
-{
-    const LevelDev &F = C.lv[ig], &K = C.lv[ig + 1];
-    for_cells(dom_all(F), [&](int i, int j) { cell_restv_fluxes(F, K, C, i, j, 0, 1); });
-    __syncthreads();
-    for_cells(dom_all(K), [&](int i, int j) { cell_restrict_fluxes(F, K, C, i, j, 0, 1); });
-    __syncthreads();
-}
-
-__device__ void tail_prolong(const CaseDev &C, int ig)
-{
-    const LevelDev &F = C.lv[ig], &K = C.lv[ig + 1];
-    for_cells(dom_interior(K), [&](int i, int j) { cell_prol_corr(F, K, i, j); });
-    __syncthreads();
-    for_cells(dom_interior(F), [&](int i, int j) { cell_prol_apply(F, K, i, j); });
-    __syncthreads();
+    for (int ig = C.ngrid - 1; ig > C.tail; --ig) {
+        tail_prolong(cx, ig - 1);
+        if (ig != 1) tail_step(cx, ST, ig - 1, false, S, sm, smd);
+    }
 }
 
 // Every level at or below C.tail of one case (blockIdx.x): the down leg from
@@ -1134,14 +1193,19 @@ __global__ void __launch_bounds__(TAIL_BLOCK, 1) k_tail(const CaseDev *__restric
     const CaseDev &C = cs[blockIdx.x];
     CaseState &ST = st[blockIdx.x];
     if (ST.done || C.tail >= C.ngrid) return;
-    for (int ig = C.tail; ig < C.ngrid; ++ig) {
-        tail_step(C, ST, ig, true, S, tsm, smem_doubles);
-        if (ig != C.ngrid - 1) tail_restrict(C, ig);
-    }
-    for (int ig = C.ngrid - 1; ig > C.tail; --ig) {
-        tail_prolong(C, ig - 1);
-        if (ig != 1) tail_step(C, ST, ig - 1, false, S, tsm, smem_doubles);
-    }
+    tail_cycle(PrimCase{C}, ST, S, tsm, smem_doubles);
+}
+
+// The same levels with every value paired with its derivative along the case's
+// parameter direction (forward mode, mg_tangent.cuh): the value bits are those of
+// k_tail, the derivatives those of the same V-cycle.
+__global__ void __launch_bounds__(TAIL_BLOCK, 1) k_tail_tan(const CaseDev *__restrict__ cs, CaseState *st,
+                                                            const CaseTan *__restrict__ ts, Sched S)
+{
+    const CaseDev &C = cs[blockIdx.x];
+    CaseState &ST = st[blockIdx.x];
+    if (ST.done || C.tail >= C.ngrid) return;
+    tail_cycle(TanCase{C, ts[blockIdx.x]}, ST, S, nullptr, 0);
 }
 
 // ------------------------------------------------------------- launcher
@@ -1168,7 +1232,8 @@ static void launch_smooth(const Launch &X, dim3 g, int b, const CaseDev *dc, Cas
         k_smooth<ISOLVE, SMOOTH_BLOCK><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
 }
 
-cudaError_t launch_one(const Launch &X, const CaseDev *dc, CaseState *ds, const Sched &S, cudaStream_t st)
+cudaError_t launch_one(const Launch &X, const CaseDev *dc, CaseState *ds, const CaseTan *dt, const Sched &S,
+                       cudaStream_t st)
 {
     const dim3 g = X.grid;
     const int b = X.block;
@@ -1229,6 +1294,10 @@ cudaError_t launch_one(const Launch &X, const CaseDev *dc, CaseState *ds, const 
     case K_PROL_CORR: k_prol_corr<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode); break;
     case K_PROL_APPLY: k_prol_apply<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode); break;
     case K_TAIL: k_tail<<<g, b, X.smem, st>>>(dc, ds, S, X.smem / (int)sizeof(double)); break;
+    case K_TAIL_TAN:
+        if (!dt) return cudaErrorInvalidValue;
+        k_tail_tan<<<g, b, 0, st>>>(dc, ds, dt, S);
+        break;
     case K_ENDCYCLE: k_endcycle<<<g, b, 0, st>>>(dc, ds); break;
     case K_PROL_APPLY_END: k_prol_apply_end<<<g, b, 0, st>>>(dc, ds, X.mode); break;
     default: return cudaErrorInvalidValue;

@@ -23,6 +23,7 @@ enum KernelId {
     K_PFIX_BOUND,    // K_PFIX then K_BOUND (a0 = bits), one CTA per case
     K_PP_LEVEL,      // masserror+coefp, p' smoothing, update on a one-CTA level: a0 = units,
                      // a1 = reduce, a2 = update fuse bits
+    K_TAIL_TAN,      // K_TAIL with derivatives (a tangent context)
     K_LEVEL_VISIT,   // a whole one-CTA level visit, a cluster of 3 CTAs per case: K_PP_LEVEL's
                      // a0-a2, a3 = assembly bits (0: done), a4 = u/v/sc units
     K_NKERNELS
@@ -50,8 +51,10 @@ constexpr int MAX_UNITS = 10;   // default cap of half-sweeps (GS) or sweeps (Ja
 constexpr int MIN_TILE = 8;     // smallest tile side a units cap may leave
 int smooth_pairs_side(int units, int threads);   // tile side whose region fits `threads` pairs
 
-cudaError_t launch_one(const Launch &L, const CaseDev *dcases, CaseState *dstate, const Sched &S,
-                       cudaStream_t stream);
+struct CaseTan;
+// `dtan`: the derivative storage of a tangent context (K_TAIL_TAN), else unused
+cudaError_t launch_one(const Launch &L, const CaseDev *dcases, CaseState *dstate, const CaseTan *dtan,
+                       const Sched &S, cudaStream_t stream);
 cudaError_t configure_kernels();
 
 // Kernels of the raw-pointer entry points.

@@ -11,7 +11,7 @@ The compute path is libmgfvm.so (CUDA, sm_100a) behind the C ABI of include/mgfv
 from ._abi import FIELDS, OPS  # noqa: F401
 from ._lib import MgfvmError, lib  # noqa: F401
 from .inputs import CaseConfig, obstacle_ranges  # noqa: F401
-from .solver import Solver, read_case, validate  # noqa: F401
+from .solver import Solver, gradient, read_case, validate  # noqa: F401
 
-__all__ = ["CaseConfig", "Solver", "read_case", "validate", "MgfvmError", "FIELDS", "OPS",
+__all__ = ["CaseConfig", "Solver", "gradient", "read_case", "validate", "MgfvmError", "FIELDS", "OPS",
            "obstacle_ranges", "lib"]

@@ -27,6 +27,7 @@ OP = {name: k for k, name in enumerate(OPS)}
 
 JACOBI, GAUSS_SEIDEL = 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
+DIR = {"none": 0, "inlet": 1, "amuf": 2, "prsc": 3}
 
 
 class Config(C.Structure):
@@ -63,7 +64,7 @@ class Config(C.Structure):
 class Options(C.Structure):
     """struct mgfvm_options."""
     _fields_ = [("device", C.c_int), ("precision", C.c_int), ("tail_level", C.c_int),
-                ("use_graph", C.c_int), ("sync_every", C.c_int)]
+                ("use_graph", C.c_int), ("sync_every", C.c_int), ("tangent", C.c_int)]
 
 
 MAX_LEVELS = 16

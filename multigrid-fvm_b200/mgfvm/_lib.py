@@ -83,6 +83,10 @@ def lib() -> C.CDLL:
         "mgfvm_masserror_f64_noalloc": (C.c_int, [_vp] * 6 + [C.c_int, C.c_int, _vp, _vp]),
         "mgfvm_check_division": (C.c_int, [C.c_int, C.c_longlong, C.c_ulonglong, _vp]),
         "mgfvm_field_device_ptr": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p), _ip, _ip]),
+        "mgfvm_set_direction": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int]),
+        "mgfvm_get_tangent": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _dp]),
+        "mgfvm_objective": (C.c_int, [_vp, C.c_int, _dp, _dp]),
+        "mgfvm_gradient": (C.c_int, [C.POINTER(_abi.Config), _dp, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _dp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

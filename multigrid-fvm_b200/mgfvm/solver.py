@@ -45,7 +45,7 @@ class Solver:
 
     def __init__(self, cases: Union[CaseConfig, Sequence[CaseConfig]], device: int = 0,
                  precision: str = "fp64", tail_level: int = -1, use_graph: bool = True,
-                 sync_every: int = 64):
+                 sync_every: int = 64, tangent: bool = False):
         if isinstance(cases, CaseConfig):
             cases = [cases]
         self.cases: List[CaseConfig] = list(cases)
@@ -63,11 +63,13 @@ class Solver:
         opt.tail_level = tail_level
         opt.use_graph = int(use_graph)
         opt.sync_every = sync_every
+        opt.tangent = int(tangent)
         h = C.c_void_p()
         check(L.mgfvm_create(arr, len(self.cases), C.byref(opt), C.byref(h)))
         self._h = h
         self._lib = L
         self.device = device
+        self._opt_tangent = bool(tangent)
 
     # ------------------------------------------------------------ lifetime
     def close(self) -> None:
@@ -181,7 +183,7 @@ class Solver:
 
     KERNELS = ["fluxes", "asm", "mass_coefp", "update", "pfix", "bound", "smooth", "copy", "restv_fluxes",
                "restrict", "prol_corr", "prol_apply", "tail", "endcycle", "prol_apply_end", "smooth_mixed", "pfix_bound", "pp_level",
-               "level_visit"]
+               "tail_tan", "level_visit"]
 
     def profile_cycle(self):
         """One directly-launched V-cycle with an event after every kernel: a list of
@@ -238,6 +240,29 @@ class Solver:
         check(self._lib.mgfvm_autotune(self._h, cycles, C.byref(t), C.byref(a), C.byref(b)))
         return a.value, b.value, t.as_dict()
 
+    # ------------------------------------------------------------ derivatives
+    def set_direction(self, case: int, kind: str, index: int = 0) -> None:
+        """Tangent contexts: differentiate case `case` along `kind` ("inlet" face
+        `index`, "amuf", "prsc"); the case restarts from its initial state."""
+        check(self._lib.mgfvm_set_direction(self._h, case, _abi.DIR[kind], index))
+
+    def tangent(self, case: int, level: int, name: Union[str, int]) -> np.ndarray:
+        """Derivative of a field along the case's direction (npy, npx)."""
+        npx, npy = self.dims(case, level)
+        f = _abi.FIELD[name] if isinstance(name, str) else name
+        out = np.empty(npx * npy, dtype=np.float64)
+        check(self._lib.mgfvm_get_tangent(self._h, case, level, f, out.ctypes.data_as(_dp)))
+        return out.reshape(npy, npx)
+
+    def objective(self, case: int = 0) -> Tuple[float, Optional[float]]:
+        """(J, dJ): the pressure drop plus mean outlet scalar of the level-0 state
+        (mgfvm_objective) and, in a tangent context, its derivative."""
+        j = C.c_double()
+        d = C.c_double()
+        tan = bool(self._opt_tangent)
+        check(self._lib.mgfvm_objective(self._h, case, C.byref(j), C.byref(d) if tan else None))
+        return j.value, (d.value if tan else None)
+
     @property
     def transfer_bytes(self) -> Tuple[int, int]:
         """(host->device, device->host) bytes copied by this context so far."""
@@ -250,3 +275,20 @@ class Solver:
         s = C.c_void_p()
         check(self._lib.mgfvm_stream(self._h, C.byref(s)))
         return s.value or 0
+
+
+def gradient(cfg: CaseConfig, inlet_u=None, cycles: int = 100, device: int = 0):
+    """J after `cycles` V-cycles from cfg's initial state (with the per-face inlet
+    profile `inlet_u`, or none) and its exact derivatives with respect to every inlet
+    face (nfy values), amuf and prsc: one batched tangent run (mgfvm_gradient).
+    Returns (J, dJ_dinlet, dJ_damuf, dJ_dprsc)."""
+    c, keep = cfg.to_c()
+    prof = np.ascontiguousarray(np.zeros(0) if inlet_u is None else np.asarray(inlet_u, dtype=np.float64))
+    nf = int(cfg.nfy)
+    g_in = np.zeros(nf)
+    j, ga, gp = C.c_double(), C.c_double(), C.c_double()
+    check(lib().mgfvm_gradient(C.byref(c), prof.ctypes.data_as(_dp) if prof.size else None, int(prof.size),
+                               int(cycles), int(device), C.byref(j), g_in.ctypes.data_as(_dp), C.byref(ga),
+                               C.byref(gp)))
+    del keep
+    return j.value, g_in, ga.value, gp.value
