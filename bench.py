@@ -133,6 +133,60 @@ def batched_rate(nb, device, tune, cycles_per_solve, ncyc=40):
     return out
 
 
+def gradient_rate(device, cycles=4, check=True):
+    """Forward-mode gradient of J (mgfvm_objective) for the first adjoint-configuration
+    case (256 x 256, seeded random obstacles, Re 100, per-face inlet profile): one
+    tangent context of nfy + 2 cases (every inlet face, amuf, prsc), timed per
+    V-cycle; two of its derivatives checked against central differences (h = 1e-6)
+    of the CPU oracle's V-cycles."""
+    from mgfvm import Solver, configs
+    cases, profs = configs.c4(1, seed=4)
+    cfg, prof = cases[0], profs[0]
+    dirs = [("inlet", k) for k in range(cfg.nfy)] + [("amuf", 0), ("prsc", 0)]
+    s = Solver([cfg] * len(dirs), device=device, tangent=True)
+    for c, (kind, idx) in enumerate(dirs):
+        s.set_inlet_profile(c, prof)
+        s.set_direction(c, kind, idx)
+    s.cycle(1)                                  # untimed warm-up cycle
+    s.cycle(cycles)
+    ms = s.last_elapsed_ms / cycles
+    total = 1 + cycles
+    dj = np.array([s.objective(c)[1] for c in range(len(dirs))])
+    s.close()
+    out = {"config": "adjoint configuration case 0: 256x256, ngrid 5, seeded random obstacles, Re 100, "
+                     "inlet profile 1 + 0.1 N(0,1)",
+           "method": "forward mode (tangent-linear, dual numbers), one batch of all directions",
+           "directions": len(dirs), "ms_per_cycle": round(ms, 3),
+           "direction_cycles_per_s": round(len(dirs) / (ms / 1e3), 1)}
+    if check:
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        import dataclasses
+        import oracle
+
+        def j_after(c, pr):
+            o = oracle.OracleCase(c, pr)
+            o.cycle(total)
+            p, sc = o.get(0, "p"), o.get(0, "sc")
+            o.close()
+            ny = p.shape[0] - 2
+            return (p[1:-1, 1].sum() / ny - p[1:-1, -2].sum() / ny) + sc[1:-1, -1].sum() / ny
+
+        k = int(np.argmax(np.abs(dj[:cfg.nfy])))
+        h = 1e-6 * abs(prof[k])
+        pp, pm = prof.copy(), prof.copy()
+        pp[k] += h
+        pm[k] -= h
+        fd_in = (j_after(cfg, pp) - j_after(cfg, pm)) / (2 * h)
+        ha = 1e-6 * cfg.amuf
+        fd_a = (j_after(dataclasses.replace(cfg, amuf=cfg.amuf + ha), prof)
+                - j_after(dataclasses.replace(cfg, amuf=cfg.amuf - ha), prof)) / (2 * ha)
+        out["check"] = {"cycles": total, "inlet_face": k,
+                        "rel_err_inlet": abs(dj[k] - fd_in) / abs(fd_in),
+                        "rel_err_amuf": abs(dj[cfg.nfy] - fd_a) / abs(fd_a),
+                        "bar": 1e-4}
+    return out
+
+
 def mixed_solve(cases, device, ref_solver, tune, profiles=None):
     """One solve of the workload with MGFVM_PREC_MIXED (FP32 correction smoothing
     against FP64 residuals), timed like a bench step, and the relative L2 distance of
@@ -296,6 +350,7 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the engine's default schedule")
     ap.add_argument("--batch", type=int, default=64,
                     help="cases of the batched obstacle-flow measurement (0: skip it)")
+    ap.add_argument("--no-gradient", action="store_true", help="skip the forward-mode gradient measurement")
     ap.add_argument("--profile-cycles", type=int, default=0,
                     help="only run 3 warm-up V-cycles then this many V-cycles of the workload "
                          "(for ncu launch lists) and exit")
@@ -393,16 +448,27 @@ def main():
     e2e = None
     if rank == 0 or True:
         def e2e_step():
+            t = [time.perf_counter()]
             with Solver(cases, device=local) as s2:
+                t.append(time.perf_counter())
                 for k, pr in enumerate(profiles or []):
                     s2.set_inlet_profile(k, pr)
                 if tuned:
                     s2.set_tuning(**tuned)
+                t.append(time.perf_counter())
                 s2.solve(max(c.nvcycle for c in cases), FP_TOL)
+                t.append(time.perf_counter())
+                dev = s2.last_elapsed_ms
                 for k in range(n_cases):
                     for f in ("u", "v", "p", "sc"):
                         s2.field(k, 0, f)
-                return s2.transfer_bytes
+                t.append(time.perf_counter())
+                b = s2.transfer_bytes
+            t.append(time.perf_counter())
+            d = np.diff(t) * 1e3
+            log(f"e2e step: create {d[0]:.1f} ms, inputs+schedule {d[1]:.1f}, solve {d[2]:.1f} "
+                f"(device {dev:.1f}), fields {d[3]:.1f}, release {d[4]:.1f}")
+            return b
 
         e2e_step()                           # untimed warm-up step
         torch.cuda.synchronize()
@@ -430,6 +496,11 @@ def main():
     batched = None
     if a.batch > 0 and a.workload == "c1":
         batched = batched_rate(a.batch, local, not a.no_autotune, cycles_per_solve)
+
+    # ---- derivatives: a whole gradient of J by forward mode, one batch
+    grad = None
+    if world == 1 and not a.no_gradient:
+        grad = gradient_rate(local, check=not a.no_cpu_baseline)
 
     # ---- parity spot check at full size: 3 cycles against the CPU oracle
     l2err = None
@@ -469,6 +540,7 @@ def main():
             "roofline": roofline,
             "batched": batched,
             "mixed": mixed,
+            "gradient": grad,
             "schedule": {"autotuned": tuned is not None,
                          "tuning": {k: v[:max(c.ngrid for c in cases)] for k, v in tuned.items()} if tuned else None},
             "cpu_baseline": cpu,
