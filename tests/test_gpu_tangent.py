@@ -64,7 +64,13 @@ CASES = {
     "obs_jacobi": lambda: small_cases()["obs_jacobi"],
     "obs_gs_touch": lambda: small_cases()["obs_gs_touch"],
     "odd_sweeps": lambda: small_cases()["odd_sweeps"],
+    "ports": lambda: small_cases()["ports"],
+    "bc_mix": lambda: small_cases()["bc_mix"],
+    "obs_below_coarsest": lambda: small_cases()["obs_below_coarsest"],
 }
+# a derivative the iteration does not see (an inlet face overwritten by a periodic copy,
+# or blocked): both sides are zero to rounding
+DJ_ATOL = 1e-12
 DIRECTIONS = [("inlet", 0), ("inlet", 9), ("inlet", 31), ("amuf", 0), ("prsc", 0)]
 
 
@@ -118,12 +124,17 @@ def test_tangent_matches_oracle_differences(name, oracle_built):
         d, dj_fd = oracle_fd(cfg, prof, cycles, kind, idx)
         for f in ["u", "v", "p", "sc"]:
             t = s.tangent(c, 0, f)
-            scale = max(np.abs(t).max(), np.abs(d[f]).max(), 1e-300)
+            scale = max(np.abs(t).max(), np.abs(d[f]).max())
+            if scale <= DJ_ATOL:
+                continue
             err = np.abs(t - d[f]).max() / scale
             assert err <= FIELD_RTOL, f"{kind}[{idx}] d{f}: max error {err:.2e} of its max {scale:.3e}"
         j, dj = s.objective(c)
         assert j == pytest.approx(j_of(*(oracle_state(cfg, prof, cycles)[f] for f in ("p", "sc"))), rel=1e-13)
-        rel = abs(dj - dj_fd) / max(abs(dj_fd), 1e-300)
+        if abs(dj_fd) <= DJ_ATOL:
+            assert abs(dj) <= DJ_ATOL, f"{kind}[{idx}]: dJ {dj:.3e} where the central difference is {dj_fd:.3e}"
+            continue
+        rel = abs(dj - dj_fd) / abs(dj_fd)
         worst = max(worst, rel)
         assert rel <= DJ_RTOL, f"{kind}[{idx}]: dJ {dj:.12e} vs central difference {dj_fd:.12e} ({rel:.2e})"
     s.close()
