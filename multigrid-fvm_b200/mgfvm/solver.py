@@ -115,10 +115,23 @@ class Solver:
     def cycle(self, n: int = 1) -> None:
         check(self._lib.mgfvm_cycle(self._h, n))
 
-    def solve(self, max_cycles: int, fp_tol: float = 0.0) -> np.ndarray:
+    def solve(self, max_cycles: int, fp_tol: float = 0.0, allow_nonfinite: bool = False) -> np.ndarray:
+        """Cycles each case ran.  A case whose mass error turns NaN/Inf stops there;
+        the call then fails with ENONFINITE unless `allow_nonfinite` (see `diverged`)."""
         out = np.zeros(self.ncases, dtype=np.int32)
-        check(self._lib.mgfvm_solve(self._h, max_cycles, fp_tol, out.ctypes.data_as(_ip)))
+        st = self._lib.mgfvm_solve(self._h, max_cycles, fp_tol, out.ctypes.data_as(_ip))
+        if not (allow_nonfinite and st == _abi.ENONFINITE):
+            check(st)
         return out
+
+    def diverged(self) -> List[int]:
+        """Cases whose last recorded mass error is NaN/Inf."""
+        bad = []
+        for k in range(self.ncases):
+            e, _ = self.history(k)
+            if e.size and not np.isfinite(e[-1]):
+                bad.append(k)
+        return bad
 
     def op(self, name: Union[str, int], level: int) -> None:
         op = _abi.OP[name] if isinstance(name, str) else name
