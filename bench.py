@@ -72,6 +72,22 @@ def cell_sweeps_per_cycle(cfg):
     return (3 * cfg.nswpm + cfg.nswpp) * tot
 
 
+def cycle_bytes(cfg):
+    """Algorithmic bytes of one V-cycle of a case, from the per-routine FP64 word counts
+    of the reference's loops: per cell and level visit 85 words of assembly (fluxes,
+    coefficient assembly, masserror/coefp, update) plus 8 per cell-sweep of smoothing
+    (3 nswpm + nswpp sweeps); per fine cell of each transfer 100 words of restriction
+    and 24 of prolongation."""
+    words = 0
+    for ig in range(cfg.ngrid):
+        cells = (cfg.nfx >> ig) * (cfg.nfy >> ig)
+        visits = 1 if ig in (0, cfg.ngrid - 1) else 2
+        words += visits * cells * (85 + 8 * (3 * cfg.nswpm + cfg.nswpp))
+        if ig < cfg.ngrid - 1:
+            words += cells * (100 + 24)
+    return 8 * words
+
+
 def load_peaks():
     try:
         with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
@@ -122,9 +138,16 @@ def batched_rate(nb, device, tune, cycles_per_solve, ncyc=40):
             s.cycle(3)
             s.cycle(ncyc)
             ms = s.last_elapsed_ms / ncyc
+            gbs = sum(cycle_bytes(c) for c in cases) / (ms / 1e3) / 1e9
+            peaks = load_peaks()
+            peak = peaks.get("hbm_gbs", 6650.0)
             out[label] = {"cases": n, "ms_per_cycle": round(ms, 4),
                           "case_cycles_per_s": round(n / (ms / 1e3), 1),
-                          "solves_per_s": round(n / (ms / 1e3) / max(cycles_per_solve), 4)}
+                          "solves_per_s": round(n / (ms / 1e3) / max(cycles_per_solve), 4),
+                          "cycle_roofline": {"bound": "hbm", "algorithmic_bytes_per_case_cycle": cycle_bytes(cases[0]),
+                                             "achieved": round(gbs, 1), "peak": peak, "unit": "GB/s",
+                                             "frac": round(gbs / peak, 4),
+                                             "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}}
             if n > 1:   # level-0 fields of the batch exceed L2: the smoother against HBM
                 out[label]["smoother_roofline"] = smoother_roofline(s, cases, ROOFLINE_TRAFFIC.get(f"c1x{n}"))
     out["speedup_per_case"] = round(out["batch"]["case_cycles_per_s"] / out["one_case"]["case_cycles_per_s"], 2)

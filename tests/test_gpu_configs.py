@@ -73,3 +73,33 @@ def test_inlet_profiles(oracle_built):
         o = OracleCase(cfg, pr)
         o.cycle(3)
         _check(s, k, o, 3, f"profile case {k}")
+
+
+def test_divergence_as_the_reference(oracle_built):
+    """A random-particle case on which the reference's iteration blows up (case 34 of
+    the adjoint configuration, seed 4: max |u| ~1e7 after cycle 2, NaN in cycle 3 in the
+    reference build): the engine follows it bit for bit while the values are finite,
+    goes non-finite in the same cycle, stops that case there in a solve, and keeps
+    solving the other cases of the batch."""
+    from mgfvm import MgfvmError, Solver, configs
+    from oracle import OracleCase
+    cases, profs = configs.c4(64, seed=4)
+    pick = [33, 34]
+    o = OracleCase(cases[34], profs[34])
+    s = Solver([cases[k] for k in pick])
+    for c, k in enumerate(pick):
+        s.set_inlet_profile(c, profs[k])
+    s.cycle(2)
+    o.cycle(2)
+    _check(s, 1, o, 2, "diverging case", levels=range(cases[34].ngrid))
+    assert np.abs(s.field(1, 0, "u")).max() > 1e6
+    s.cycle(1)
+    o.cycle(1)
+    assert not np.isfinite(s.history(1)[0][-1]) and not np.isfinite(o.history()[0][-1])
+    s.reset()
+    with pytest.raises(MgfvmError):
+        s.solve(10)
+    s.reset()
+    ran = s.solve(10, allow_nonfinite=True)
+    assert list(ran) == [10, 3] and s.diverged() == [1]
+    s.close()
