@@ -1527,32 +1527,47 @@ int mgfvm_gradient(const mgfvm_config *cfg, const double *inlet_u, int n_inlet, 
     mgfvm_clear_error();
     if (!cfg || ncycles < 0 || n_inlet < 0 || (n_inlet > 0 && !inlet_u))
         return mgfvm_fail(MGFVM_EINVAL, "bad gradient arguments");
-    const int nf = cfg->nfy, ncase = nf + 2;
-    std::vector<mgfvm_config> cases(ncase, *cfg);
+    const int nf = cfg->nfy, ndir = nf + 2;
     mgfvm_options opt;
     mgfvm_options_default(&opt);
     opt.device = device;
     opt.tangent = 1;
-    mgfvm_ctx *x = nullptr;
-    RC(mgfvm_create(cases.data(), ncase, &opt, &x));
-    int rc = MGFVM_OK;
-    do {
-        for (int c = 0; c < ncase; ++c) {
-            x->profile[c].assign(inlet_u, inlet_u + n_inlet);
-            x->dir_kind[c] = c < nf ? MGFVM_DIR_INLET : c == nf ? MGFVM_DIR_AMUF : MGFVM_DIR_PRSC;
-            x->dir_index[c] = c < nf ? c : 0;
+    // directions in batches: all at once where the device holds them, else halved
+    // until a batch fits
+    int chunk = ndir;
+    for (int d0 = 0; d0 < ndir;) {
+        const int n = std::min(chunk, ndir - d0);
+        std::vector<mgfvm_config> cases(n, *cfg);
+        mgfvm_ctx *x = nullptr;
+        int rc = mgfvm_create(cases.data(), n, &opt, &x);
+        if (rc == MGFVM_ENOMEM && chunk > 1) {
+            cudaGetLastError();   // the failed allocation's error must not reach the next batch's checks
+            chunk = (chunk + 1) / 2;
+            continue;
         }
-        if ((rc = upload_profiles(x)) != MGFVM_OK) break;
-        if ((rc = init_state(x, -1)) != MGFVM_OK) break;
-        if ((rc = mgfvm_cycle(x, ncycles)) != MGFVM_OK) break;
-        if (J && (rc = mgfvm_objective(x, 0, J, nullptr)) != MGFVM_OK) break;
-        for (int c = 0; c < ncase && rc == MGFVM_OK; ++c) {
-            double *dst = c < nf ? (dJ_dinlet ? dJ_dinlet + c : nullptr) : c == nf ? dJ_damuf : dJ_dprsc;
-            if (dst) rc = mgfvm_objective(x, c, nullptr, dst);
-        }
-    } while (0);
-    mgfvm_destroy(x);
-    return rc;
+        RC(rc);
+        do {
+            for (int c = 0; c < n; ++c) {
+                const int d = d0 + c;
+                x->profile[c].assign(inlet_u, inlet_u + n_inlet);
+                x->dir_kind[c] = d < nf ? MGFVM_DIR_INLET : d == nf ? MGFVM_DIR_AMUF : MGFVM_DIR_PRSC;
+                x->dir_index[c] = d < nf ? d : 0;
+            }
+            if ((rc = upload_profiles(x)) != MGFVM_OK) break;
+            if ((rc = init_state(x, -1)) != MGFVM_OK) break;
+            if ((rc = mgfvm_cycle(x, ncycles)) != MGFVM_OK) break;
+            if (d0 == 0 && J && (rc = mgfvm_objective(x, 0, J, nullptr)) != MGFVM_OK) break;
+            for (int c = 0; c < n && rc == MGFVM_OK; ++c) {
+                const int d = d0 + c;
+                double *dst = d < nf ? (dJ_dinlet ? dJ_dinlet + d : nullptr) : d == nf ? dJ_damuf : dJ_dprsc;
+                if (dst) rc = mgfvm_objective(x, c, nullptr, dst);
+            }
+        } while (0);
+        mgfvm_destroy(x);
+        RC(rc);
+        d0 += n;
+    }
+    return MGFVM_OK;
 }
 
 }  // extern "C"
