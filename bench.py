@@ -380,6 +380,9 @@ def main():
     ap.add_argument("--profile-cycles", type=int, default=0,
                     help="only run 3 warm-up V-cycles then this many V-cycles of the workload "
                          "(for ncu launch lists) and exit")
+    ap.add_argument("--profile-tangent", type=int, default=0,
+                    help="only run this many tangent V-cycles of a small gradient batch (64x64 channel, "
+                         "all 66 directions) after 2 warm-up cycles, inside the NVTX range 'profile', and exit")
     a = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -397,6 +400,19 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
 
     from mgfvm import Solver
+    if a.profile_tangent:
+        from mgfvm import configs
+        cfg = configs.c0(2)
+        dirs = [("inlet", k) for k in range(cfg.nfy)] + [("amuf", 0), ("prsc", 0)]
+        with Solver([cfg] * len(dirs), device=local, tangent=True) as t:
+            for c, (kind, idx) in enumerate(dirs):
+                t.set_direction(c, kind, idx)
+            t.cycle(2)
+            torch.cuda.nvtx.range_push("profile")
+            t.cycle(a.profile_tangent)
+            torch.cuda.nvtx.range_pop()
+            log(f"tangent: {len(dirs)} directions, {t.last_elapsed_ms / a.profile_tangent:.3f} ms per V-cycle")
+        return
     cases, desc, profiles = workload(a.workload)
     n_cases = len(cases)
     solver = Solver(cases, device=local, sync_every=64, tail_level=a.tail)
