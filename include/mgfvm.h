@@ -314,7 +314,8 @@ int mgfvm_objective(mgfvm_ctx *ctx, int icase, double *J, double *dJ);
  * the given per-face inlet profile (may be empty): creates a tangent context of
  * nfy + 2 cases (every inlet face, amuf, prsc) on `device`, runs it and releases it;
  * where the device cannot hold them all, the directions run in batches of half the
- * size, halved again until one fits.  dJ_dinlet receives nfy values; any output may be
+ * size, halved again until one fits (the environment variable MGFVM_GRADIENT_BATCH,
+ * if set to n >= 1, caps a batch at n directions).  dJ_dinlet receives nfy values; any output may be
  * NULL. */
 int mgfvm_gradient(const mgfvm_config *cfg, const double *inlet_u, int n_inlet, int ncycles, int device,
                    double *J, double *dJ_dinlet, double *dJ_damuf, double *dJ_dprsc);

@@ -1532,9 +1532,13 @@ int mgfvm_gradient(const mgfvm_config *cfg, const double *inlet_u, int n_inlet, 
     mgfvm_options_default(&opt);
     opt.device = device;
     opt.tangent = 1;
-    // directions in batches: all at once where the device holds them, else halved
-    // until a batch fits
+    // directions in batches: all at once where the device holds them (or at most
+    // MGFVM_GRADIENT_BATCH, when set), else halved until a batch fits
     int chunk = ndir;
+    if (const char *env = std::getenv("MGFVM_GRADIENT_BATCH")) {
+        const int cap = std::atoi(env);
+        if (cap >= 1) chunk = std::min(chunk, cap);
+    }
     for (int d0 = 0; d0 < ndir;) {
         const int n = std::min(chunk, ndir - d0);
         std::vector<mgfvm_config> cases(n, *cfg);

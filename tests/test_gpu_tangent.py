@@ -190,3 +190,32 @@ def test_tangent_context_refuses_state_edits(oracle_built):
     s.close()
     with pytest.raises(MgfvmError):
         Solver(cfg, tangent=True, precision="mixed")
+
+
+def test_gradient_in_batches_and_mixed_cases(oracle_built, monkeypatch):
+    """The gradient is the same whether its directions run in one batch or in batches of
+    five (MGFVM_GRADIENT_BATCH), and a tangent context may hold cases of different sizes
+    and obstacles, each differentiated as on its own."""
+    import mgfvm
+    cfg = CASES["obs_jacobi"]()
+    prof = _profile(cfg)
+    whole = mgfvm.gradient(cfg, prof, 2)
+    monkeypatch.setenv("MGFVM_GRADIENT_BATCH", "5")
+    parts = mgfvm.gradient(cfg, prof, 2)
+    assert whole[0] == parts[0] and whole[2] == parts[2] and whole[3] == parts[3]
+    np.testing.assert_array_equal(whole[1], parts[1])
+
+    from mgfvm import Solver
+    other = small_cases()["c0_jacobi"].replace(nfx=64, nfy=32, xl=2.0)
+    prof2 = _profile(other, seed=5)
+    s = Solver([cfg, other], tangent=True)
+    s.set_inlet_profile(0, prof)
+    s.set_inlet_profile(1, prof2)
+    s.set_direction(0, "amuf")
+    s.set_direction(1, "inlet", 7)
+    s.cycle(3)
+    for c, (cc, pr, kind, idx) in enumerate([(cfg, prof, "amuf", 0), (other, prof2, "inlet", 7)]):
+        _, dj_fd = oracle_fd(cc, pr, 3, kind, idx)
+        _, dj = s.objective(c)
+        assert abs(dj - dj_fd) <= DJ_RTOL * abs(dj_fd), f"case {c}: {dj} vs {dj_fd}"
+    s.close()
