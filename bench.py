@@ -383,6 +383,10 @@ def main():
     ap.add_argument("--profile-tangent", type=int, default=0,
                     help="only run this many tangent V-cycles of a small gradient batch (64x64 channel, "
                          "all 66 directions) after 2 warm-up cycles, inside the NVTX range 'profile', and exit")
+    ap.add_argument("--profile-batch-smoother", choices=["plain", "tma"], default=None,
+                    help="only run one V-cycle of the 64-case obstacle-flow batch (levels 0-2 smoothed by "
+                         "512-thread tiles of 6 units, per-thread or TMA-staged loads) after 3 warm-up cycles, "
+                         "inside the NVTX range 'profile', and exit")
     a = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -400,6 +404,20 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
 
     from mgfvm import Solver
+    if a.profile_batch_smoother:
+        from mgfvm import configs
+        cases = [configs.c1(10.0 if k % 2 == 0 else 100.0, seed=k + 1) for k in range(64)]
+        t = 2 if a.profile_batch_smoother == "tma" else 1
+        with Solver(cases, device=local) as s:
+            s.set_tuning(smooth_units={0: 6, 1: 6, 2: 6}, smooth_threads={0: 512, 1: 512, 2: 512},
+                         smooth_tma={0: t, 1: t, 2: t})
+            s.cycle(3)
+            torch.cuda.nvtx.range_push("profile")
+            s.cycle(1)
+            torch.cuda.nvtx.range_pop()
+            s.cycle(10)
+            log(f"batch smoother {a.profile_batch_smoother}: {s.last_elapsed_ms / 10:.3f} ms per V-cycle")
+        return
     if a.profile_tangent:
         from mgfvm import configs
         cfg = configs.c0(2)

@@ -161,6 +161,8 @@ typedef struct mgfvm_tuning {
                                               whole visit (assembly, u/v/sc smoothing,
                                               p', update) in one launch: 0 or 2 yes,
                                               1 no                                      */
+    int smooth_tma[MGFVM_MAX_LEVELS];      /* tile smoother regions staged in shared memory
+                                              by TMA box loads: 2 yes, 0 or 1 no        */
 } mgfvm_tuning;
 
 typedef struct mgfvm_ctx mgfvm_ctx;

@@ -7,6 +7,9 @@
 // `sync_every` cycles and a converged case costs nothing but early-exiting blocks.
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
+#include <map>
+#include <tuple>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -18,6 +21,8 @@
 #include "mg_kernels.cuh"
 #include "mg_tangent.cuh"
 #include "mgfvm_host.h"
+
+#include <cudaTypedefs.h>
 
 using namespace mg;
 
@@ -79,6 +84,9 @@ struct mgfvm_ctx {
     std::vector<CaseTan> ht;
     CaseTan *dt = nullptr;
     std::vector<int> dir_kind, dir_index;
+    // tensor maps of the V-cycle's TMA-staged smoother launches (host copy, device table)
+    std::vector<SmoothMap> hmaps;
+    SmoothMap *dmaps = nullptr;
 };
 
 static inline int npx_of(const mgfvm_config &c, int ig) { return c.nfx / (1 << ig) + 2; }
@@ -89,9 +97,76 @@ static inline int nblk(long long n) { return (int)std::max<long long>(1, (n + BL
 // ------------------------------------------------------------------ schedule
 namespace {
 
+// cuTensorMapEncodeTiled from the driver (through the runtime: no link to libcuda), or
+// nullptr where the driver does not provide it
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+        cudaGetLastError();
+    }
+    return fn;
+}
+
+// The two tensor maps of a TMA-staged smoother launch on level L with a bw x bh box:
+// the level's first NSLOTS_LEVEL slot arrays as an (x, y, slot) tensor.  False where
+// the layout does not allow it (slots not at one stride, a row not a multiple of 16
+// bytes) or the encoder refuses.
+static bool encode_smooth_maps(const LevelDev &L, int bw, int bh, SmoothMap &m)
+{
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc || !L.f[0] || !L.f[1] || (bw & 1) || bw > 256 || bh > 256) return false;
+    const char *base = (const char *)L.f[0];
+    const long long stride = (const char *)L.f[1] - base;
+    for (int s = 0; s < NSLOTS_LEVEL; ++s)
+        if (!L.f[s] || (const char *)L.f[s] - base != s * stride) return false;
+    const long long row = (long long)L.npx * (long long)sizeof(double);
+    if (row % 16 || stride % 16 || stride < row * L.npy || ((uintptr_t)base & 15)) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)L.npx, (cuuint64_t)L.npy, (cuuint64_t)NSLOTS_LEVEL};
+    const cuuint64_t strides[2] = {(cuuint64_t)row, (cuuint64_t)stride};
+    const cuuint32_t boxc[3] = {(cuuint32_t)bw, (cuuint32_t)bh, (cuuint32_t)NCOEF};
+    const cuuint32_t boxf[3] = {(cuuint32_t)bw, (cuuint32_t)bh, 1u};
+    const cuuint32_t es[3] = {1u, 1u, 1u};
+    return enc(&m.coef, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void *)base, dims, strides, boxc, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS &&
+           enc(&m.field, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void *)base, dims, strides, boxf, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 struct Builder {
     mgfvm_ctx *x;
     std::vector<Launch> *out;
+    std::vector<SmoothMap> *maps = nullptr;               // where TMA-staged launches may be emitted
+    std::map<std::tuple<int, int, int>, int> map_index{};   // (level, bw, bh) -> first map of its cases
+
+    // index of the per-case tensor maps of a (level, box) shape, or -1 where some case's
+    // level cannot be staged by TMA
+    int smooth_maps(int ig, int bw, int bh)
+    {
+        const auto key = std::make_tuple(ig, bw, bh);
+        auto it = map_index.find(key);
+        if (it != map_index.end()) return it->second;
+        const int base = (int)maps->size();
+        std::vector<SmoothMap> m(x->ncases);
+        bool ok = true;
+        for (int c = 0; c < x->ncases && ok; ++c) {
+            std::memset(&m[c], 0, sizeof(SmoothMap));
+            if (ig < x->cfg[c].ngrid) ok = encode_smooth_maps(x->hc[c].lv[ig], bw, bh, m[c]);
+        }
+        const int idx = ok ? base : -1;
+        if (ok) maps->insert(maps->end(), m.begin(), m.end());
+        map_index[key] = idx;
+        return idx;
+    }
 
     bool any(int ig, int mode) const
     {
@@ -176,14 +251,22 @@ struct Builder {
         const int hmax = (units + chunks - 1) / chunks;
         const int tile = smooth_pairs_side(hmax, nt);
         const int side = tile + 2 * hmax;
+        // TMA staging: a box one column wider than the region where it starts at an odd x
+        const int bw = (side + 2) & ~1, bh = side;
+        const int tma_smem = (NCOEF + 1 + bufs - 1) * bw * bh * (int)sizeof(double);
+        const int mi = maps && kern == K_SMOOTH && mode != M_OP && x->tune.smooth_tma[ig] == 2 &&
+                               tma_smem <= SMOOTH_TMA_SMEM_MAX
+                           ? smooth_maps(ig, bw, bh)
+                           : -1;
         int u0 = 0;
         for (int c = 0; c < chunks; ++c) {
             const int nu = units / chunks + (c < units % chunks ? 1 : 0);
-            Launch &L = add(kern, ig, mode, 0, mask, u0, nu, c & 1);
+            Launch &L = add(mi >= 0 ? K_SMOOTH_TMA : kern, ig, mode, 0, mask, u0, nu, c & 1);
             L.a4 = tile;
             L.grid = dim3((unsigned)tiles(ig, tile), x->ncases, neq);
             L.block = std::min(nt, round32(side * ((side + 1) / 2)));
-            L.smem = smem_for(side * side);
+            L.smem = mi >= 0 ? tma_smem : smem_for(side * side);
+            if (mi >= 0) { L.bw = bw; L.bh = bh; L.map = mi; }
             u0 += nu;
         }
         if (chunks & 1) {
@@ -630,6 +713,41 @@ int seed_tangent(mgfvm_ctx *x, int c)
     return MGFVM_OK;
 }
 
+// The V-cycle's launch list, and the device table of tensor maps its TMA-staged
+// smoother launches read (without that table, those launches are plain tile launches).
+int build_cycle(mgfvm_ctx *x)
+{
+    x->cyc.clear();
+    x->hmaps.clear();
+    if (x->dmaps) {
+        cudaStreamSynchronize(x->stream);
+        cudaFree(x->dmaps);
+        x->dmaps = nullptr;
+    }
+    {
+        Builder b{x, &x->cyc, &x->hmaps};
+        b.cycle();
+    }
+    if (x->hmaps.empty()) return MGFVM_OK;
+    cudaError_t e = cudaMalloc(&x->dmaps, sizeof(SmoothMap) * x->hmaps.size());
+    if (e == cudaSuccess)
+        e = cudaMemcpy(x->dmaps, x->hmaps.data(), sizeof(SmoothMap) * x->hmaps.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        if (x->dmaps) cudaFree(x->dmaps);
+        x->dmaps = nullptr;
+        x->cyc.clear();
+        x->hmaps.clear();
+        Builder b{x, &x->cyc};
+        b.cycle();
+        return MGFVM_OK;
+    }
+    x->h2d += (long long)(sizeof(SmoothMap) * x->hmaps.size());
+    for (Launch &L : x->cyc)
+        if (L.kernel == K_SMOOTH_TMA) L.ptr = x->dmaps + L.map;
+    return MGFVM_OK;
+}
+
 int init_state(mgfvm_ctx *x, int only_case)
 {
     for (int c = 0; c < x->ncases; ++c) {
@@ -688,6 +806,7 @@ void destroy_all(mgfvm_ctx *x)
     if (x->graph) cudaGraphDestroy(x->graph);
     if (x->pool) cudaFree(x->pool);
     if (x->tpool) cudaFree(x->tpool);
+    if (x->dmaps) cudaFree(x->dmaps);
     if (x->dt) cudaFree(x->dt);
     if (x->hist) cudaFree(x->hist);
     if (x->dprofile) cudaFree(x->dprofile);
@@ -918,9 +1037,7 @@ int create_impl(const mgfvm_config *cases, int ncases, const mgfvm_options *opt_
     CK(configure_kernels());
     if (opt.tangent) RC(alloc_tangent(x));
     RC(init_state(x, -1));
-    Builder b{x, &x->cyc};
-    b.cycle();
-    return MGFVM_OK;
+    return build_cycle(x);
 }
 
 }  // namespace
@@ -973,9 +1090,12 @@ int mgfvm_set_inlet_profile(mgfvm_ctx *x, int icase, const double *u, int n)
 // A kernel found its launch shape too small for its tile (a schedule bug): fail loudly.
 static int check_status(mgfvm_ctx *x)
 {
-    for (int c = 0; c < x->ncases; ++c)
+    for (int c = 0; c < x->ncases; ++c) {
         if (x->hs[c].status & CASE_BAD_LAUNCH)
             return mgfvm_fail(MGFVM_ECUDA, "case %d: a smoother launch was too small for its tile", c);
+        if (x->hs[c].status & CASE_WAIT_TIMEOUT)
+            return mgfvm_fail(MGFVM_ETIMEOUT, "case %d: a smoother CTA gave up waiting for its TMA loads", c);
+    }
     return MGFVM_OK;
 }
 
@@ -1225,6 +1345,7 @@ static bool tuning_valid(const mgfvm_tuning &t)
         if (t.update_pfix[ig] < 0 || t.update_pfix[ig] > 2) return false;
         if (t.odd_chunks[ig] < 0 || t.odd_chunks[ig] > 2) return false;
         if (t.pp_level[ig] < 0 || t.pp_level[ig] > 2) return false;
+        if (t.smooth_tma[ig] < 0 || t.smooth_tma[ig] > 2) return false;
     }
     return true;
 }
@@ -1236,9 +1357,7 @@ static void rebuild_schedule(mgfvm_ctx *x)
     if (x->graph) cudaGraphDestroy(x->graph);
     x->gexec = nullptr;
     x->graph = nullptr;
-    x->cyc.clear();
-    Builder b{x, &x->cyc};
-    b.cycle();
+    build_cycle(x);
 }
 
 // Milliseconds per graph-replayed V-cycle (best of two runs of n), stop rule off.
@@ -1316,6 +1435,7 @@ int mgfvm_autotune(mgfvm_ctx *x, int cycles, mgfvm_tuning *chosen, double *ms_be
                                               {SMOOTH_BLOCK / 4, 3}, {SMOOTH_BLOCK / 4, 5}};
                 for (auto &o : opts) knobs.push_back({0, o[0], o[1]});
             }
+            if (!probe.whole_level(ig, mx, my)) knobs.push_back({3, 2, 0});
             knobs.push_back({1, 1, 0});
             knobs.push_back({1, 3, 0});
             if (ig + 1 < x->maxng) {
@@ -1327,6 +1447,7 @@ int mgfvm_autotune(mgfvm_ctx *x, int cycles, mgfvm_tuning *chosen, double *ms_be
                 if (k[0] == 0) { cand.smooth_threads[ig] = k[1]; cand.smooth_units[ig] = k[2]; }
                 if (k[0] == 1) cand.asm_slices[ig] = k[1];
                 if (k[0] == 2) cand.restrict_slices[ig] = k[1];
+                if (k[0] == 3) cand.smooth_tma[ig] = k[1];
                 if (memcmp(&cand, &keep, sizeof cand) == 0) continue;
                 x->tune = cand;
                 rebuild_schedule(x);

@@ -442,6 +442,123 @@ __global__ void __launch_bounds__(NT, SMOOTH_BLOCK / NT) k_smooth(const CaseDev 
     if (P.outB) dst[P.gB] = res[kB];
 }
 
+// ------------------------------------------------ TMA-staged tile smoother
+// The same tiles, units and windows as k_smooth, with the region staged in shared
+// memory by two tensor-memory-accelerator box loads instead of per-thread loads: the
+// six coefficient arrays of the equation as one box (they are consecutive slots of the
+// level) and the field (or its ping-pong buffer).  The tensor maps view a level's
+// slot arrays as one 3-D tensor (x, y, slot; the slots sit at a constant stride) and
+// are built per case and launch shape by the host (SmoothMaps).  A box starts at an
+// even x (8-byte elements: the copy's x must be a multiple of 2) and is one column
+// wider where the region starts at an odd x; cells the box holds beyond the region are
+// loaded and never written.  The field box is the shared-memory field the units
+// update, so the results are those of k_smooth bit for bit.
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+// Wait for the mbarrier's phase 0 with a bounded number of polls; false on timeout.
+__device__ __forceinline__ bool mbar_wait0(unsigned bar)
+{
+    for (int it = 0; it < (1 << 22); ++it) {
+        unsigned done;
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(done)
+                     : "r"(bar)
+                     : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+template <int ISOLVE, int NT>
+__global__ void __launch_bounds__(NT, SMOOTH_BLOCK / NT)
+    k_smooth_tma(const CaseDev *__restrict__ cs, CaseState *st, const SmoothMap *__restrict__ maps, int ig, int mode,
+                 int mask, int u0, int nu, int dir, int tile, int bw, int bh)
+{
+    extern __shared__ __align__(128) double smt[];
+    __shared__ __align__(8) unsigned long long mbar;
+    const CaseDev &C = cs[blockIdx.y];
+    if (!case_active(C, st[blockIdx.y], ig, mode)) return;
+    const int e = nth_eq(mask, blockIdx.z);
+    const LevelDev &L = C.lv[ig];
+    PairTile P;
+    const int g = pair_tile(L, e, nu, tile, P, blockIdx.x);
+    if (g == 1) return;
+    const int x0 = P.rx0 & ~1, off = P.rx0 - x0;
+    if (g == 2 || P.W + off > bw || P.Hh > bh) {   // the schedule sizes blocks and boxes to fit; never taken
+        if (threadIdx.x == 0) atomicOr(&st[blockIdx.y].status, (int)CASE_BAD_LAUNCH);
+        return;
+    }
+    const int box = bw * bh;
+    double *coef = smt, *phi = smt + NCOEF * box, *phi2 = phi + box;
+    const unsigned bar = smem_u32(&mbar);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const SmoothMap &M = maps[blockIdx.y];
+        const unsigned bytes = (unsigned)((NCOEF + 1) * box * sizeof(double));
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+        asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+                     ::"r"(smem_u32(coef)), "l"(&M.coef), "r"(x0), "r"(P.ry0), "r"(co_slot(e, CK_AW)), "r"(bar)
+                     : "memory");
+        asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+                     ::"r"(smem_u32(phi)), "l"(&M.field), "r"(x0), "r"(P.ry0), "r"(dir == 1 ? eq_tmp(e) : eq_field(e)),
+                       "r"(bar)
+                     : "memory");
+    }
+    if (!mbar_wait0(bar)) {
+        // record the stall and give the copies a second bounded wait before leaving
+        if (threadIdx.x == 0) atomicOr(&st[blockIdx.y].status, (int)CASE_WAIT_TIMEOUT);
+        mbar_wait0(bar);
+        return;
+    }
+    const int W = bw, limA = P.limA, limB = P.limB;
+    const int kA = (P.jA - P.ry0) * bw + (P.i - x0), kB = (P.jB - P.ry0) * bw + (P.i - x0);
+    double *dst = L.f[dir == 0 ? eq_tmp(e) : eq_field(e)];
+    double A[6] = {0, 0, 0, 0, 0, 0}, B[6] = {0, 0, 0, 0, 0, 0};
+    if (P.okA)
+        for (int a = 0; a < 6; ++a) A[a] = coef[a * box + kA];
+    if (P.okB)
+        for (int a = 0; a < 6; ++a) B[a] = coef[a * box + kB];
+    const double eps = ISOLVE == MGFVM_JACOBI ? 1.0e-30 : 0.0;   // solver's (ap + 1e-30), solvergs' ap
+    const Recip RA = make_recip(ISOLVE == MGFVM_JACOBI ? A[4] + eps : A[4]);
+    const Recip RB = make_recip(ISOLVE == MGFVM_JACOBI ? B[4] + eps : B[4]);
+    if (ISOLVE == MGFVM_JACOBI) {
+        if (P.okA) phi2[kA] = phi[kA];
+        if (P.okB) phi2[kB] = phi[kB];
+        __syncthreads();
+    }
+    for (int h = 1; h <= nu; ++h) {
+        if (ISOLVE == MGFVM_GAUSS_SEIDEL) {
+            if (((u0 + h - 1) & 1) == 0) {
+                if (h <= limA)
+                    phi[kA] = gs_value_r(A[0], A[1], A[2], A[3], RA, A[5], phi[kA - 1], phi[kA + 1], phi[kA - W],
+                                         phi[kA + W]);
+            } else {
+                if (h <= limB)
+                    phi[kB] = gs_value_r(B[0], B[1], B[2], B[3], RB, B[5], phi[kB - 1], phi[kB + 1], phi[kB - W],
+                                         phi[kB + W]);
+            }
+        } else {
+            const double *cur = ((h - 1) & 1) ? phi2 : phi;
+            double *nxt = ((h - 1) & 1) ? phi : phi2;
+            if (h <= limA)
+                nxt[kA] = jacobi_value_r(A[0], A[1], A[2], A[3], RA, A[5], cur[kA - 1], cur[kA + 1], cur[kA - W],
+                                         cur[kA + W], cur[kA]);
+            if (h <= limB)
+                nxt[kB] = jacobi_value_r(B[0], B[1], B[2], B[3], RB, B[5], cur[kB - 1], cur[kB + 1], cur[kB - W],
+                                         cur[kB + W], cur[kB]);
+        }
+        __syncthreads();
+    }
+    const double *res = (ISOLVE == MGFVM_JACOBI && (nu & 1)) ? phi2 : phi;
+    if (P.outA) dst[P.gA] = res[kA];
+    if (P.outB) dst[P.gB] = res[kB];
+}
+
 // All `mu` units of equation e on a level that one CTA holds, in place (k_smooth with
 // one tile covering the domain).  Returns pair_tile's verdict (uniform over the CTA).
 template <int ISOLVE>
@@ -1218,7 +1335,31 @@ int smooth_pairs_side(int units, int threads)
 
 cudaError_t configure_kernels()
 {
-    return cudaFuncSetAttribute(k_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, TAIL_SMEM_MAX);
+    cudaError_t e = cudaFuncSetAttribute(k_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, TAIL_SMEM_MAX);
+    const void *tma[] = {(const void *)k_smooth_tma<MGFVM_JACOBI, SMOOTH_BLOCK>,
+                         (const void *)k_smooth_tma<MGFVM_JACOBI, SMOOTH_BLOCK / 2>,
+                         (const void *)k_smooth_tma<MGFVM_JACOBI, SMOOTH_BLOCK / 4>,
+                         (const void *)k_smooth_tma<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK>,
+                         (const void *)k_smooth_tma<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK / 2>,
+                         (const void *)k_smooth_tma<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK / 4>};
+    for (const void *f : tma)
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, SMOOTH_TMA_SMEM_MAX);
+    return e;
+}
+
+template <int ISOLVE>
+static void launch_smooth_tma(const Launch &X, dim3 g, int b, const CaseDev *dc, CaseState *ds, cudaStream_t st)
+{
+    const SmoothMap *m = (const SmoothMap *)X.ptr;
+    if (b <= SMOOTH_BLOCK / 4)
+        k_smooth_tma<ISOLVE, SMOOTH_BLOCK / 4><<<g, b, X.smem, st>>>(dc, ds, m, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3,
+                                                                     X.a4, X.bw, X.bh);
+    else if (b <= SMOOTH_BLOCK / 2)
+        k_smooth_tma<ISOLVE, SMOOTH_BLOCK / 2><<<g, b, X.smem, st>>>(dc, ds, m, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3,
+                                                                     X.a4, X.bw, X.bh);
+    else
+        k_smooth_tma<ISOLVE, SMOOTH_BLOCK><<<g, b, X.smem, st>>>(dc, ds, m, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3,
+                                                                 X.a4, X.bw, X.bh);
 }
 
 template <int ISOLVE>
@@ -1273,6 +1414,11 @@ cudaError_t launch_one(const Launch &X, const CaseDev *dc, CaseState *ds, const 
         }
         break;
     case K_COPY: k_copy<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, X.a0); break;
+    case K_SMOOTH_TMA:
+        if (b > SMOOTH_BLOCK || !X.ptr || X.smem > SMOOTH_TMA_SMEM_MAX || (X.bw & 1)) return cudaErrorInvalidValue;
+        if (S.isolve == MGFVM_JACOBI) launch_smooth_tma<MGFVM_JACOBI>(X, g, b, dc, ds, st);
+        else launch_smooth_tma<MGFVM_GAUSS_SEIDEL>(X, g, b, dc, ds, st);
+        break;
     case K_PP_LEVEL:
         if (b > SMOOTH_BLOCK) return cudaErrorInvalidValue;
         if (S.isolve == MGFVM_JACOBI)

@@ -1,6 +1,8 @@
 // mg_kernels.cuh — host-side launchers of the engine's kernels.
 #pragma once
 
+#include <cuda.h>
+
 #include "mg_common.cuh"
 
 namespace mg {
@@ -26,6 +28,7 @@ enum KernelId {
     K_TAIL_TAN,      // K_TAIL with derivatives (a tangent context)
     K_LEVEL_VISIT,   // a whole one-CTA level visit, a cluster of 3 CTAs per case: K_PP_LEVEL's
                      // a0-a2, a3 = assembly bits (0: done), a4 = u/v/sc units
+    K_SMOOTH_TMA,    // as K_SMOOTH, the region staged by TMA box loads (bw, bh, ptr)
     K_NKERNELS
 };
 
@@ -37,6 +40,16 @@ struct Launch {
     dim3 grid;
     int block;
     int smem;
+    int bw, bh;        // K_SMOOTH_TMA: box width and height
+    int map;           // K_SMOOTH_TMA: index of its first tensor-map pair in the schedule's table
+    const void *ptr;   // K_SMOOTH_TMA: that pair on the device (one per case)
+};
+
+// The tensor maps of one case for a TMA-staged smoother launch: the level's slot
+// arrays as one (x, y, slot) tensor, with a box of NCOEF slots (the coefficients) and
+// one of a single slot (the field).
+struct __align__(64) SmoothMap {
+    CUtensorMap coef, field;
 };
 
 struct Sched {
@@ -72,6 +85,7 @@ cudaError_t raw_check_division(long long n, unsigned long long seed, unsigned lo
 
 constexpr int BLOCK = 256;
 constexpr int PFIX_BOUND_BLOCK = 1024;
+constexpr int SMOOTH_TMA_SMEM_MAX = 200 * 1024;   // dynamic shared memory of a TMA-staged smoother CTA
 constexpr int TAIL_BLOCK = 512;
 constexpr int TAIL_SMEM_MAX = 220 * 1024;   // dynamic shared memory of the coarse kernel (+ its static 256 B)
 

@@ -187,6 +187,9 @@ TUNINGS = [
     {"smooth_units": [3, 7, 5], "smooth_threads": [256, 256, 256]},
     {"update_pfix": [1, 1, 1], "odd_chunks": [1, 1, 1], "pp_level": [1, 1, 1]},
     {"smooth_units": [5, 3, 7], "odd_chunks": [2, 2, 2]},
+    {"smooth_tma": [2, 2, 2]},
+    {"smooth_tma": [2, 2, 2], "smooth_units": [3, 5, 7], "smooth_threads": [512, 256, 1024]},
+    {"smooth_tma": [2, 2, 2], "smooth_units": [7, 1, 4], "smooth_threads": [256, 512, 512], "odd_chunks": [1, 1, 1]},
 ]
 
 
@@ -220,7 +223,8 @@ def test_autotune_keeps_state(oracle_built):
     o.cycle(2)
     before, after, chosen = s.autotune(2)
     assert before > 0 and 0 < after <= before
-    assert set(chosen) == {"smooth_units", "smooth_threads", "asm_slices", "restrict_slices", "update_pfix", "odd_chunks", "pp_level"}
+    assert set(chosen) == {"smooth_units", "smooth_threads", "asm_slices", "restrict_slices", "update_pfix", "odd_chunks", "pp_level",
+                           "smooth_tma"}
     _compare(s, o, STATE, what="after autotune")
     s.cycle(3)
     o.cycle(3)
