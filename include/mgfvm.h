@@ -163,6 +163,10 @@ typedef struct mgfvm_tuning {
                                               1 no                                      */
     int smooth_tma[MGFVM_MAX_LEVELS];      /* tile smoother regions staged in shared memory
                                               by TMA box loads: 2 yes, 0 or 1 no        */
+    int coarse_kernel[MGFVM_MAX_LEVELS];   /* 2: this level and every coarser one run in
+                                              the one-CTA-per-case coarse kernel (the
+                                              first level marked 2 counts); 0 or 1
+                                              everywhere: mgfvm_options.tail_level      */
 } mgfvm_tuning;
 
 typedef struct mgfvm_ctx mgfvm_ctx;

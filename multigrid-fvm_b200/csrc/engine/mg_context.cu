@@ -87,6 +87,7 @@ struct mgfvm_ctx {
     // tensor maps of the V-cycle's TMA-staged smoother launches (host copy, device table)
     std::vector<SmoothMap> hmaps;
     SmoothMap *dmaps = nullptr;
+    std::vector<int> tail0;                   // per case: first one-CTA-kernel level chosen at creation
 };
 
 static inline int npx_of(const mgfvm_config &c, int ig) { return c.nfx / (1 << ig) + 2; }
@@ -940,6 +941,7 @@ int create_impl(const mgfvm_config *cases, int ncases, const mgfvm_options *opt_
             for (int ig = 0; ig < g.ngrid; ++ig)
                 if (npx_of(g, ig) * npy_of(g, ig) <= TAIL_AUTO_CELLS) { tail = ig; break; }
         C.tail = tail;
+        x->tail0.push_back(tail);
         C.partials = (double *)(x->pool + part_off[c]);
         C.counters = (unsigned *)(x->pool + cnt_off[c]);
     }
@@ -1346,18 +1348,39 @@ static bool tuning_valid(const mgfvm_tuning &t)
         if (t.odd_chunks[ig] < 0 || t.odd_chunks[ig] > 2) return false;
         if (t.pp_level[ig] < 0 || t.pp_level[ig] > 2) return false;
         if (t.smooth_tma[ig] < 0 || t.smooth_tma[ig] > 2) return false;
+        if (t.coarse_kernel[ig] < 0 || t.coarse_kernel[ig] > 2) return false;
     }
     return true;
 }
 
+// The first level of the one-CTA coarse kernel from x->tune.coarse_kernel (the first
+// level marked 2), else as chosen at creation; written to the cases where it changes.
+static int apply_tail(mgfvm_ctx *x)
+{
+    int from = -1;
+    for (int ig = 0; ig < MGFVM_MAX_LEVELS && from < 0; ++ig)
+        if (x->tune.coarse_kernel[ig] == 2) from = ig;
+    bool change = false;
+    for (int c = 0; c < x->ncases; ++c) {
+        const int t = x->opt.tangent ? 0 : from >= 0 ? std::min(from, x->cfg[c].ngrid) : x->tail0[c];
+        change |= x->hc[c].tail != t;
+    }
+    if (!change) return MGFVM_OK;
+    RC(pull(x));
+    for (int c = 0; c < x->ncases; ++c)
+        x->hc[c].tail = x->opt.tangent ? 0 : from >= 0 ? std::min(from, x->cfg[c].ngrid) : x->tail0[c];
+    return push(x);
+}
+
 // Drop the captured graph and rebuild the V-cycle's launch list from x->tune.
-static void rebuild_schedule(mgfvm_ctx *x)
+static int rebuild_schedule(mgfvm_ctx *x)
 {
     if (x->gexec) cudaGraphExecDestroy(x->gexec);
     if (x->graph) cudaGraphDestroy(x->graph);
     x->gexec = nullptr;
     x->graph = nullptr;
-    build_cycle(x);
+    RC(apply_tail(x));
+    return build_cycle(x);
 }
 
 // Milliseconds per graph-replayed V-cycle (best of two runs of n), stop rule off.
@@ -1393,8 +1416,7 @@ int mgfvm_set_tuning(mgfvm_ctx *x, const mgfvm_tuning *t)
     RC(check_ctx(x));
     if (!t || !tuning_valid(*t)) return mgfvm_fail(MGFVM_EINVAL, "tuning values outside the allowed sets");
     x->tune = *t;
-    rebuild_schedule(x);
-    return MGFVM_OK;
+    return rebuild_schedule(x);
 }
 
 int mgfvm_autotune(mgfvm_ctx *x, int cycles, mgfvm_tuning *chosen, double *ms_before, double *ms_after)
@@ -1436,6 +1458,7 @@ int mgfvm_autotune(mgfvm_ctx *x, int cycles, mgfvm_tuning *chosen, double *ms_be
                 for (auto &o : opts) knobs.push_back({0, o[0], o[1]});
             }
             if (!probe.whole_level(ig, mx, my)) knobs.push_back({3, 2, 0});
+            if (ig >= 1 && ig >= x->maxng - 3) knobs.push_back({4, 2, 0});   // one-CTA kernel from here down
             knobs.push_back({1, 1, 0});
             knobs.push_back({1, 3, 0});
             if (ig + 1 < x->maxng) {
@@ -1448,6 +1471,7 @@ int mgfvm_autotune(mgfvm_ctx *x, int cycles, mgfvm_tuning *chosen, double *ms_be
                 if (k[0] == 1) cand.asm_slices[ig] = k[1];
                 if (k[0] == 2) cand.restrict_slices[ig] = k[1];
                 if (k[0] == 3) cand.smooth_tma[ig] = k[1];
+                if (k[0] == 4) cand.coarse_kernel[ig] = k[1];
                 if (memcmp(&cand, &keep, sizeof cand) == 0) continue;
                 x->tune = cand;
                 rebuild_schedule(x);
