@@ -167,6 +167,10 @@ typedef struct mgfvm_tuning {
                                               the one-CTA-per-case coarse kernel (the
                                               first level marked 2 counts); 0 or 1
                                               everywhere: mgfvm_options.tail_level      */
+    int prol_fused[MGFVM_MAX_LEVELS];      /* prolongation into this level forms the coarse
+                                              corrections in the gather from the
+                                              restriction's saved R(x_f) (no separate
+                                              correction kernel): 0 or 2 yes, 1 no      */
 } mgfvm_tuning;
 
 typedef struct mgfvm_ctx mgfvm_ctx;

@@ -458,11 +458,16 @@ __device__ __forceinline__ void cell_gs(const LevelDev &L, int e, int phi, int q
 template <class IO>
 __device__ __forceinline__ void cell_restv_io(const IO &F, const IO &K, int ic, int jc)
 {
+    using T = typename IO::T;
     const int nxf = F.L.npx, qc = jc * K.L.npx + ic, q = 2 * jc * nxf + 2 * ic, qw = q - 1, qs = q - nxf;
-    K.st(S_U, qc, (F.ld(S_U, q) * F.g(S_AREAX, q) + F.ld(S_U, qs) * F.g(S_AREAX, qs)) / (K.g(S_AREAX, qc) + 1.0e-30));
-    K.st(S_V, qc, (F.ld(S_V, q) * F.g(S_AREAY, q) + F.ld(S_V, qw) * F.g(S_AREAY, qw)) / (K.g(S_AREAY, qc) + 1.0e-30));
-    K.st(S_P, qc, 0.25 * (F.ld(S_P, q) + F.ld(S_P, qw) + F.ld(S_P, qs) + F.ld(S_P, qs - 1)));
-    K.st(S_SC, qc, 0.25 * (F.ld(S_SC, q) + F.ld(S_SC, qw) + F.ld(S_SC, qs) + F.ld(S_SC, qs - 1)));
+    const T u = (F.ld(S_U, q) * F.g(S_AREAX, q) + F.ld(S_U, qs) * F.g(S_AREAX, qs)) / (K.g(S_AREAX, qc) + 1.0e-30);
+    const T v = (F.ld(S_V, q) * F.g(S_AREAY, q) + F.ld(S_V, qw) * F.g(S_AREAY, qw)) / (K.g(S_AREAY, qc) + 1.0e-30);
+    const T p = 0.25 * (F.ld(S_P, q) + F.ld(S_P, qw) + F.ld(S_P, qs) + F.ld(S_P, qs - 1));
+    const T sc = 0.25 * (F.ld(S_SC, q) + F.ld(S_SC, qw) + F.ld(S_SC, qs) + F.ld(S_SC, qs - 1));
+    K.st(S_U, qc, u); K.st(S_V, qc, v); K.st(S_P, qc, p); K.st(S_SC, qc, sc);
+    // the fine level does not change until the prolongation back into it, so these are
+    // the R(x_f) the corrections subtract (prol_corr's r, same operations)
+    K.st(S_RU, qc, u); K.st(S_RV, qc, v); K.st(S_RP, qc, p); K.st(S_RSC, qc, sc);
 }
 __device__ __forceinline__ void cell_restv(const LevelDev &F, const LevelDev &K, int ic, int jc)
 {
@@ -610,36 +615,83 @@ __device__ __forceinline__ void cell_prol_corr(const LevelDev &F, const LevelDev
     cell_prol_corr_io(Prim{F}, Prim{K}, ic, jc);
 }
 
+// The coarse corrections a prolongation gathers, either read from the arrays
+// cell_prol_corr filled (FUSED = false) or formed where they are needed from the coarse
+// state and the R(x_f) restv saved (FUSED = true): the same subtraction on the same
+// operands (and the same zeroing of p's correction under solid cells), so the same
+// bits.  Outside a correction's domain both read the array (nothing writes it there).
+template <class IO, bool FUSED>
+struct ProlCorr {
+    const IO &F, &K;
+    using T = typename IO::T;
+    __device__ __forceinline__ T u(int ic, int jc) const
+    {
+        const int nxc = K.L.npx, qc = jc * nxc + ic;
+        if (FUSED && ic >= 1 && ic <= nxc - 3 && jc >= 1 && jc <= K.L.npy - 2) return K.ld(S_U, qc) - K.ld(S_RU, qc);
+        return K.ld(S_CU, qc);
+    }
+    __device__ __forceinline__ T v(int ic, int jc) const
+    {
+        const int nxc = K.L.npx, qc = jc * nxc + ic;
+        if (FUSED && ic >= 1 && ic <= nxc - 2 && jc >= 1 && jc <= K.L.npy - 3) return K.ld(S_V, qc) - K.ld(S_RV, qc);
+        return K.ld(S_CV, qc);
+    }
+    __device__ __forceinline__ T p(int ic, int jc) const
+    {
+        const int nxc = K.L.npx, qc = jc * nxc + ic;
+        if (FUSED && ic >= 1 && ic <= nxc - 2 && jc >= 1 && jc <= K.L.npy - 2) {
+            T c = K.ld(S_P, qc) - K.ld(S_RP, qc);
+            if (F.g(S_SPU, 2 * jc * F.L.npx + 2 * ic) > 1.0e10) c = 0.0;
+            return c;
+        }
+        return K.ld(S_CP, qc);
+    }
+    __device__ __forceinline__ T sc(int ic, int jc) const
+    {
+        const int nxc = K.L.npx, qc = jc * nxc + ic;
+        if (FUSED && ic >= 1 && ic <= nxc - 2 && jc >= 1 && jc <= K.L.npy - 2) return K.ld(S_SC, qc) - K.ld(S_RSC, qc);
+        return K.ld(S_C, qc);
+    }
+};
+
 // Fine-cell gather of the reference's scatter-add prolongation (same additions in
-// the same order as its sequential loops): fine interior cell (i, j).
-template <class IO>
+// the same order as its sequential loops): fine interior cell (i, j).  FUSED: the
+// corrections are formed here (ProlCorr), and the fine cell (2 ic, 2 jc) also writes
+// coarse cell (ic, jc)'s corrections to the arrays, as cell_prol_corr would have.
+template <class IO, bool FUSED = false>
 __device__ __forceinline__ void cell_prol_apply_io(const IO &F, const IO &K, int i, int j)
 {
     using T = typename IO::T;
     const int nxf = F.L.npx, nyf = F.L.npy, nxc = K.L.npx, nyc = K.L.npy, q = j * nxf + i;
     const double f1 = 3. / 4., f2 = 1. / 4.;
+    const ProlCorr<IO, FUSED> cr{F, K};
+    if (FUSED && ((i | j) & 1) == 0) {
+        const int ic = i / 2, jc = j / 2, qc = jc * nxc + ic;
+        if (ic <= nxc - 3) K.st(S_CU, qc, cr.u(ic, jc));
+        if (jc <= nyc - 3) K.st(S_CV, qc, cr.v(ic, jc));
+        K.st(S_CP, qc, cr.p(ic, jc));
+        K.st(S_C, qc, cr.sc(ic, jc));
+    }
     // u faces, i in [1, nxf-3]: prolu :1782-1814
     if (i <= nxf - 3) {
         const bool up = (j & 1) == 0;                  // even row: corr1 of jc = j/2
         const int jc = up ? j / 2 : (j + 1) / 2;       // odd row: corr2 of jc = (j+1)/2
-        const int dj = up ? nxc : -nxc;
+        const int jn = up ? jc + 1 : jc - 1;           // the other row of the pair
         T u = F.ld(S_U, q);
         if ((i & 1) == 0) {
-            const int ic = i / 2, qc = jc * nxc + ic;
-            T corr = f1 * K.ld(S_CU, qc) + f2 * K.ld(S_CU, qc + dj);
+            const int ic = i / 2;
+            T corr = f1 * cr.u(ic, jc) + f2 * cr.u(ic, jn);
             if (F.g(S_SPU, 2 * jc * nxf + 2 * ic) > 1.0e10) corr = 0.0;
             u = u + corr;
         } else {
             const int ia = (i - 1) / 2, ib = (i + 1) / 2;
             if (ia >= 1) {
-                const int qc = jc * nxc + ia;
-                T corr = f1 * K.ld(S_CU, qc) + f2 * K.ld(S_CU, qc + dj);
+                T corr = f1 * cr.u(ia, jc) + f2 * cr.u(ia, jn);
                 if (F.g(S_SPU, 2 * jc * nxf + 2 * ia) > 1.0e10) corr = 0.0;
                 u = u + 0.5 * corr;
             }
             if (ib <= nxc - 3) {
-                const int qc = jc * nxc + ib;
-                T corr = f1 * K.ld(S_CU, qc) + f2 * K.ld(S_CU, qc + dj);
+                T corr = f1 * cr.u(ib, jc) + f2 * cr.u(ib, jn);
                 if (F.g(S_SPU, 2 * jc * nxf + 2 * ib) > 1.0e10) corr = 0.0;
                 u = u + 0.5 * corr;
             }
@@ -650,24 +702,22 @@ __device__ __forceinline__ void cell_prol_apply_io(const IO &F, const IO &K, int
     if (j <= nyf - 3) {
         const bool right = (i & 1) == 0;               // even column: corr1 of ic = i/2
         const int ic = right ? i / 2 : (i + 1) / 2;
-        const int di = right ? 1 : -1;
+        const int in = right ? ic + 1 : ic - 1;        // the other column of the pair
         T v = F.ld(S_V, q);
         if ((j & 1) == 0) {
-            const int jc = j / 2, qc = jc * nxc + ic;
-            T corr = f1 * K.ld(S_CV, qc) + f2 * K.ld(S_CV, qc + di);
+            const int jc = j / 2;
+            T corr = f1 * cr.v(ic, jc) + f2 * cr.v(in, jc);
             if (F.g(S_SPV, 2 * jc * nxf + 2 * ic) > 1.0e10) corr = 0.0;
             v = v + corr;
         } else {
             const int ja = (j - 1) / 2, jb = (j + 1) / 2;
             if (ja >= 1) {
-                const int qc = ja * nxc + ic;
-                T corr = f1 * K.ld(S_CV, qc) + f2 * K.ld(S_CV, qc + di);
+                T corr = f1 * cr.v(ic, ja) + f2 * cr.v(in, ja);
                 if (F.g(S_SPV, 2 * ja * nxf + 2 * ic) > 1.0e10) corr = 0.0;
                 v = v + 0.5 * corr;
             }
             if (jb <= nyc - 3) {
-                const int qc = jb * nxc + ic;
-                T corr = f1 * K.ld(S_CV, qc) + f2 * K.ld(S_CV, qc + di);
+                T corr = f1 * cr.v(ic, jb) + f2 * cr.v(in, jb);
                 if (F.g(S_SPV, 2 * jb * nxf + 2 * ic) > 1.0e10) corr = 0.0;
                 v = v + 0.5 * corr;
             }
@@ -677,18 +727,19 @@ __device__ __forceinline__ void cell_prol_apply_io(const IO &F, const IO &K, int
     // p and sc cells: prolp :1933-1958, prolsc :1999-2025
     {
         const double g1 = 9. / 16., g2 = 3. / 16., g3 = 3. / 16., g4 = 1. / 16.;
-        const int ic = (i + 1) / 2, jc = (j + 1) / 2, qc = jc * nxc + ic;
-        const int di = (i & 1) == 0 ? 1 : -1;
-        const int dj = (j & 1) == 0 ? nxc : -nxc;
-        F.st(S_P, q, F.ld(S_P, q) + (g1 * K.ld(S_CP, qc) + g2 * K.ld(S_CP, qc + di) + g3 * K.ld(S_CP, qc + dj)
-                                     + g4 * K.ld(S_CP, qc + di + dj)));
-        F.st(S_SC, q, F.ld(S_SC, q) + (g1 * K.ld(S_C, qc) + g2 * K.ld(S_C, qc + di) + g3 * K.ld(S_C, qc + dj)
-                                       + g4 * K.ld(S_C, qc + di + dj)));
+        const int ic = (i + 1) / 2, jc = (j + 1) / 2;
+        const int in = (i & 1) == 0 ? ic + 1 : ic - 1;
+        const int jn = (j & 1) == 0 ? jc + 1 : jc - 1;
+        F.st(S_P, q, F.ld(S_P, q) + (g1 * cr.p(ic, jc) + g2 * cr.p(in, jc) + g3 * cr.p(ic, jn)
+                                     + g4 * cr.p(in, jn)));
+        F.st(S_SC, q, F.ld(S_SC, q) + (g1 * cr.sc(ic, jc) + g2 * cr.sc(in, jc) + g3 * cr.sc(ic, jn)
+                                       + g4 * cr.sc(in, jn)));
     }
 }
+template <bool FUSED = false>
 __device__ __forceinline__ void cell_prol_apply(const LevelDev &F, const LevelDev &K, int i, int j)
 {
-    cell_prol_apply_io(Prim{F}, Prim{K}, i, j);
+    cell_prol_apply_io<Prim, FUSED>(Prim{F}, Prim{K}, i, j);
 }
 
 // ---------------------------------------------------------- boundary lines

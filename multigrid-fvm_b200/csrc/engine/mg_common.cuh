@@ -28,6 +28,7 @@ enum Slot {
     S_CX, S_CY, S_AREAX, S_AREAY, S_RS,
     S_C,                     // scalar prolongation correction (the reference's c after prolsc)
     S_CU, S_CV, S_CP,        // u, v, p prolongation corrections
+    S_RU, S_RV, S_RP, S_RSC, // R(x_f) of u, v, p, sc as restv computed them (the gather's corrections)
     S_TMP0, S_TMP1, S_TMP2,  // Jacobi ping-pong buffers (u or p', v, sc)
     S_CO,                    // 4 equations x {aw, ae, as, an, ap, su}
     NSLOTS_LEVEL = S_CO + 4 * NCOEF,

@@ -413,10 +413,13 @@ struct Builder {
         L.grid.z = z;
     }
     // :230-233
+    // In a V-cycle the gather may form the coarse corrections from the R(x_f) that the
+    // restriction saved (the fine level has not changed since), unless tuned off.
     void prolong(int ig, int mode)
     {
-        add(K_PROL_CORR, ig, mode, cells(ig + 1));
-        add(K_PROL_APPLY, ig, mode, cells(ig));
+        const bool fused = mode == M_PROLONG && x->tune.prol_fused[ig] != 1;
+        if (!fused) add(K_PROL_CORR, ig, mode, cells(ig + 1));
+        add(K_PROL_APPLY, ig, mode, cells(ig), fused ? 1 : 0);
     }
     void cycle()
     {
@@ -1349,6 +1352,7 @@ static bool tuning_valid(const mgfvm_tuning &t)
         if (t.pp_level[ig] < 0 || t.pp_level[ig] > 2) return false;
         if (t.smooth_tma[ig] < 0 || t.smooth_tma[ig] > 2) return false;
         if (t.coarse_kernel[ig] < 0 || t.coarse_kernel[ig] > 2) return false;
+        if (t.prol_fused[ig] < 0 || t.prol_fused[ig] > 2) return false;
     }
     return true;
 }
@@ -1459,6 +1463,7 @@ int mgfvm_autotune(mgfvm_ctx *x, int cycles, mgfvm_tuning *chosen, double *ms_be
             }
             if (!probe.whole_level(ig, mx, my)) knobs.push_back({3, 2, 0});
             if (ig >= 1 && ig >= x->maxng - 3) knobs.push_back({4, 2, 0});   // one-CTA kernel from here down
+            if (ig + 1 < x->maxng) knobs.push_back({5, 1, 0});                 // separate correction kernel
             knobs.push_back({1, 1, 0});
             knobs.push_back({1, 3, 0});
             if (ig + 1 < x->maxng) {
@@ -1472,6 +1477,7 @@ int mgfvm_autotune(mgfvm_ctx *x, int cycles, mgfvm_tuning *chosen, double *ms_be
                 if (k[0] == 2) cand.restrict_slices[ig] = k[1];
                 if (k[0] == 3) cand.smooth_tma[ig] = k[1];
                 if (k[0] == 4) cand.coarse_kernel[ig] = k[1];
+                if (k[0] == 5) cand.prol_fused[ig] = k[1];
                 if (memcmp(&cand, &keep, sizeof cand) == 0) continue;
                 x->tune = cand;
                 rebuild_schedule(x);

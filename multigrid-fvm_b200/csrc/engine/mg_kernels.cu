@@ -944,12 +944,13 @@ __global__ void __launch_bounds__(BLOCK) k_prol_corr(const CaseDev *__restrict__
     if (cell_at(dom_interior(K), t, i, j)) cell_prol_corr(L, K, i, j);
 }
 
+template <bool FUSED>
 __global__ void __launch_bounds__(BLOCK) k_prol_apply(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode)
 {
     CASE_PROLOGUE(mode);
     const LevelDev &K = C.lv[ig + 1];
     int i, j;
-    if (cell_at(dom_interior(L), t, i, j)) cell_prol_apply(L, K, i, j);
+    if (cell_at(dom_interior(L), t, i, j)) cell_prol_apply<FUSED>(L, K, i, j);
 }
 
 // End of a V-cycle on the level-0 interior: relative change of u, v, sc and of p
@@ -1061,6 +1062,7 @@ __global__ void __launch_bounds__(BLOCK) k_endcycle(const CaseDev *__restrict__ 
 
 // prolongation into level 0 followed by the end of the cycle: every thread reads
 // back only the level-0 cell it just wrote.
+template <bool FUSED>
 __global__ void __launch_bounds__(BLOCK) k_prol_apply_end(const CaseDev *__restrict__ cs, CaseState *st, int mode)
 {
     const int ig = 0;
@@ -1069,7 +1071,7 @@ __global__ void __launch_bounds__(BLOCK) k_prol_apply_end(const CaseDev *__restr
     const int n = d.wi * d.wj, nb = (n + blockDim.x - 1) / blockDim.x;
     if ((int)blockIdx.x >= nb) return;
     int i, j;
-    if (cell_at(d, t, i, j)) cell_prol_apply(L, C.lv[1], i, j);
+    if (cell_at(d, t, i, j)) cell_prol_apply<FUSED>(L, C.lv[1], i, j);
     end_of_cycle(C, ST, t, nb);
 }
 
@@ -1438,14 +1440,20 @@ cudaError_t launch_one(const Launch &X, const CaseDev *dc, CaseState *ds, const 
     case K_RESTV_FLUXES: k_restv_fluxes<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode); break;
     case K_RESTRICT: k_restrict<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, (unsigned)X.a0); break;
     case K_PROL_CORR: k_prol_corr<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode); break;
-    case K_PROL_APPLY: k_prol_apply<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode); break;
+    case K_PROL_APPLY:
+        if (X.a0) k_prol_apply<true><<<g, b, 0, st>>>(dc, ds, X.ig, X.mode);
+        else k_prol_apply<false><<<g, b, 0, st>>>(dc, ds, X.ig, X.mode);
+        break;
     case K_TAIL: k_tail<<<g, b, X.smem, st>>>(dc, ds, S, X.smem / (int)sizeof(double)); break;
     case K_TAIL_TAN:
         if (!dt) return cudaErrorInvalidValue;
         k_tail_tan<<<g, b, 0, st>>>(dc, ds, dt, S);
         break;
     case K_ENDCYCLE: k_endcycle<<<g, b, 0, st>>>(dc, ds); break;
-    case K_PROL_APPLY_END: k_prol_apply_end<<<g, b, 0, st>>>(dc, ds, X.mode); break;
+    case K_PROL_APPLY_END:
+        if (X.a0) k_prol_apply_end<true><<<g, b, 0, st>>>(dc, ds, X.mode);
+        else k_prol_apply_end<false><<<g, b, 0, st>>>(dc, ds, X.mode);
+        break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

@@ -19,7 +19,7 @@ enum KernelId {
     K_COPY,          // copy equations' buffers back: a0 = eq mask
     K_RESTV_FLUXES,  // restv + fine fluxes
     K_RESTRICT,      // restr{u,v,sc} + coarse fluxes
-    K_PROL_CORR, K_PROL_APPLY,
+    K_PROL_CORR, K_PROL_APPLY,   // prol_apply: a0 = 1 forms the corrections itself (no K_PROL_CORR before it)
     K_TAIL, K_ENDCYCLE, K_PROL_APPLY_END,
     K_SMOOTH_MIXED,  // as K_SMOOTH, FP32 correction smoothing with an FP64 residual
     K_PFIX_BOUND,    // K_PFIX then K_BOUND (a0 = bits), one CTA per case

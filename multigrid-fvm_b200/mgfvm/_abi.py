@@ -76,7 +76,7 @@ class Tuning(C.Structure):
                 ("asm_slices", C.c_int * MAX_LEVELS), ("restrict_slices", C.c_int * MAX_LEVELS),
                 ("update_pfix", C.c_int * MAX_LEVELS), ("odd_chunks", C.c_int * MAX_LEVELS),
                 ("pp_level", C.c_int * MAX_LEVELS), ("smooth_tma", C.c_int * MAX_LEVELS),
-                ("coarse_kernel", C.c_int * MAX_LEVELS)]
+                ("coarse_kernel", C.c_int * MAX_LEVELS), ("prol_fused", C.c_int * MAX_LEVELS)]
 
     def as_dict(self):
         return {k: list(getattr(self, k)) for k, _ in self._fields_}

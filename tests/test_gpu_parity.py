@@ -185,7 +185,7 @@ TUNINGS = [
      "restrict_slices": [1, 3, 1]},
     {"smooth_units": [16, 12, 20], "smooth_threads": [1024, 512, 1024]},
     {"smooth_units": [3, 7, 5], "smooth_threads": [256, 256, 256]},
-    {"update_pfix": [1, 1, 1], "odd_chunks": [1, 1, 1], "pp_level": [1, 1, 1]},
+    {"update_pfix": [1, 1, 1], "odd_chunks": [1, 1, 1], "pp_level": [1, 1, 1], "prol_fused": [1, 1, 1]},
     {"smooth_units": [5, 3, 7], "odd_chunks": [2, 2, 2]},
     {"smooth_tma": [2, 2, 2]},
     {"smooth_tma": [2, 2, 2], "smooth_units": [3, 5, 7], "smooth_threads": [512, 256, 1024]},
@@ -226,7 +226,7 @@ def test_autotune_keeps_state(oracle_built):
     before, after, chosen = s.autotune(2)
     assert before > 0 and 0 < after <= before
     assert set(chosen) == {"smooth_units", "smooth_threads", "asm_slices", "restrict_slices", "update_pfix", "odd_chunks", "pp_level",
-                           "smooth_tma", "coarse_kernel"}
+                           "smooth_tma", "coarse_kernel", "prol_fused"}
     _compare(s, o, STATE, what="after autotune")
     s.cycle(3)
     o.cycle(3)
