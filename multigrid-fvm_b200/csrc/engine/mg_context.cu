@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdint>
 #include <map>
+#include <mutex>
 #include <tuple>
 #include <cstdio>
 #include <cstdlib>
@@ -88,6 +89,7 @@ struct mgfvm_ctx {
     std::vector<SmoothMap> hmaps;
     SmoothMap *dmaps = nullptr;
     std::vector<int> tail0;                   // per case: first one-CTA-kernel level chosen at creation
+    std::vector<void *> pooled;               // buffers taken from the device's memory pool
 };
 
 static inline int npx_of(const mgfvm_config &c, int ig) { return c.nfx / (1 << ig) + 2; }
@@ -574,6 +576,75 @@ int push(mgfvm_ctx *x)
     return MGFVM_OK;
 }
 
+// A context's device buffers (state pool, derivative storage, histories, case tables,
+// the autotuner's backup) come from one stream-ordered memory pool per device that
+// keeps up to KEEP_BYTES reserved after they are released, so programs that create and
+// release contexts in a loop reuse that memory instead of mapping and unmapping it, and
+// releasing a context calls no cudaFree (which waits for the whole device).  Allocation
+// waits for the context stream, so the memory is usable from any stream when it
+// returns.
+static const unsigned long long KEEP_BYTES = 4ull << 30;
+static cudaMemPool_t device_pool(int device)
+{
+    static std::mutex mu;
+    static std::map<int, cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = pools.find(device);
+    if (it != pools.end()) return it->second;
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t mp = nullptr;
+    if (cudaMemPoolCreate(&mp, &props) != cudaSuccess) {
+        cudaGetLastError();
+        mp = nullptr;
+    } else {
+        unsigned long long keep = KEEP_BYTES;
+        cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    pools[device] = mp;
+    return mp;
+}
+
+static cudaError_t ctx_malloc(mgfvm_ctx *x, void **p, size_t bytes)
+{
+    cudaMemPool_t mp = device_pool(x->device);
+    if (mp) {
+        cudaError_t e = cudaMallocFromPoolAsync(p, bytes, mp, x->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(x->stream);
+        if (e == cudaSuccess && ((uintptr_t)*p & 255) == 0) {
+            x->pooled.push_back(*p);
+            return cudaSuccess;
+        }
+        if (e == cudaSuccess) {          // not 256-byte aligned: take the plain allocator
+            cudaFreeAsync(*p, x->stream);
+            cudaStreamSynchronize(x->stream);
+        } else if (e == cudaErrorMemoryAllocation) {
+            *p = nullptr;
+            return e;
+        }
+        cudaGetLastError();
+    }
+    return cudaMalloc(p, bytes);
+}
+
+static void ctx_free(mgfvm_ctx *x, void *p)
+{
+    if (!p) return;
+    auto it = std::find(x->pooled.begin(), x->pooled.end(), p);
+    if (it == x->pooled.end()) {
+        cudaFree(p);
+        return;
+    }
+    x->pooled.erase(it);
+    // returned to the pool in stream order (the callers have drained the stream)
+    if (!x->stream || cudaFreeAsync(p, x->stream) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(p);
+    }
+}
+
 int ensure_hist(mgfvm_ctx *x, int need)
 {
     if (need <= x->hist_cap) return MGFVM_OK;
@@ -581,12 +652,12 @@ int ensure_hist(mgfvm_ctx *x, int need)
     while (cap < need) cap *= 2;
     RC(pull(x));
     double *h = nullptr;
-    CK(cudaMalloc(&h, sizeof(double) * 2 * (size_t)cap * x->ncases));
+    CK(ctx_malloc(x, (void **)&h, sizeof(double) * 2 * (size_t)cap * x->ncases));
     CK(cudaMemset(h, 0, sizeof(double) * 2 * (size_t)cap * x->ncases));
     if (x->hist && x->hist_cap > 0)
         CK(cudaMemcpy2D(h, sizeof(double) * cap, x->hist, sizeof(double) * x->hist_cap,
                         sizeof(double) * x->hist_cap, 2 * (size_t)x->ncases, cudaMemcpyDeviceToDevice));
-    if (x->hist) cudaFree(x->hist);
+    if (x->hist) ctx_free(x, x->hist);
     x->hist = h;
     x->hist_cap = cap;
     for (int c = 0; c < x->ncases; ++c) {
@@ -660,7 +731,7 @@ int alloc_tangent(mgfvm_ctx *x)
         x->tcase_bytes[c] = align_up(off, 256) - x->tcase_off[c];
     }
     const size_t bytes = align_up(off, 256);
-    cudaError_t me = cudaMalloc(&x->tpool, bytes);
+    cudaError_t me = ctx_malloc(x, (void **)&x->tpool, bytes);
     if (me != cudaSuccess)
         return mgfvm_fail(me == cudaErrorMemoryAllocation ? MGFVM_ENOMEM : MGFVM_ECUDA,
                           "derivative storage of %zu bytes: %s", bytes, cudaGetErrorString(me));
@@ -676,7 +747,7 @@ int alloc_tangent(mgfvm_ctx *x)
     }
     x->dir_kind.assign(x->ncases, MGFVM_DIR_NONE);
     x->dir_index.assign(x->ncases, 0);
-    CK(cudaMalloc(&x->dt, sizeof(CaseTan) * x->ncases));
+    CK(ctx_malloc(x, (void **)&x->dt, sizeof(CaseTan) * x->ncases));
     CK(cudaMemcpy(x->dt, x->ht.data(), sizeof(CaseTan) * x->ncases, cudaMemcpyHostToDevice));
     x->h2d += (long long)sizeof(CaseTan) * x->ncases;
     return MGFVM_OK;
@@ -725,7 +796,7 @@ int build_cycle(mgfvm_ctx *x)
     x->hmaps.clear();
     if (x->dmaps) {
         cudaStreamSynchronize(x->stream);
-        cudaFree(x->dmaps);
+        ctx_free(x, x->dmaps);
         x->dmaps = nullptr;
     }
     {
@@ -733,12 +804,12 @@ int build_cycle(mgfvm_ctx *x)
         b.cycle();
     }
     if (x->hmaps.empty()) return MGFVM_OK;
-    cudaError_t e = cudaMalloc(&x->dmaps, sizeof(SmoothMap) * x->hmaps.size());
+    cudaError_t e = ctx_malloc(x, (void **)&x->dmaps, sizeof(SmoothMap) * x->hmaps.size());
     if (e == cudaSuccess)
         e = cudaMemcpy(x->dmaps, x->hmaps.data(), sizeof(SmoothMap) * x->hmaps.size(), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
         cudaGetLastError();
-        if (x->dmaps) cudaFree(x->dmaps);
+        if (x->dmaps) ctx_free(x, x->dmaps);
         x->dmaps = nullptr;
         x->cyc.clear();
         x->hmaps.clear();
@@ -783,9 +854,9 @@ int upload_profiles(mgfvm_ctx *x)
 {
     size_t tot = 0;
     for (auto &p : x->profile) tot += p.size();
-    if (x->dprofile) { cudaFree(x->dprofile); x->dprofile = nullptr; }
+    if (x->dprofile) { ctx_free(x, x->dprofile); x->dprofile = nullptr; }
     if (tot) {
-        CK(cudaMalloc(&x->dprofile, sizeof(double) * tot));
+        CK(ctx_malloc(x, (void **)&x->dprofile, sizeof(double) * tot));
     }
     size_t off = 0;
     for (int c = 0; c < x->ncases; ++c) {
@@ -808,16 +879,16 @@ void destroy_all(mgfvm_ctx *x)
     if (x->stream) cudaStreamSynchronize(x->stream);
     if (x->gexec) cudaGraphExecDestroy(x->gexec);
     if (x->graph) cudaGraphDestroy(x->graph);
-    if (x->pool) cudaFree(x->pool);
-    if (x->tpool) cudaFree(x->tpool);
-    if (x->dmaps) cudaFree(x->dmaps);
-    if (x->dt) cudaFree(x->dt);
-    if (x->hist) cudaFree(x->hist);
-    if (x->dprofile) cudaFree(x->dprofile);
-    if (x->dobs) cudaFree(x->dobs);
-    if (x->dc) cudaFree(x->dc);
-    if (x->ds) cudaFree(x->ds);
-    if (x->dinit) cudaFree(x->dinit);
+    if (x->pool) ctx_free(x, x->pool);
+    if (x->tpool) ctx_free(x, x->tpool);
+    if (x->dmaps) ctx_free(x, x->dmaps);
+    if (x->dt) ctx_free(x, x->dt);
+    if (x->hist) ctx_free(x, x->hist);
+    if (x->dprofile) ctx_free(x, x->dprofile);
+    if (x->dobs) ctx_free(x, x->dobs);
+    if (x->dc) ctx_free(x, x->dc);
+    if (x->ds) ctx_free(x, x->ds);
+    if (x->dinit) ctx_free(x, x->dinit);
     if (x->hflags) cudaFreeHost(x->hflags);
     if (x->e0) cudaEventDestroy(x->e0);
     if (x->e1) cudaEventDestroy(x->e1);
@@ -924,7 +995,7 @@ int create_impl(const mgfvm_config *cases, int ncases, const mgfvm_options *opt_
     }
     const size_t pool_bytes = align_up(off, 256);
     x->pool_bytes = pool_bytes;
-    cudaError_t me = cudaMalloc(&x->pool, pool_bytes);
+    cudaError_t me = ctx_malloc(x, (void **)&x->pool, pool_bytes);
     if (me != cudaSuccess)
         return mgfvm_fail(me == cudaErrorMemoryAllocation ? MGFVM_ENOMEM : MGFVM_ECUDA,
                           "device pool of %zu bytes: %s", pool_bytes, cudaGetErrorString(me));
@@ -1003,7 +1074,7 @@ int create_impl(const mgfvm_config *cases, int ncases, const mgfvm_options *opt_
     // init parameters
     size_t nobs_tot = 0;
     for (int c = 0; c < ncases; ++c) nobs_tot += x->obs[c].size();
-    if (nobs_tot) CK(cudaMalloc(&x->dobs, sizeof(int) * nobs_tot));
+    if (nobs_tot) CK(ctx_malloc(x, (void **)&x->dobs, sizeof(int) * nobs_tot));
     x->hinit.assign(ncases, InitDev{});
     size_t ooff = 0;
     for (int c = 0; c < ncases; ++c) {
@@ -1030,9 +1101,9 @@ int create_impl(const mgfvm_config *cases, int ncases, const mgfvm_options *opt_
             P.out_val[k][0] = g.uoutlt[k]; P.out_val[k][1] = g.voutlt[k]; P.out_val[k][2] = g.scoutlt[k];
         }
     }
-    CK(cudaMalloc(&x->dc, sizeof(CaseDev) * ncases));
-    CK(cudaMalloc(&x->ds, sizeof(CaseState) * ncases));
-    CK(cudaMalloc(&x->dinit, sizeof(InitDev) * ncases));
+    CK(ctx_malloc(x, (void **)&x->dc, sizeof(CaseDev) * ncases));
+    CK(ctx_malloc(x, (void **)&x->ds, sizeof(CaseState) * ncases));
+    CK(ctx_malloc(x, (void **)&x->dinit, sizeof(InitDev) * ncases));
     RC(upload_profiles(x));
     // histories
     x->hist_cap = 0;
@@ -1431,7 +1502,7 @@ int mgfvm_autotune(mgfvm_ctx *x, int cycles, mgfvm_tuning *chosen, double *ms_be
     RC(pull(x));
     const std::vector<CaseState> saved = x->hs;
     char *backup = nullptr;
-    cudaError_t me = cudaMalloc(&backup, x->pool_bytes);
+    cudaError_t me = ctx_malloc(x, (void **)&backup, x->pool_bytes);
     if (me != cudaSuccess)
         return mgfvm_fail(me == cudaErrorMemoryAllocation ? MGFVM_ENOMEM : MGFVM_ECUDA,
                           "autotune state backup of %zu bytes: %s", x->pool_bytes, cudaGetErrorString(me));
@@ -1494,7 +1565,7 @@ int mgfvm_autotune(mgfvm_ctx *x, int cycles, mgfvm_tuning *chosen, double *ms_be
     // restore the batch exactly as it was
     cudaError_t e = cudaMemcpyAsync(x->pool, backup, x->pool_bytes, cudaMemcpyDeviceToDevice, x->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(x->stream);
-    cudaFree(backup);
+    ctx_free(x, backup);
     x->hs = saved;
     const int rp = push(x);
     if (rc != MGFVM_OK) return rc;
