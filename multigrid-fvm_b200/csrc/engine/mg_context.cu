@@ -67,7 +67,9 @@ struct mgfvm_ctx {
     int hist_cap = 0;
     double *dprofile = nullptr;
     int *dobs = nullptr;
-    int *hflags = nullptr;                    // pinned readback of the per-case done flags
+    int *hflags = nullptr;                    // pinned readback of the per-case done flags, two sets
+    size_t hflags_bytes = 0;
+    cudaEvent_t eflag[2] = {nullptr, nullptr};  // completion of each set's copy
     cudaStream_t stream = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
@@ -607,6 +609,34 @@ static cudaMemPool_t device_pool(int device)
     return mp;
 }
 
+// Small pinned host buffers (the stop-flag readbacks) are kept for reuse once a context
+// releases them: pinning and unpinning host memory costs milliseconds per context.
+static std::mutex pinned_mu;
+static std::multimap<size_t, void *> pinned_cache;
+static void *pinned_get(size_t bytes)
+{
+    {
+        std::lock_guard<std::mutex> lock(pinned_mu);
+        auto it = pinned_cache.lower_bound(bytes);
+        if (it != pinned_cache.end() && it->first == bytes) {
+            void *p = it->second;
+            pinned_cache.erase(it);
+            return p;
+        }
+    }
+    void *p = nullptr;
+    if (cudaMallocHost(&p, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return p;
+}
+static void pinned_put(void *p, size_t bytes)
+{
+    std::lock_guard<std::mutex> lock(pinned_mu);
+    pinned_cache.emplace(bytes, p);
+}
+
 static cudaError_t ctx_malloc(mgfvm_ctx *x, void **p, size_t bytes)
 {
     cudaMemPool_t mp = device_pool(x->device);
@@ -889,7 +919,9 @@ void destroy_all(mgfvm_ctx *x)
     if (x->dc) ctx_free(x, x->dc);
     if (x->ds) ctx_free(x, x->ds);
     if (x->dinit) ctx_free(x, x->dinit);
-    if (x->hflags) cudaFreeHost(x->hflags);
+    if (x->hflags) pinned_put(x->hflags, x->hflags_bytes);
+    for (cudaEvent_t &e : x->eflag)
+        if (e) cudaEventDestroy(e);
     if (x->e0) cudaEventDestroy(x->e0);
     if (x->e1) cudaEventDestroy(x->e1);
     if (x->stream) cudaStreamDestroy(x->stream);
@@ -959,7 +991,10 @@ int create_impl(const mgfvm_config *cases, int ncases, const mgfvm_options *opt_
     CK(cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking));
     CK(cudaEventCreate(&x->e0));
     CK(cudaEventCreate(&x->e1));
-    CK(cudaMallocHost(&x->hflags, sizeof(int) * ncases));
+    x->hflags_bytes = sizeof(int) * 2 * (size_t)ncases;
+    x->hflags = (int *)pinned_get(x->hflags_bytes);
+    if (!x->hflags) return mgfvm_fail(MGFVM_ENOMEM, "pinned host memory for %d flags", 2 * ncases);
+    for (cudaEvent_t &e : x->eflag) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
 
     // pool layout: pass 0 sizes, pass 1 assigns
     x->hc.assign(ncases, CaseDev{});
@@ -1210,17 +1245,30 @@ int mgfvm_solve(mgfvm_ctx *x, int max_cycles, double fp_tol, int *cycles_out)
     RC(ensure_hist(x, need));
     RC(set_controls(x, 1, fp_tol));
     CK(cudaEventRecord(x->e0, x->stream));
-    int run = 0;
-    while (run < max_cycles) {
+    // Chunks of sync_every cycles, each followed by a copy of the stop flags; the next
+    // chunk is queued before the host looks at the previous chunk's flags, so the GPU
+    // never waits for the host.  Once every case has stopped, a chunk already queued
+    // runs as cycles in which every kernel skips its stopped case.
+    int run = 0, issued = 0;
+    auto issue = [&]() -> int {
         const int n = std::min(x->opt.sync_every, max_cycles - run);
         RC(run_cycles(x, n));
         run += n;
-        CK(cudaMemcpy2DAsync(x->hflags, sizeof(int), &x->ds[0].done, sizeof(CaseState), sizeof(int), x->ncases,
+        int *f = x->hflags + (size_t)(issued & 1) * x->ncases;
+        CK(cudaMemcpy2DAsync(f, sizeof(int), &x->ds[0].done, sizeof(CaseState), sizeof(int), x->ncases,
                              cudaMemcpyDeviceToHost, x->stream));
-        CK(cudaStreamSynchronize(x->stream));
+        CK(cudaEventRecord(x->eflag[issued & 1], x->stream));
         x->d2h += (long long)sizeof(int) * x->ncases;
+        ++issued;
+        return MGFVM_OK;
+    };
+    if (run < max_cycles) RC(issue());
+    for (int k = 0; k < issued; ++k) {
+        if (run < max_cycles) RC(issue());
+        CK(cudaEventSynchronize(x->eflag[k & 1]));
+        const int *f = x->hflags + (size_t)(k & 1) * x->ncases;
         bool all = true;
-        for (int c = 0; c < x->ncases; ++c) all &= x->hflags[c] != 0;
+        for (int c = 0; c < x->ncases; ++c) all &= f[c] != 0;
         if (all) break;
     }
     CK(cudaEventRecord(x->e1, x->stream));
