@@ -135,7 +135,8 @@ typedef struct mgfvm_options {
                           -1 = chosen by the tuner, >= ngrid = no coarse kernel      */
     int use_graph;     /* replay V-cycles from a captured CUDA graph (1) or launch
                           every kernel directly (0)                                   */
-    int sync_every;    /* cycles between host reads of the stop flags in mgfvm_solve */
+    int sync_every;    /* cycles per chunk of mgfvm_solve; the host reads a chunk's stop
+                          flags while the next chunk runs (stopped cases skip it)     */
     int tangent;       /* 1: every case also carries the derivative of its state along
                           one parameter direction (mgfvm_set_direction); FP64 only, and
                           the whole V-cycle runs in the one-CTA-per-case kernel       */
