@@ -509,7 +509,9 @@ __global__ void __launch_bounds__(NT, SMOOTH_BLOCK / NT)
                        "r"(bar)
                      : "memory");
     }
-    if (!mbar_wait0(bar)) {
+    // one decision for the whole block (a thread that gave up at the limit while the
+    // others saw the copies land must not split the block at the barriers below)
+    if (!__syncthreads_and(mbar_wait0(bar))) {
         // record the stall and give the copies a second bounded wait before leaving
         if (threadIdx.x == 0) atomicOr(&st[blockIdx.y].status, (int)CASE_WAIT_TIMEOUT);
         mbar_wait0(bar);
