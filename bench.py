@@ -24,6 +24,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -44,11 +45,23 @@ def log(*a):
 
 
 # --------------------------------------------------------------- workloads
+WORKLOAD_DIRS = {"c1": [os.path.join(REPO, "workloads", n) for n in ("obstacle256_re10", "obstacle256_re100")]}
+WORKLOAD_DESC = {"c1": "obstacle flow 256x256 ngrid 5 RBGS Re {10,100} (2 cases)"}
+
+
+def workload_config(desc, n_cases, nvcycle, world):
+    """The `config` object of both arms' JSON lines."""
+    return {"workload": desc, "cases_per_gpu": n_cases,
+            "stop_rule": "reference: mass error < convergence or nvcycle V-cycles",
+            "nvcycle": nvcycle, "l2": "flushed between steps (256 MiB write)",
+            "parallelism": f"independent cases, {world} rank(s)"}
+
+
 def workload(name):
     """(cases, description, per-case inlet u profiles or None)."""
     from mgfvm import configs
-    if name == "c1":
-        return configs.c1_pair(seed=1), "obstacle flow 256x256 ngrid 5 RBGS Re {10,100} (2 cases)", None
+    if name == "c1":   # the cases of WORKLOAD_DIRS["c1"] (tests/test_workloads.py)
+        return configs.c1_pair(seed=1), WORKLOAD_DESC["c1"], None
     if name == "c0":
         return [configs.c0(1)], "channel 64x64 ngrid 3 Jacobi Re 100", None
     if name == "c2":
@@ -214,7 +227,8 @@ def mixed_solve(cases, device, ref_solver, tune, profiles=None):
     """One solve of the workload with MGFVM_PREC_MIXED (FP32 correction smoothing
     against FP64 residuals), timed like a bench step, and the relative L2 distance of
     its final fields to the FP64 solve's (`ref_solver` holds the FP64 result; p
-    compared mean-free over the interior, its level being arbitrary)."""
+    compared mean-free over the interior, its level being arbitrary).  Also returns
+    the mixed solve's level-0 fields (for the comparison with the CPU oracle)."""
     import torch
     from mgfvm import Solver
     with Solver(cases, device=device, precision="mixed", sync_every=64) as s:
@@ -228,19 +242,15 @@ def mixed_solve(cases, device, ref_solver, tune, profiles=None):
         s.solve(max(c.nvcycle for c in cases), FP_TOL, allow_nonfinite=True)
         ms = s.last_elapsed_ms
         bad = set(s.diverged()) | set(ref_solver.diverged())
+        fields = [{f: s.field(k, 0, f) for f in ("u", "v", "p", "sc")} for k in range(len(cases))]
         err = 0.0
         for k in range(len(cases)):
             if k in bad:
                 continue
-            for f in ("u", "v", "sc"):
-                a, b = s.field(k, 0, f), ref_solver.field(k, 0, f)
-                err = max(err, float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)))
-            a, b = s.field(k, 0, "p")[1:-1, 1:-1], ref_solver.field(k, 0, "p")[1:-1, 1:-1]
-            a, b = a - a.mean(), b - b.mean()
-            err = max(err, float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)))
+            err = max(err, field_errors(fields[k], {f: ref_solver.field(k, 0, f) for f in ("u", "v", "p", "sc")}))
     return {"value": round((len(cases) - len(bad)) / (ms / 1e3), 4), "unit": "solves/s", "ms_per_step": round(ms, 3),
             "rel_l2_vs_fp64_solve": err, "diverged": len(bad),
-            "form": "smoothers iterate an FP32 correction against FP64 residuals; the rest FP64"}
+            "form": "smoothers iterate an FP32 correction against FP64 residuals; the rest FP64"}, fields, bad
 
 
 # --------------------------------------------------------------- clocks
@@ -248,7 +258,7 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(REPO, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        self.path = os.path.join(tempfile.gettempdir(), f"mgfvm_bench_clocks_{os.getpid()}.csv")
 
     def __enter__(self):
         try:
@@ -293,24 +303,58 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------- CPU side
-def _ref_worker(args):
-    """One process: time `ncyc` V-cycles of one case with the reference build (or the
-    oracle port when the reference build is absent)."""
-    cfg_dict, ncyc, warm = args
+def _cpu_case(src):
+    """The reference build (or the oracle port where the reference build is absent) on
+    one case: `src` is a directory holding InputData + pattern.txt (read by the
+    reference itself) or a CaseConfig as a dict."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     sys.path.insert(0, os.path.join(REPO, "multigrid-fvm_b200"))
     import oracle
     from mgfvm.inputs import CaseConfig
-    cfg = CaseConfig(**cfg_dict)
     if oracle.ref_available():
-        r = oracle.RefCase(cfg)
+        if isinstance(src, str):
+            return "reference", oracle.RefCase(None, workdir=src)
+        return "reference", oracle.RefCase(CaseConfig(**src))
+    if isinstance(src, str):
+        from mgfvm import read_case
+        return "port", oracle.OracleCase(read_case(src))
+    return "port", oracle.OracleCase(CaseConfig(**src))
+
+
+def _ref_worker(args):
+    """One process: time `ncyc` V-cycles of one case on the CPU."""
+    src, ncyc, warm = args
+    kind, r = _cpu_case(src)
+    if kind == "reference":
         r.time_cycles(warm)
-        return "reference", r.time_cycles(ncyc) / ncyc
-    o = oracle.OracleCase(cfg)
-    o.cycle(warm)
+        return kind, r.time_cycles(ncyc) / ncyc
+    r.cycle(warm)
     t = time.perf_counter()
-    o.cycle(ncyc)
-    return "port", (time.perf_counter() - t) / ncyc
+    r.cycle(ncyc)
+    return kind, (time.perf_counter() - t) / ncyc
+
+
+def _ref_solve_worker(args):
+    """One process: `ncyc` V-cycles of one case on the CPU from its initial state (the
+    solve a GPU step ran); returns the level-0 u, v, p, sc and the seconds taken."""
+    src, ncyc = args
+    kind, r = _cpu_case(src)
+    t = time.perf_counter()
+    r.cycle(ncyc)
+    sec = time.perf_counter() - t
+    return kind, sec, {f: r.get(0, f) for f in ("u", "v", "p", "sc")}
+
+
+def field_errors(got, ref):
+    """Relative L2 distance of one case's level-0 fields: u, v, sc over the whole array,
+    p over the interior with its mean removed (its level is arbitrary); the max."""
+    err = 0.0
+    for f in ("u", "v", "sc"):
+        a, b = got[f], ref[f]
+        err = max(err, float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)))
+    a, b = got["p"][1:-1, 1:-1], ref["p"][1:-1, 1:-1]
+    a, b = a - a.mean(), b - b.mean()
+    return max(err, float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)))
 
 
 def cpu_sample(cases, cycles_to_converge, ncyc, procs):
@@ -318,7 +362,8 @@ def cpu_sample(cases, cycles_to_converge, ncyc, procs):
     round-robin over the workload's cases), from the mean time per V-cycle."""
     import dataclasses
     import multiprocessing as mp
-    jobs = [(dataclasses.asdict(cases[k % len(cases)]), ncyc, 2) for k in range(procs)]
+    srcs = cases if isinstance(cases[0], str) else [dataclasses.asdict(c) for c in cases]
+    jobs = [(srcs[k % len(srcs)], ncyc, 2) for k in range(procs)]
     ctx = mp.get_context("spawn")
     t0 = time.perf_counter()
     with ctx.Pool(procs) as pool:
@@ -336,7 +381,13 @@ def cpu_sample(cases, cycles_to_converge, ncyc, procs):
 def run_reference_arm(a, rank, world):
     if rank != 0:
         return
-    cases, desc, _ = workload(a.workload)
+    # the reference reads the workload's own InputData/pattern.txt directories; nothing
+    # of this package's native code is loaded
+    if a.workload in WORKLOAD_DIRS:
+        cases, nvcycle, desc = WORKLOAD_DIRS[a.workload], [2000, 2000], WORKLOAD_DESC[a.workload]
+    else:
+        cs, desc, _ = workload(a.workload)
+        cases, nvcycle = cs, [c.nvcycle for c in cs]
     ctc = CYCLES_TO_CONVERGE.get(a.workload)
     if ctc is None:
         print(json.dumps({"impl": "reference", "unavailable": f"no converged cycle counts for {a.workload}"}))
@@ -355,8 +406,8 @@ def run_reference_arm(a, rank, world):
     line = {
         "impl": "reference", "metric": "converged solves/s", "value": value, "unit": "solves/s",
         "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": desc},
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded obstacle patterns)",
+        "config": workload_config(desc, len(cases), nvcycle, world),
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": procs, "kind": kind, "sample": sample},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -474,6 +525,20 @@ def main():
     # cases on which the reference's own iteration turns NaN/Inf stop at that cycle and
     # are not counted as solves (the reference's stop test never fires on NaN)
     diverged = solver.diverged()
+    # Parity of the timed result: the CPU runs every case of the workload for the cycles
+    # its GPU solve runs, from the same initial state, in background processes (one per
+    # case) while the GPU part runs; its final fields are the oracle of the solve.
+    parity_jobs = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline and n_cases <= 8:
+        import dataclasses
+        import multiprocessing as mp
+        srcs = WORKLOAD_DIRS.get(a.workload) or [dataclasses.asdict(c) for c in cases]
+        if profiles:
+            srcs = None    # per-face inlet profiles: not expressible as reference input files
+        if srcs:
+            parity_pool = mp.get_context("spawn").Pool(n_cases)
+            parity_t0 = time.perf_counter()
+            parity_jobs = parity_pool.map_async(_ref_solve_worker, [(srcs[k], int(cyc[k])) for k in range(n_cases)])
     launches0 = solver.kernel_launches
     cycles = []
     e0 = torch.cuda.Event(enable_timing=True)
@@ -493,6 +558,9 @@ def main():
         dist.barrier()
     ms = e0.elapsed_time(e1)
     launches = solver.kernel_launches - launches0
+    # the timed solve's final level-0 fields (later measurements change the state)
+    gpu_fields = [{f: solver.field(k, 0, f) for f in ("u", "v", "p", "sc")} for k in range(n_cases)] \
+        if parity_jobs is not None else None
     if world > 1:
         t = torch.tensor([ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -551,9 +619,10 @@ def main():
             e2e["value"] = (n_cases - len(diverged)) * max(1, a.steps) * world / float(t.item())
 
     # ---- mixed precision: the same solve with FP32 correction smoothing
-    mixed = None
+    mixed = mixed_fields = None
+    mixed_bad = set()
     if world == 1:
-        mixed = mixed_solve(cases, local, solver, tuned is not None, profiles)
+        mixed, mixed_fields, mixed_bad = mixed_solve(cases, local, solver, tuned is not None, profiles)
 
     # ---- batched throughput: many obstacle-flow cases in one context
     batched = None
@@ -565,23 +634,35 @@ def main():
     if world == 1 and not a.no_gradient:
         grad = gradient_rate(local, check=not a.no_cpu_baseline)
 
-    # ---- parity spot check at full size: 3 cycles against the CPU oracle
-    l2err = None
+    # ---- parity of the timed solve against the CPU oracle's run of the same cycles
+    parity = None
+    if parity_jobs is not None:
+        res = parity_jobs.get()
+        parity_pool.close()
+        parity_pool.join()
+        wall = time.perf_counter() - parity_t0
+        per_case, per_case_mixed = [], []
+        for k, (kind, sec, ref) in enumerate(res):
+            per_case.append(None if k in diverged else field_errors(gpu_fields[k], ref))
+            if mixed_fields is not None:
+                per_case_mixed.append(None if k in mixed_bad else field_errors(mixed_fields[k], ref))
+        ok = [e for e in per_case if e is not None]
+        okm = [e for e in per_case_mixed if e is not None]
+        parity = {
+            "oracle": f"{'the reference build (gcc -O3)' if res[0][0] == 'reference' else 'the oracle port'}: "
+                      f"every case for the cycles its GPU solve ran {cycles_per_solve}, one host process per case "
+                      f"({wall:.0f} s wall, longest case {max(r[1] for r in res):.0f} s)",
+            "metric": "relative L2 of level-0 u, v, sc and mean-free interior p, max over fields",
+            "fp64": {"max": max(ok) if ok else None, "per_case": per_case},
+            "mixed": {"max": max(okm) if okm else None, "per_case": per_case_mixed} if mixed_fields else None,
+            "bar": 1e-6,
+        }
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        sys.path.insert(0, os.path.join(REPO, "oracle"))
-        import oracle
-        with Solver(cases[:1], device=local) as s3:
-            pr0 = profiles[0] if profiles else None
-            if pr0 is not None:
-                s3.set_inlet_profile(0, pr0)
-            o = oracle.OracleCase(cases[0], pr0)
-            s3.cycle(3)
-            o.cycle(3)
-            l2err = max(float(np.linalg.norm(s3.field(0, 0, f) - o.get(0, f)) /
-                              max(np.linalg.norm(o.get(0, f)), 1e-300)) for f in ("u", "v", "p", "sc"))
         ctc = cycles_per_solve
-        v, kind, wall, tcyc = cpu_sample(cases, ctc, {"c1": 30, "c0": 400}.get(a.workload, 20),
+        v, kind, wall, tcyc = cpu_sample(WORKLOAD_DIRS.get(a.workload) or cases, ctc,
+                                         {"c1": 30, "c0": 400}.get(a.workload, 20),
                                          max(1, min(os.cpu_count() or 1, 64)))
         cpu = {"value": v, "unit": "solves/s", "cores": max(1, min(os.cpu_count() or 1, 64)), "kind": kind,
                "sample": f"V-cycles timed per host process ({wall:.1f} s wall), one case per process, "
@@ -593,10 +674,7 @@ def main():
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms / a.steps, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded obstacle patterns)",
-            "config": {"workload": desc, "cases_per_gpu": n_cases,
-                       "stop_rule": "reference: mass error < convergence or nvcycle V-cycles",
-                       "nvcycle": [c.nvcycle for c in cases], "l2": "flushed between steps (256 MiB write)",
-                       "parallelism": f"independent cases, {world} rank(s)"},
+            "config": workload_config(desc, n_cases, [c.nvcycle for c in cases], world),
             "cycles_per_solve": cycles_per_solve if n_cases <= 8 else
             {"min": int(min(cycles_per_solve)), "max": int(max(cycles_per_solve)),
              "mean": float(np.mean(cycles_per_solve))},
@@ -604,13 +682,14 @@ def main():
                          "note": "the mass error turned NaN/Inf (the reference build diverges on the same "
                                  "inputs); stopped at that cycle, not counted as solves"} if diverged else None,
             "cell_sweeps_per_s": cell_sweeps_per_s,
-            "l2_rel_err_vs_oracle_3cycles": l2err,
+            "l2_rel_err_vs_oracle": parity,
             "roofline": roofline,
             "batched": batched,
             "mixed": mixed,
             "gradient": grad,
             "schedule": {"autotuned": tuned is not None,
-                         "tuning": {k: v[:max(c.ngrid for c in cases)] for k, v in tuned.items()} if tuned else None},
+                         "tuning": {k: v[:max(c.ngrid for c in cases)] if isinstance(v, list) else v
+                                    for k, v in tuned.items()} if tuned else None},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": int(launches),

@@ -172,6 +172,12 @@ typedef struct mgfvm_tuning {
                                               corrections in the gather from the
                                               restriction's saved R(x_f) (no separate
                                               correction kernel): 0 or 2 yes, 1 no      */
+    int tma_first_wait;                    /* polls of a TMA-staged smoother CTA's first
+                                              wait for its loads before it gives up and
+                                              the call fails with MGFVM_ETIMEOUT: 0 = the
+                                              default (2^22), n > 0 = n, -1 = none (the
+                                              wait gives up at once; exercises the
+                                              timeout path)                             */
 } mgfvm_tuning;
 
 typedef struct mgfvm_ctx mgfvm_ctx;
@@ -416,7 +422,9 @@ int mgfvm_check_division(int device, long long n, unsigned long long seed, long 
  * ((npx-2)*(npy-2)) are rejected with MGFVM_EINVAL.  Allocates nothing.  All calls
  * on a device share that array: calls that overlap on the GPU race.  The first call
  * on each device looks up the array's device address; make it before any stream
- * capture. */
+ * capture.  That address is cached per device for the life of the process and does
+ * not survive a cudaDeviceReset of that device.  A non-null `stream` must belong to
+ * the current device (MGFVM_EINVAL otherwise). */
 int mgfvm_masserror_f64_noalloc(const double *u, const double *v, const double *areax,
                                 const double *areay, double *su, double *pp, int npx,
                                 int npy, double *err_out, void *stream);

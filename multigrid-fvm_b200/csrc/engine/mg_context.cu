@@ -965,6 +965,7 @@ int create_impl(const mgfvm_config *cases, int ncases, const mgfvm_options *opt_
     x->sched.isolve = cases[0].isolve;
     x->sched.nswpm = cases[0].nswpm;
     x->sched.nswpp = cases[0].nswpp;
+    x->sched.tma_wait_polls = TMA_WAIT_POLLS;
     x->cfg.assign(cases, cases + ncases);
     x->obs.resize(ncases);
     x->profile.resize(ncases);
@@ -1205,7 +1206,10 @@ static int check_status(mgfvm_ctx *x)
         if (x->hs[c].status & CASE_BAD_LAUNCH)
             return mgfvm_fail(MGFVM_ECUDA, "case %d: a smoother launch was too small for its tile", c);
         if (x->hs[c].status & CASE_WAIT_TIMEOUT)
-            return mgfvm_fail(MGFVM_ETIMEOUT, "case %d: a smoother CTA gave up waiting for its TMA loads", c);
+            return mgfvm_fail(MGFVM_ETIMEOUT,
+                              "a smoother CTA of case %d gave up waiting for its TMA loads: the results of every "
+                              "case from this call are invalid; mgfvm_reset returns the context to a defined state",
+                              c);
     }
     return MGFVM_OK;
 }
@@ -1473,7 +1477,7 @@ static bool tuning_valid(const mgfvm_tuning &t)
         if (t.coarse_kernel[ig] < 0 || t.coarse_kernel[ig] > 2) return false;
         if (t.prol_fused[ig] < 0 || t.prol_fused[ig] > 2) return false;
     }
-    return true;
+    return t.tma_first_wait >= -1;
 }
 
 // The first level of the one-CTA coarse kernel from x->tune.coarse_kernel (the first
@@ -1539,6 +1543,7 @@ int mgfvm_set_tuning(mgfvm_ctx *x, const mgfvm_tuning *t)
     RC(check_ctx(x));
     if (!t || !tuning_valid(*t)) return mgfvm_fail(MGFVM_EINVAL, "tuning values outside the allowed sets");
     x->tune = *t;
+    x->sched.tma_wait_polls = t->tma_first_wait == 0 ? TMA_WAIT_POLLS : std::max(0, t->tma_first_wait);
     return rebuild_schedule(x);
 }
 

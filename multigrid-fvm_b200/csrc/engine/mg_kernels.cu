@@ -455,10 +455,10 @@ __global__ void __launch_bounds__(NT, SMOOTH_BLOCK / NT) k_smooth(const CaseDev 
 // update, so the results are those of k_smooth bit for bit.
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 
-// Wait for the mbarrier's phase 0 with a bounded number of polls; false on timeout.
-__device__ __forceinline__ bool mbar_wait0(unsigned bar)
+// Wait for the mbarrier's phase 0 with at most `polls` polls; false on timeout.
+__device__ __forceinline__ bool mbar_wait0(unsigned bar, int polls)
 {
-    for (int it = 0; it < (1 << 22); ++it) {
+    for (int it = 0; it < polls; ++it) {
         unsigned done;
         asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
                      "selp.u32 %0, 1, 0, p;\n\t}"
@@ -473,7 +473,7 @@ __device__ __forceinline__ bool mbar_wait0(unsigned bar)
 template <int ISOLVE, int NT>
 __global__ void __launch_bounds__(NT, SMOOTH_BLOCK / NT)
     k_smooth_tma(const CaseDev *__restrict__ cs, CaseState *st, const SmoothMap *__restrict__ maps, int ig, int mode,
-                 int mask, int u0, int nu, int dir, int tile, int bw, int bh)
+                 int mask, int u0, int nu, int dir, int tile, int bw, int bh, int polls)
 {
     extern __shared__ __align__(128) double smt[];
     __shared__ __align__(8) unsigned long long mbar;
@@ -511,10 +511,13 @@ __global__ void __launch_bounds__(NT, SMOOTH_BLOCK / NT)
     }
     // one decision for the whole block (a thread that gave up at the limit while the
     // others saw the copies land must not split the block at the barriers below)
-    if (!__syncthreads_and(mbar_wait0(bar))) {
-        // record the stall and give the copies a second bounded wait before leaving
+    if (!__syncthreads_and(mbar_wait0(bar, polls))) {
+        // record the stall and give the copies a second wait, at the full bound, so they
+        // land before the CTA leaves; should that wait expire too, the CTA leaves with
+        // copies in flight into shared memory a later CTA on this SM may take, and the
+        // call fails with every case's results undefined until mgfvm_reset
         if (threadIdx.x == 0) atomicOr(&st[blockIdx.y].status, (int)CASE_WAIT_TIMEOUT);
-        mbar_wait0(bar);
+        mbar_wait0(bar, TMA_WAIT_POLLS);
         return;
     }
     const int W = bw, limA = P.limA, limB = P.limB;
@@ -1352,18 +1355,19 @@ cudaError_t configure_kernels()
 }
 
 template <int ISOLVE>
-static void launch_smooth_tma(const Launch &X, dim3 g, int b, const CaseDev *dc, CaseState *ds, cudaStream_t st)
+static void launch_smooth_tma(const Launch &X, dim3 g, int b, const CaseDev *dc, CaseState *ds, int polls,
+                              cudaStream_t st)
 {
     const SmoothMap *m = (const SmoothMap *)X.ptr;
     if (b <= SMOOTH_BLOCK / 4)
         k_smooth_tma<ISOLVE, SMOOTH_BLOCK / 4><<<g, b, X.smem, st>>>(dc, ds, m, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3,
-                                                                     X.a4, X.bw, X.bh);
+                                                                     X.a4, X.bw, X.bh, polls);
     else if (b <= SMOOTH_BLOCK / 2)
         k_smooth_tma<ISOLVE, SMOOTH_BLOCK / 2><<<g, b, X.smem, st>>>(dc, ds, m, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3,
-                                                                     X.a4, X.bw, X.bh);
+                                                                     X.a4, X.bw, X.bh, polls);
     else
         k_smooth_tma<ISOLVE, SMOOTH_BLOCK><<<g, b, X.smem, st>>>(dc, ds, m, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3,
-                                                                 X.a4, X.bw, X.bh);
+                                                                 X.a4, X.bw, X.bh, polls);
 }
 
 template <int ISOLVE>
@@ -1420,8 +1424,8 @@ cudaError_t launch_one(const Launch &X, const CaseDev *dc, CaseState *ds, const 
     case K_COPY: k_copy<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, X.a0); break;
     case K_SMOOTH_TMA:
         if (b > SMOOTH_BLOCK || !X.ptr || X.smem > SMOOTH_TMA_SMEM_MAX || (X.bw & 1)) return cudaErrorInvalidValue;
-        if (S.isolve == MGFVM_JACOBI) launch_smooth_tma<MGFVM_JACOBI>(X, g, b, dc, ds, st);
-        else launch_smooth_tma<MGFVM_GAUSS_SEIDEL>(X, g, b, dc, ds, st);
+        if (S.isolve == MGFVM_JACOBI) launch_smooth_tma<MGFVM_JACOBI>(X, g, b, dc, ds, S.tma_wait_polls, st);
+        else launch_smooth_tma<MGFVM_GAUSS_SEIDEL>(X, g, b, dc, ds, S.tma_wait_polls, st);
         break;
     case K_PP_LEVEL:
         if (b > SMOOTH_BLOCK) return cudaErrorInvalidValue;

@@ -52,8 +52,12 @@ struct __align__(64) SmoothMap {
     CUtensorMap coef, field;
 };
 
+// Polls of an mbarrier wait before a TMA-staged smoother CTA gives up on its loads.
+constexpr int TMA_WAIT_POLLS = 1 << 22;
+
 struct Sched {
     int isolve, nswpm, nswpp;
+    int tma_wait_polls;   // first wait of a TMA-staged smoother CTA (mgfvm_tuning.tma_first_wait)
 };
 
 // Tile smoother geometry: a CTA of SMOOTH_BLOCK (one per SM) or SMOOTH_BLOCK/2 (two per

@@ -17,7 +17,12 @@
 //     on the GPU (different streams, or different host threads) race on the array.
 //   * The first call on a device looks up the array's device address with
 //     cudaGetSymbolAddress (the host-side name of a __device__ array is not a device
-//     address); make that first call on each device before any stream capture.
+//     address); make that first call on each device before any stream capture.  The
+//     address is cached per device ordinal for the life of the process: after a
+//     cudaDeviceReset the cached address is stale, so do not call this entry point
+//     on a device after resetting it.
+//   * The work runs on the caller's stream, with the scratch address of the current
+//     device: a non-null stream must belong to the current device (checked, EINVAL).
 //   * Nothing here calls cudaMalloc, cudaFree or an allocating library routine.
 #include <mutex>
 
@@ -71,11 +76,23 @@ extern "C" int mgfvm_masserror_f64_noalloc(const double *u, const double *v, con
                           "mgfvm_masserror_f64_noalloc: %lld interior cells exceed its fixed scratch "
                           "limit of %lld; use mgfvm_masserror_f64 with a caller buffer",
                           cells, NOALLOC_MAX_CELLS);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (s) {
+        // the scratch address is that of the current device; a stream of another device
+        // would hand its kernel a foreign address
+        int cur = -1, sdev = -1;
+        cudaError_t e = cudaGetDevice(&cur);
+        if (e == cudaSuccess) e = cudaStreamGetDevice(s, &sdev);
+        if (e != cudaSuccess) return mgfvm_fail(MGFVM_ECUDA, "stream device: %s", cudaGetErrorString(e));
+        if (sdev != cur)
+            return mgfvm_fail(MGFVM_EINVAL,
+                              "mgfvm_masserror_f64_noalloc: the stream belongs to device %d, the current device is %d",
+                              sdev, cur);
+    }
     double *scratch = nullptr;
     int rc = scratch_address(&scratch);
     if (rc != MGFVM_OK) return rc;
     const size_t nb = mg::raw_masserror_blocks(npx, npy);
-    cudaStream_t s = (cudaStream_t)stream;
     // the completion counter sits right after this call's partial sums; an earlier
     // call with more blocks may have left a partial sum there
     cudaError_t e = cudaMemsetAsync(scratch + nb * mg::RED_STRIDE, 0, sizeof(double), s);

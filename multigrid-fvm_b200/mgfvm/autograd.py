@@ -40,4 +40,6 @@ def objective(inlet_u: torch.Tensor, amuf: torch.Tensor, prsc: torch.Tensor, cfg
     """J(inlet_u, amuf, prsc) after `cycles` V-cycles of `cfg` (its own amuf and prsc
     are replaced by the arguments); inlet_u holds one value per level-0 inlet face
     (cfg.nfy values)."""
+    if inlet_u.numel() != cfg.nfy:
+        raise ValueError(f"inlet_u holds {inlet_u.numel()} values; the case has {cfg.nfy} inlet faces")
     return Objective.apply(inlet_u, amuf, prsc, cfg, int(cycles), int(device))

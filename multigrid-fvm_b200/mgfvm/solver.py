@@ -236,10 +236,13 @@ class Solver:
 
     def set_tuning(self, **per_level) -> None:
         """Replace schedule choices, e.g. set_tuning(smooth_units={0: 4}, asm_slices={1: 1});
-        unspecified levels keep their values."""
+        unspecified levels keep their values.  Scalar fields (tma_first_wait) take an int."""
         t = _abi.Tuning()
         check(self._lib.mgfvm_get_tuning(self._h, C.byref(t)))
         for key, vals in per_level.items():
+            if isinstance(vals, (int, np.integer)):
+                setattr(t, key, int(vals))
+                continue
             arr = getattr(t, key)
             for lv, v in (vals.items() if isinstance(vals, dict) else enumerate(vals)):
                 arr[lv] = int(v)

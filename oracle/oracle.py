@@ -33,8 +33,11 @@ _ip = C.POINTER(C.c_int)
 
 
 def build(quiet: bool = True) -> None:
-    """Compile liboracle.so (and _ref/ where the reference source exists)."""
-    out = subprocess.run(["make", "-C", HERE, "all"], capture_output=True, text=True)
+    """Compile liboracle.so (and _ref/ when the environment variable MGFVM_REF_DIR names
+    the directory holding the reference's Version-6-26-04.c)."""
+    ref = os.environ.get("MGFVM_REF_DIR")
+    out = subprocess.run(["make", "-C", HERE, "all"] + ([f"REF_DIR={ref}"] if ref else []),
+                         capture_output=True, text=True)
     if out.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
     if not quiet:
@@ -189,13 +192,15 @@ class RefCase:
     """The reference itself (one case at a time: its state is process-global)."""
 
     def __init__(self, cfg: CaseConfig, inlet_u=None, workdir=None):
+        """cfg = None: `workdir` already holds the case's InputData and pattern.txt."""
         self.lib = _ref_lib()
         self.cfg = cfg
         self._tmp = None
         if workdir is None:
             self._tmp = tempfile.TemporaryDirectory()
             workdir = self._tmp.name
-        cfg.write(workdir)
+        if cfg is not None:
+            cfg.write(workdir)
         prof, n = None, 0
         if inlet_u is not None:
             prof = np.ascontiguousarray(inlet_u, dtype=np.float64)

@@ -1,9 +1,9 @@
 """Regenerate the golden fixtures of tests/golden/ from the reference itself.
 
 Runs only where the reference source exists (it builds oracle/_ref from
-Version-6-26-04.c with oracle/Makefile):
+Version-6-26-04.c with oracle/Makefile; MGFVM_REF_DIR names its directory):
 
-    python tests/golden/make_golden.py
+    MGFVM_REF_DIR=<reference checkout> python tests/golden/make_golden.py
 
 Writes, per case,
   <name>.npz     initial state (masks, areas, boundary values) of every level, the

@@ -36,6 +36,27 @@ def test_obstacle_flow_pair(oracle_built):
         _check(s, k, o, 3, f"obstacle flow case {k}", levels=range(cfg.ngrid))
 
 
+def test_obstacle_flow_pair_long_run(oracle_built):
+    """The benchmark's solve, shortened to 250 V-cycles: the autotuned schedule and the
+    chunked solve with the reference's stop rule, then every level-0 field against the
+    oracle's 250 cycles, bit for bit (the converged-field error of the benchmark is 0)."""
+    from mgfvm import Solver, configs
+    from oracle import OracleCase
+    cases = configs.c1_pair(seed=1)
+    n = 250
+    with Solver(cases, sync_every=64) as s:
+        s.autotune(2)
+        ran = s.solve(n, 0.0)
+        assert list(ran) == [n, n]
+        for k, cfg in enumerate(cases):
+            o = OracleCase(cfg)
+            o.cycle(n)
+            for f in ("u", "v", "p", "pp", "sc"):
+                assert_bitexact(s.field(k, 0, f), o.get(0, f), f"obstacle flow case {k} after {n} cycles, {f}")
+            np.testing.assert_allclose(s.history(k)[0], o.history()[0], rtol=1e-12, atol=0)
+            o.close()
+
+
 def test_mixed_size_batch(oracle_built):
     from mgfvm import Solver, configs
     from oracle import OracleCase

@@ -226,7 +226,7 @@ def test_autotune_keeps_state(oracle_built):
     before, after, chosen = s.autotune(2)
     assert before > 0 and 0 < after <= before
     assert set(chosen) == {"smooth_units", "smooth_threads", "asm_slices", "restrict_slices", "update_pfix", "odd_chunks", "pp_level",
-                           "smooth_tma", "coarse_kernel", "prol_fused"}
+                           "smooth_tma", "coarse_kernel", "prol_fused", "tma_first_wait"}
     _compare(s, o, STATE, what="after autotune")
     s.cycle(3)
     o.cycle(3)
@@ -267,4 +267,26 @@ def test_zero_cycles_and_mixed_depth_batch(oracle_built):
     osh.cycle(1)
     _compare(s, od, STATE, case=0, what="deep case")
     _compare(s, osh, STATE, case=1, what="shallow case")
+    s.close()
+
+
+def test_tma_wait_timeout_fails_the_call_and_reset_recovers(oracle_built):
+    """A TMA-staged smoother CTA whose first wait for its loads gives up (here at once:
+    tma_first_wait = -1, a wait with no polls) records the stall, lets its copies land
+    in a second wait at the full bound and leaves; the call fails with ETIMEOUT.  After
+    mgfvm_reset, with the default wait, the context runs the oracle's cycles again."""
+    from mgfvm import MgfvmError, configs
+    from mgfvm._abi import ETIMEOUT
+    cfg = configs.small(64, 3, isolve=2, ig_obs=3, sc_obs=0.2, obstacles=[(2, 3, 2, 2), (5, 6, 4, 6)])
+    s, o = _pair(cfg)
+    s.set_tuning(smooth_tma=[2, 2, 2], smooth_units=[3, 3, 3], tma_first_wait=-1)
+    with pytest.raises(MgfvmError) as ei:
+        s.cycle(1)
+    assert ei.value.status == ETIMEOUT
+    assert "every case" in str(ei.value)
+    s.set_tuning(tma_first_wait=0)
+    s.reset()
+    s.cycle(2)
+    o.cycle(2)
+    _compare(s, o, STATE, what="after a timed-out call, reset and 2 cycles")
     s.close()
