@@ -223,6 +223,60 @@ def gradient_rate(device, cycles=4, check=True):
     return out
 
 
+def adjoint_rate(device, ncases=64, cycles=10, check=True):
+    """Reverse-mode gradients of the adjoint configuration (ncases cases of 256 x 256,
+    seeded random obstacles, Re 100, per-face inlet profiles): one mgfvm_adjoint run of
+    the whole batch over `cycles` V-cycles (forward run with checkpoints, re-runs, and
+    the taped cycle + transpose per cycle), against a plain forward run of the same
+    cycles; case 0's gradient checked against the forward mode (all nfy + 2 directions)
+    and one inlet face against the oracle's central difference."""
+    from mgfvm import Solver, configs, gradient
+    cases, profs = configs.c4(ncases, seed=4)
+    with Solver(cases, device=device, sync_every=64) as s:
+        for k, pr in enumerate(profs):
+            s.set_inlet_profile(k, pr)
+        s.cycle(cycles)
+        fwd_ms = s.last_elapsed_ms / cycles
+        s.adjoint(2)                                   # warm-up
+        s.adjoint(cycles)
+        adj_ms = s.last_elapsed_ms
+        res0 = s.adjoint_gradient(0)
+    out = {"config": f"adjoint configuration: {ncases} cases 256x256, ngrid 5, seeded random obstacles, Re 100, "
+                     f"inlet profile 1 + 0.1 N(0,1)",
+           "method": "reverse mode: taped V-cycle and its phase-by-phase transpose, checkpoints every ~sqrt(n) "
+                     "cycles",
+           "cycles": cycles, "gradients": ncases, "directions_per_gradient": cases[0].nfy + 2,
+           "ms_total": round(adj_ms, 3), "ms_per_cycle": round(adj_ms / cycles, 3),
+           "forward_ms_per_cycle": round(fwd_ms, 3),
+           "cost_vs_forward_cycles": round(adj_ms / cycles / fwd_ms, 2),
+           "note": "a gradient over n cycles costs cost_vs_forward_cycles x the plain batch's n cycles"}
+    if check:
+        j, g_in, g_a, g_p = res0
+        jf, gf, af, pf = gradient(cases[0], profs[0], cycles, device)
+        full_a, full_f = np.concatenate([g_in, [g_a, g_p]]), np.concatenate([gf, [af, pf]])
+        out["check_vs_forward_mode"] = float(np.abs(full_a - full_f).max() / np.abs(full_f).max())
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        import oracle
+
+        def j_after(pr):
+            o = oracle.OracleCase(cases[0], pr)
+            o.cycle(cycles)
+            p, sc = o.get(0, "p"), o.get(0, "sc")
+            o.close()
+            ny = p.shape[0] - 2
+            return (p[1:-1, 1].sum() / ny - p[1:-1, -2].sum() / ny) + sc[1:-1, -1].sum() / ny
+
+        k = int(np.argmax(np.abs(g_in)))
+        h = 1e-6 * abs(profs[0][k])
+        pp, pm = profs[0].copy(), profs[0].copy()
+        pp[k] += h
+        pm[k] -= h
+        fd = (j_after(pp) - j_after(pm)) / (2 * h)
+        out["check_vs_oracle_central_difference"] = {"inlet_face": k, "rel_err": abs(g_in[k] - fd) / abs(fd),
+                                                     "bar": 1e-4}
+    return out
+
+
 def mixed_solve(cases, device, ref_solver, tune, profiles=None):
     """One solve of the workload with MGFVM_PREC_MIXED (FP32 correction smoothing
     against FP64 residuals), timed like a bench step, and the relative L2 distance of
@@ -427,7 +481,7 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the engine's default schedule")
     ap.add_argument("--batch", type=int, default=64,
                     help="cases of the batched obstacle-flow measurement (0: skip it)")
-    ap.add_argument("--no-gradient", action="store_true", help="skip the forward-mode gradient measurement")
+    ap.add_argument("--no-gradient", action="store_true", help="skip the gradient measurements")
     ap.add_argument("--profile-cycles", type=int, default=0,
                     help="only run 3 warm-up V-cycles then this many V-cycles of the workload "
                          "(for ncu launch lists) and exit")
@@ -630,9 +684,10 @@ def main():
         batched = batched_rate(a.batch, local, not a.no_autotune, cycles_per_solve)
 
     # ---- derivatives: a whole gradient of J by forward mode, one batch
-    grad = None
+    grad = adj = None
     if world == 1 and not a.no_gradient:
         grad = gradient_rate(local, check=not a.no_cpu_baseline)
+        adj = adjoint_rate(local, check=not a.no_cpu_baseline)
 
     # ---- parity of the timed solve against the CPU oracle's run of the same cycles
     parity = None
@@ -687,6 +742,7 @@ def main():
             "batched": batched,
             "mixed": mixed,
             "gradient": grad,
+            "adjoint": adj,
             "schedule": {"autotuned": tuned is not None,
                          "tuning": {k: v[:max(c.ngrid for c in cases)] if isinstance(v, list) else v
                                     for k, v in tuned.items()} if tuned else None},

@@ -178,6 +178,11 @@ typedef struct mgfvm_tuning {
                                               default (2^22), n > 0 = n, -1 = none (the
                                               wait gives up at once; exercises the
                                               timeout path)                             */
+    int pdl;                               /* programmatic dependent launch between the
+                                              V-cycle's kernels (a kernel's CTAs are
+                                              scheduled while its predecessor finishes
+                                              and wait for it on the device): 0 or 2
+                                              yes, 1 no                                 */
 } mgfvm_tuning;
 
 typedef struct mgfvm_ctx mgfvm_ctx;
@@ -336,6 +341,29 @@ int mgfvm_objective(mgfvm_ctx *ctx, int icase, double *J, double *dJ);
  * NULL. */
 int mgfvm_gradient(const mgfvm_config *cfg, const double *inlet_u, int n_inlet, int ncycles, int device,
                    double *J, double *dJ_dinlet, double *dJ_damuf, double *dJ_dprsc);
+
+/* Reverse mode (discrete adjoint) of the same iteration: every case of a plain FP64
+ * context is returned to its initial state and run `ncycles` V-cycles, then the
+ * transpose of those cycles is applied from the adjoint of J (mgfvm_objective) back to
+ * the initial state, so one call gives the whole gradient of every case's J after
+ * ncycles cycles — the inlet faces, amuf and prsc — at the cost of a few V-cycles per
+ * cycle instead of nfy + 2 tangent runs.  Each cycle is transposed phase by phase:
+ * the cycle is re-run with the arrays every phase overwrites saved, then each phase,
+ * last to first, restores them and passes the adjoints of its outputs to its inputs
+ * with the derivatives the forward mode uses (so the two agree to rounding).  Earlier
+ * cycles' states come back from checkpoints of u, v, p, sc taken every ~sqrt(ncycles)
+ * cycles and re-runs between them.  Afterwards u, v, p, sc and the histories are
+ * those after ncycles cycles (other arrays unspecified).  Periodic boundaries are not
+ * covered (MGFVM_EUNSUPPORTED); a case that turns non-finite fails the call
+ * (MGFVM_ENONFINITE).  Replaces no routine of the reference: the reference computes
+ * no derivatives. */
+int mgfvm_adjoint(mgfvm_ctx *ctx, int ncycles);
+
+/* The last mgfvm_adjoint's result for case `icase`: J after the cycles and its
+ * gradient (dJ_dinlet: nfy values, the inlet faces of mgfvm_set_inlet_profile).  Any
+ * pointer may be NULL. */
+int mgfvm_adjoint_gradient(mgfvm_ctx *ctx, int icase, double *J, double *dJ_dinlet, double *dJ_damuf,
+                           double *dJ_dprsc);
 
 /* Bytes this context copied host->device and device->host since it was created. */
 int mgfvm_transfer_bytes(mgfvm_ctx *ctx, long long *h2d, long long *d2h);

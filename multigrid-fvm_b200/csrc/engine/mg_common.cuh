@@ -64,7 +64,8 @@ constexpr int PFAN_END = 1 << 30;    // pfan bit: last copy of its owner (PFAN_L
 
 // Stop-rule and status flags of one case.
 enum CaseStatus { CASE_RUNNING = 0, CASE_CONVERGED_REF = 1, CASE_CONVERGED_FP = 2,
-                  CASE_NONFINITE = 4, CASE_BAD_LAUNCH = 8, CASE_WAIT_TIMEOUT = 16 };
+                  CASE_NONFINITE = 4, CASE_BAD_LAUNCH = 8, CASE_WAIT_TIMEOUT = 16,
+                  CASE_TAPE_ESCAPE = 32 };   // an adjoint phase wrote outside its tape (mg_adjoint.cu)
 
 // Read-only description of one case during a launch (the host rewrites it between
 // launches): physics, boundary codes, the level table and where histories and

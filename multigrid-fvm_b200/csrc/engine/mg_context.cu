@@ -18,6 +18,7 @@
 #include <string>
 #include <vector>
 
+#include "mg_adjoint.cuh"
 #include "mg_init.cuh"
 #include "mg_kernels.cuh"
 #include "mg_tangent.cuh"
@@ -92,6 +93,10 @@ struct mgfvm_ctx {
     SmoothMap *dmaps = nullptr;
     std::vector<int> tail0;                   // per case: first one-CTA-kernel level chosen at creation
     std::vector<void *> pooled;               // buffers taken from the device's memory pool
+    // the last mgfvm_adjoint: per case J and its gradient (nfy inlet faces, amuf, prsc)
+    int adj_cycles = -1;
+    std::vector<double> adj_J, adj_gamuf, adj_gprsc;
+    std::vector<std::vector<double>> adj_gin;
 };
 
 static inline int npx_of(const mgfvm_config &c, int ig) { return c.nfx / (1 << ig) + 2; }
@@ -966,6 +971,7 @@ int create_impl(const mgfvm_config *cases, int ncases, const mgfvm_options *opt_
     x->sched.nswpm = cases[0].nswpm;
     x->sched.nswpp = cases[0].nswpp;
     x->sched.tma_wait_polls = TMA_WAIT_POLLS;
+    x->sched.pdl = true;
     x->cfg.assign(cases, cases + ncases);
     x->obs.resize(ncases);
     x->profile.resize(ncases);
@@ -1477,7 +1483,7 @@ static bool tuning_valid(const mgfvm_tuning &t)
         if (t.coarse_kernel[ig] < 0 || t.coarse_kernel[ig] > 2) return false;
         if (t.prol_fused[ig] < 0 || t.prol_fused[ig] > 2) return false;
     }
-    return t.tma_first_wait >= -1;
+    return t.tma_first_wait >= -1 && t.pdl >= 0 && t.pdl <= 2;
 }
 
 // The first level of the one-CTA coarse kernel from x->tune.coarse_kernel (the first
@@ -1544,6 +1550,7 @@ int mgfvm_set_tuning(mgfvm_ctx *x, const mgfvm_tuning *t)
     if (!t || !tuning_valid(*t)) return mgfvm_fail(MGFVM_EINVAL, "tuning values outside the allowed sets");
     x->tune = *t;
     x->sched.tma_wait_polls = t->tma_first_wait == 0 ? TMA_WAIT_POLLS : std::max(0, t->tma_first_wait);
+    x->sched.pdl = t->pdl != 1;
     return rebuild_schedule(x);
 }
 
@@ -1846,6 +1853,244 @@ int mgfvm_gradient(const mgfvm_config *cfg, const double *inlet_u, int n_inlet, 
         RC(rc);
         d0 += n;
     }
+    return MGFVM_OK;
+}
+
+// ------------------------------------------------------------------ adjoint
+// Reverse mode of `ncycles` V-cycles from the initial state (mg_adjoint.cuh): the
+// forward run keeps the u, v, p, sc arrays of every level (all a cycle reads of the
+// previous cycles' results) at the start of every m-th cycle, m ~ sqrt(ncycles); the
+// reverse sweep then takes the segments last to first, re-runs each from its
+// checkpoint keeping the start of every one of its cycles, and runs the taped cycle
+// and its transpose for those cycles last to first.  Memory: (ncycles/m + m) copies
+// of those arrays, one cycle's tape and one set of adjoint arrays per case.
+int mgfvm_adjoint(mgfvm_ctx *x, int ncycles)
+{
+    RC(check_ctx(x));
+    if (x->opt.tangent) return mgfvm_fail(MGFVM_EINVAL, "mgfvm_adjoint: not available in a tangent context");
+    if (x->opt.precision != MGFVM_PREC_FP64)
+        return mgfvm_fail(MGFVM_EUNSUPPORTED, "mgfvm_adjoint: FP64 contexts only");
+    if (ncycles < 0) return mgfvm_fail(MGFVM_EINVAL, "negative cycle count");
+    const int n = x->ncases;
+    // the phase programs and their tapes
+    std::vector<std::vector<Phase>> progs(n);
+    std::vector<long long> tape_n(n), tape_off(n), prog_off(n), live_off(n);
+    long long tape_tot = 0, prog_tot = 0, live_tot = 0;
+    for (int c = 0; c < n; ++c) {
+        if (!build_adj_program(x->hc[c], x->sched, progs[c], tape_n[c]))
+            return mgfvm_fail(MGFVM_EUNSUPPORTED, "mgfvm_adjoint: case %d has periodic boundaries (not covered)", c);
+        tape_off[c] = tape_tot;
+        tape_tot += (tape_n[c] + 31) / 32 * 32;
+        prog_off[c] = prog_tot;
+        prog_tot += (long long)progs[c].size();
+        live_off[c] = live_tot;
+        for (int ig = 0; ig < x->cfg[c].ngrid; ++ig) live_tot += 4LL * npx_of(x->cfg[c], ig) * npy_of(x->cfg[c], ig);
+    }
+    RC(pull(x));
+    if (!x->tpool) RC(alloc_tangent(x));     // the adjoint arrays: the derivative storage's layout
+    const int m = std::max(1, (int)std::ceil(std::sqrt((double)std::max(ncycles, 1))));
+    const int nseg = (ncycles + m - 1) / m;
+    // device buffers
+    Phase *dprog = nullptr;
+    CaseAdj *dadj = nullptr;
+    double *tape = nullptr, *pacc = nullptr, *ckpt = nullptr, *seg = nullptr, *fin = nullptr;
+    long long *dlive = nullptr;
+    const size_t pacc_n = (size_t)n * 2 * MAXLEV;
+    std::vector<void **> bufs = {(void **)&dprog, (void **)&dadj, (void **)&tape, (void **)&pacc, (void **)&ckpt,
+                                 (void **)&seg, (void **)&fin, (void **)&dlive};
+    const size_t sizes[] = {sizeof(Phase) * (size_t)std::max<long long>(prog_tot, 1), sizeof(CaseAdj) * (size_t)n,
+                            sizeof(double) * (size_t)std::max<long long>(tape_tot, 1), sizeof(double) * pacc_n,
+                            sizeof(double) * (size_t)live_tot * std::max(nseg, 1), sizeof(double) * (size_t)live_tot * m,
+                            sizeof(double) * (size_t)live_tot, sizeof(long long) * (size_t)n};
+    auto release = [&]() {
+        cudaStreamSynchronize(x->stream);
+        for (void **b : bufs)
+            if (*b) {
+                ctx_free(x, *b);
+                *b = nullptr;
+            }
+    };
+    for (size_t k = 0; k < bufs.size(); ++k) {
+        cudaError_t me = ctx_malloc(x, bufs[k], sizes[k]);
+        if (me != cudaSuccess) {
+            *bufs[k] = nullptr;
+            release();
+            cudaGetLastError();
+            return mgfvm_fail(me == cudaErrorMemoryAllocation ? MGFVM_ENOMEM : MGFVM_ECUDA,
+                              "mgfvm_adjoint: %zu bytes of checkpoints, tape or programs: %s", sizes[k],
+                              cudaGetErrorString(me));
+        }
+    }
+    int rc = MGFVM_OK;
+    std::vector<CaseState> hs_final;
+    const int maxng = x->maxng, maxcells = *std::max_element(x->maxcells.begin(), x->maxcells.end());
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, x->device);
+    int cluster = adj_cluster_size(n, std::max(sms, 1));
+    if (const char *env = std::getenv("MGFVM_ADJOINT_CLUSTER")) {
+        const int v = std::atoi(env);
+        if (v == 1 || v == 2 || v == 4 || v == 8) cluster = v;
+    }
+    auto live = [&](double *buf, int dir) -> int {
+        cudaError_t e = launch_live_copy(x->dc, dlive, buf, n, maxcells, maxng, dir, x->stream);
+        if (e != cudaSuccess) return mgfvm_fail(MGFVM_ECUDA, "checkpoint copy: %s", cudaGetErrorString(e));
+        return MGFVM_OK;
+    };
+    do {
+        // programs, per-case descriptors
+        std::vector<Phase> flat;
+        flat.reserve((size_t)prog_tot);
+        for (auto &pg : progs) flat.insert(flat.end(), pg.begin(), pg.end());
+        std::vector<CaseAdj> ha(n);
+        for (int c = 0; c < n; ++c)
+            ha[c] = CaseAdj{dprog + prog_off[c], (int)progs[c].size(), tape + tape_off[c], pacc + (size_t)c * 2 * MAXLEV};
+        if (cudaMemcpy(dprog, flat.data(), sizeof(Phase) * flat.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(dadj, ha.data(), sizeof(CaseAdj) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(dlive, live_off.data(), sizeof(long long) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemset(pacc, 0, sizeof(double) * pacc_n) != cudaSuccess) {
+            rc = mgfvm_fail(MGFVM_ECUDA, "mgfvm_adjoint: upload: %s", cudaGetErrorString(cudaGetLastError()));
+            break;
+        }
+        x->h2d += (long long)(sizeof(Phase) * flat.size() + sizeof(CaseAdj) * n + sizeof(long long) * n);
+        // forward: from the initial state, checkpoints at the start of every m-th cycle
+        if ((rc = init_state(x, -1)) != MGFVM_OK) break;
+        if ((rc = ensure_hist(x, ncycles)) != MGFVM_OK) break;
+        if ((rc = set_controls(x, 0, 0.0)) != MGFVM_OK) break;
+        if (cudaEventRecord(x->e0, x->stream) != cudaSuccess) { rc = mgfvm_fail(MGFVM_ECUDA, "event"); break; }
+        for (int sgi = 0; sgi < nseg && rc == MGFVM_OK; ++sgi) {
+            rc = live(ckpt + (size_t)sgi * live_tot, 0);
+            if (rc == MGFVM_OK) rc = run_cycles(x, std::min(m, ncycles - sgi * m));
+        }
+        if (rc != MGFVM_OK || (rc = live(fin, 0)) != MGFVM_OK) break;
+        if ((rc = pull(x)) != MGFVM_OK || (rc = check_status(x)) != MGFVM_OK) break;
+        hs_final = x->hs;
+        // J of every case, and its adjoint seed on level 0 (zero elsewhere)
+        x->adj_J.assign(n, 0.0);
+        CK(cudaMemsetAsync(x->tpool, 0, x->tcase_off.empty() ? 0 : x->tcase_off.back() + x->tcase_bytes.back(),
+                           x->stream));
+        for (int c = 0; c < n && rc == MGFVM_OK; ++c) {
+            const LevelDev &L = x->hc[c].lv[0];
+            const size_t cells = (size_t)L.npx * L.npy;
+            std::vector<double> p(cells), sc(cells), bp(cells, 0.0), bsc(cells, 0.0);
+            if ((rc = mgfvm_get_field(x, c, 0, MGFVM_F_P, p.data())) != MGFVM_OK) break;
+            if ((rc = mgfvm_get_field(x, c, 0, MGFVM_F_SC, sc.data())) != MGFVM_OK) break;
+            bool finite = true;
+            for (size_t k = 0; k < cells; ++k) finite &= std::isfinite(p[k]) && std::isfinite(sc[k]);
+            if (!finite) {
+                rc = mgfvm_fail(MGFVM_ENONFINITE, "mgfvm_adjoint: case %d turned non-finite within %d cycles", c,
+                                ncycles);
+                break;
+            }
+            objective_of(p.data(), sc.data(), L.npx, L.npy, &x->adj_J[c]);
+            const double ny = (double)(L.npy - 2);
+            for (int j = 1; j <= L.npy - 2; ++j) {
+                bp[(size_t)j * L.npx + 1] += 1.0 / ny;
+                bp[(size_t)j * L.npx + L.npx - 2] += -1.0 / ny;
+                bsc[(size_t)j * L.npx + L.npx - 1] += 1.0 / ny;
+            }
+            const LevelTan &B = x->ht[c].lv[0];
+            if (cudaMemcpy(B.t[S_P], bp.data(), sizeof(double) * cells, cudaMemcpyHostToDevice) != cudaSuccess ||
+                cudaMemcpy(B.t[S_SC], bsc.data(), sizeof(double) * cells, cudaMemcpyHostToDevice) != cudaSuccess) {
+                rc = mgfvm_fail(MGFVM_ECUDA, "mgfvm_adjoint: seed: %s", cudaGetErrorString(cudaGetLastError()));
+                break;
+            }
+            x->h2d += (long long)(2 * sizeof(double) * cells);
+        }
+        if (rc != MGFVM_OK) break;
+        // reverse: segments last to first
+        for (int sgi = nseg - 1; sgi >= 0 && rc == MGFVM_OK; --sgi) {
+            const int cnt = std::min(m, ncycles - sgi * m);
+            rc = live(ckpt + (size_t)sgi * live_tot, 1);
+            for (int k = 0; k < cnt && rc == MGFVM_OK; ++k) {
+                rc = live(seg + (size_t)k * live_tot, 0);
+                if (rc == MGFVM_OK && k + 1 < cnt) rc = run_cycles(x, 1);
+            }
+            for (int k = cnt - 1; k >= 0 && rc == MGFVM_OK; --k) {
+                rc = live(seg + (size_t)k * live_tot, 1);
+                if (rc != MGFVM_OK) break;
+                cudaError_t e = launch_adj_cycle(x->dc, x->ds, x->dt, dadj, n, cluster, x->stream);
+                if (e != cudaSuccess) rc = mgfvm_fail(MGFVM_ECUDA, "adjoint cycle: %s", cudaGetErrorString(e));
+                x->launches += 1;
+            }
+        }
+        if (rc != MGFVM_OK) break;
+        if (cudaEventRecord(x->e1, x->stream) != cudaSuccess || cudaEventSynchronize(x->e1) != cudaSuccess) {
+            rc = mgfvm_fail(MGFVM_ECUDA, "mgfvm_adjoint: %s", cudaGetErrorString(cudaGetLastError()));
+            break;
+        }
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, x->e0, x->e1);
+        x->last_ms = ms;
+        if ((rc = pull(x)) != MGFVM_OK) break;
+        for (int c = 0; c < n; ++c)
+            if (x->hs[c].status & CASE_TAPE_ESCAPE) {
+                rc = mgfvm_fail(MGFVM_ECUDA, "mgfvm_adjoint: a phase of case %d wrote outside its tape", c);
+                break;
+            }
+        if (rc != MGFVM_OK || (rc = check_status(x)) != MGFVM_OK) break;
+        // gradients: the adjoint of the initial state through the parameters' seeding
+        // (the inlet face value and the coarse faces rest_geom averages from it; amu and
+        // amusc = amuf / prsc on every level)
+        std::vector<double> hp(pacc_n);
+        CK(cudaMemcpy(hp.data(), pacc, sizeof(double) * pacc_n, cudaMemcpyDeviceToHost));
+        x->d2h += (long long)(sizeof(double) * pacc_n);
+        x->adj_gin.assign(n, {});
+        x->adj_gamuf.assign(n, 0.0);
+        x->adj_gprsc.assign(n, 0.0);
+        for (int c = 0; c < n && rc == MGFVM_OK; ++c) {
+            const mgfvm_config &g = x->cfg[c];
+            std::vector<std::vector<double>> col(g.ngrid);
+            for (int ig = 0; ig < g.ngrid; ++ig) {
+                const int npx = npx_of(g, ig), npy = npy_of(g, ig);
+                col[ig].assign(npy, 0.0);
+                if (cudaMemcpy2D(col[ig].data(), sizeof(double), x->ht[c].lv[ig].t[S_U], sizeof(double) * npx,
+                                 sizeof(double), npy, cudaMemcpyDeviceToHost) != cudaSuccess) {
+                    rc = mgfvm_fail(MGFVM_ECUDA, "mgfvm_adjoint: %s", cudaGetErrorString(cudaGetLastError()));
+                    break;
+                }
+                x->d2h += (long long)(sizeof(double) * npy);
+            }
+            if (rc != MGFVM_OK) break;
+            std::vector<double> acc = col[g.ngrid - 1];
+            for (int ig = g.ngrid - 1; ig > 0; --ig) {
+                std::vector<double> fine = col[ig - 1];
+                for (int jc = 1; jc <= (int)acc.size() - 2; ++jc) {
+                    fine[2 * jc] += 0.5 * acc[jc];
+                    fine[2 * jc - 1] += 0.5 * acc[jc];
+                }
+                acc.swap(fine);
+            }
+            x->adj_gin[c].assign(acc.begin() + 1, acc.begin() + 1 + g.nfy);
+            double ga = 0.0, gs = 0.0;
+            for (int ig = 0; ig < g.ngrid; ++ig) {
+                const double bamu = hp[(size_t)c * 2 * MAXLEV + 2 * ig], bamusc = hp[(size_t)c * 2 * MAXLEV + 2 * ig + 1];
+                ga += bamu + bamusc * (1.0 / g.prsc);
+                gs += bamusc * (-g.amuf / (g.prsc * g.prsc));
+            }
+            x->adj_gamuf[c] = ga;
+            x->adj_gprsc[c] = gs;
+        }
+        if (rc != MGFVM_OK) break;
+        // leave u, v, p, sc and the histories as the forward run left them
+        if ((rc = live(fin, 1)) != MGFVM_OK) break;
+        x->hs = hs_final;
+        rc = push(x);
+        if (rc == MGFVM_OK) x->adj_cycles = ncycles;
+    } while (0);
+    release();
+    return rc;
+}
+
+int mgfvm_adjoint_gradient(mgfvm_ctx *x, int icase, double *J, double *dJ_dinlet, double *dJ_damuf, double *dJ_dprsc)
+{
+    RC(check_ctx(x));
+    if (icase < 0 || icase >= x->ncases) return mgfvm_fail(MGFVM_EINVAL, "case %d out of range", icase);
+    if (x->adj_cycles < 0 || (int)x->adj_J.size() != x->ncases)
+        return mgfvm_fail(MGFVM_EINVAL, "mgfvm_adjoint_gradient: no mgfvm_adjoint has run on this context");
+    if (J) *J = x->adj_J[icase];
+    if (dJ_dinlet) std::copy(x->adj_gin[icase].begin(), x->adj_gin[icase].end(), dJ_dinlet);
+    if (dJ_damuf) *dJ_damuf = x->adj_gamuf[icase];
+    if (dJ_dprsc) *dJ_dprsc = x->adj_gprsc[icase];
     return MGFVM_OK;
 }
 

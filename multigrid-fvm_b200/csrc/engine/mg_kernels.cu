@@ -108,6 +108,20 @@ __device__ __forceinline__ void gather_partials(const double *partials, int nblo
     block_sum<NV>(v);
 }
 
+// ---------------------------------------------- programmatic dependent launch
+// The V-cycle's kernels are launched with programmatic stream serialization (when the
+// schedule's `pdl` switch is on), so a kernel's CTAs may be scheduled while its
+// predecessor is still running.  Every kernel therefore starts by waiting until the
+// grids it depends on have completed and their memory is visible (a no-op for a
+// kernel launched without the attribute), and then lets its own dependent launch
+// begin: at most one kernel waits ahead of the running one, and nothing a kernel
+// reads or writes is touched before its predecessors are done.
+__device__ __forceinline__ void pdl_enter()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // ------------------------------------------------------ grid-wide kernels
 #define CASE_PROLOGUE(mode)                          \
     const CaseDev &C = cs[blockIdx.y];               \
@@ -118,6 +132,7 @@ __device__ __forceinline__ void gather_partials(const double *partials, int nblo
 
 __global__ void __launch_bounds__(BLOCK) k_fluxes(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode)
 {
+    pdl_enter();
     CASE_PROLOGUE(mode);
     int i, j;
     if (cell_at(dom_flux(L), t, i, j)) cell_fluxes(L, j * L.npx + i);
@@ -129,6 +144,7 @@ __global__ void __launch_bounds__(BLOCK) k_fluxes(const CaseDev *__restrict__ cs
 template <int LIVE>
 __global__ void __launch_bounds__(BLOCK) k_asm(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode, unsigned what)
 {
+    pdl_enter();
     CASE_PROLOGUE(mode);
     int i, j;
     if (!cell_at(dom_all(L), t, i, j)) return;
@@ -185,6 +201,7 @@ __device__ __forceinline__ void update_cell(const LevelDev &L, const CaseDev &C,
 __global__ void __launch_bounds__(BLOCK) k_update(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode,
                                                   int fuse)
 {
+    pdl_enter();
     CASE_PROLOGUE(mode);
     const Dom d = dom_interior(L);
     const int n = d.wi * d.wj, nx = L.npx;
@@ -208,6 +225,7 @@ __global__ void __launch_bounds__(BLOCK) k_update(const CaseDev *__restrict__ cs
 __global__ void __launch_bounds__(BLOCK) k_mass_coefp(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode, int reduce,
                                                       int from_tmp)
 {
+    pdl_enter();
     CASE_PROLOGUE(mode);
     const Dom d = dom_interior(L);
     const int n = d.wi * d.wj, nb = (n + blockDim.x - 1) / blockDim.x;
@@ -232,6 +250,7 @@ __global__ void __launch_bounds__(BLOCK) k_mass_coefp(const CaseDev *__restrict_
 // source is also a destination.
 __global__ void __launch_bounds__(BLOCK) k_pfix(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode, int phase)
 {
+    pdl_enter();
     CASE_PROLOGUE(mode);
     if (t >= L.ncopy) return;
     double *p = MGF(L, S_P);
@@ -266,6 +285,7 @@ __device__ __forceinline__ void bound_block(const CaseDev &C, const LevelDev &L,
 
 __global__ void __launch_bounds__(BLOCK) k_bound(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode, int bits)
 {
+    pdl_enter();
     const CaseDev &C = cs[blockIdx.y];
     if (!case_active(C, st[blockIdx.y], ig, mode)) return;
     bound_block(C, C.lv[ig], bits);
@@ -277,6 +297,7 @@ __global__ void __launch_bounds__(BLOCK) k_bound(const CaseDev *__restrict__ cs,
 __global__ void __launch_bounds__(PFIX_BOUND_BLOCK) k_pfix_bound(const CaseDev *__restrict__ cs, CaseState *st, int ig,
                                                                  int mode, int bits)
 {
+    pdl_enter();
     const CaseDev &C = cs[blockIdx.y];
     if (!case_active(C, st[blockIdx.y], ig, mode)) return;
     const LevelDev &L = C.lv[ig];
@@ -368,6 +389,7 @@ template <int ISOLVE, int NT>
 __global__ void __launch_bounds__(NT, SMOOTH_BLOCK / NT) k_smooth(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode, int mask, int u0, int nu,
                                                          int dir, int tile)
 {
+    pdl_enter();
     extern __shared__ double sm[];
     const CaseDev &C = cs[blockIdx.y];
     if (!case_active(C, st[blockIdx.y], ig, mode)) return;
@@ -475,6 +497,7 @@ __global__ void __launch_bounds__(NT, SMOOTH_BLOCK / NT)
     k_smooth_tma(const CaseDev *__restrict__ cs, CaseState *st, const SmoothMap *__restrict__ maps, int ig, int mode,
                  int mask, int u0, int nu, int dir, int tile, int bw, int bh, int polls)
 {
+    pdl_enter();
     extern __shared__ __align__(128) double smt[];
     __shared__ __align__(8) unsigned long long mbar;
     const CaseDev &C = cs[blockIdx.y];
@@ -720,6 +743,7 @@ template <int ISOLVE>
 __global__ void __launch_bounds__(SMOOTH_BLOCK, 1) k_pp_level(const CaseDev *__restrict__ cs, CaseState *st, int ig,
                                                               int mode, int nu, int reduce, int fuse)
 {
+    pdl_enter();
     extern __shared__ double sm[];
     const CaseDev &C = cs[blockIdx.y];
     CaseState &ST = st[blockIdx.y];
@@ -747,6 +771,7 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(SMOOTH_BLOCK, 1)
     k_level_visit(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode, int nu, int reduce, int fuse,
                   int what, int mu)
 {
+    pdl_enter();
     extern __shared__ double sm[];
     const CaseDev &C = cs[blockIdx.y];
     CaseState &ST = st[blockIdx.y];
@@ -780,6 +805,7 @@ template <int ISOLVE, int NT>
 __global__ void __launch_bounds__(NT, SMOOTH_BLOCK / NT) k_smooth_mixed(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode, int mask,
                                                                int u0, int nu, int dir, int tile)
 {
+    pdl_enter();
     extern __shared__ double sm[];
     const CaseDev &C = cs[blockIdx.y];
     if (!case_active(C, st[blockIdx.y], ig, mode)) return;
@@ -862,6 +888,7 @@ __global__ void __launch_bounds__(NT, SMOOTH_BLOCK / NT) k_smooth_mixed(const Ca
 // After an odd number of smoothing launches the result sits in the ping-pong buffer.
 __global__ void __launch_bounds__(BLOCK) k_copy(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode, int mask)
 {
+    pdl_enter();
     CASE_PROLOGUE(mode);
     const int e = nth_eq(mask, blockIdx.z);
     const int fs = e == EQ_U ? S_U : e == EQ_V ? S_V : e == EQ_PP ? S_PP : S_SC;
@@ -908,6 +935,7 @@ __device__ __forceinline__ void cell_restrict_fluxes(const LevelDev &F, const Le
 
 __global__ void __launch_bounds__(BLOCK) k_restv_fluxes(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode)
 {
+    pdl_enter();
     CASE_PROLOGUE(mode);
     int i, j;
     if (cell_at(dom_all(L), t, i, j)) cell_restv_fluxes(L, C.lv[ig + 1], C, i, j, blockIdx.z, gridDim.z);
@@ -920,6 +948,7 @@ __global__ void __launch_bounds__(BLOCK) k_restv_fluxes(const CaseDev *__restric
 __global__ void __launch_bounds__(BLOCK) k_restrict(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode,
                                                     unsigned what)
 {
+    pdl_enter();
     CASE_PROLOGUE(mode);
     const LevelDev &K = C.lv[ig + 1];
     int i, j;
@@ -943,6 +972,7 @@ __global__ void __launch_bounds__(BLOCK) k_restrict(const CaseDev *__restrict__ 
 
 __global__ void __launch_bounds__(BLOCK) k_prol_corr(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode)
 {
+    pdl_enter();
     CASE_PROLOGUE(mode);
     const LevelDev &K = C.lv[ig + 1];
     int i, j;
@@ -952,6 +982,7 @@ __global__ void __launch_bounds__(BLOCK) k_prol_corr(const CaseDev *__restrict__
 template <bool FUSED>
 __global__ void __launch_bounds__(BLOCK) k_prol_apply(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode)
 {
+    pdl_enter();
     CASE_PROLOGUE(mode);
     const LevelDev &K = C.lv[ig + 1];
     int i, j;
@@ -1056,6 +1087,7 @@ __device__ __forceinline__ void end_of_cycle(const CaseDev &C, CaseState &ST, in
 
 __global__ void __launch_bounds__(BLOCK) k_endcycle(const CaseDev *__restrict__ cs, CaseState *st)
 {
+    pdl_enter();
     const CaseDev &C = cs[blockIdx.y];
     CaseState &ST = st[blockIdx.y];
     if (ST.done) return;
@@ -1070,6 +1102,7 @@ __global__ void __launch_bounds__(BLOCK) k_endcycle(const CaseDev *__restrict__ 
 template <bool FUSED>
 __global__ void __launch_bounds__(BLOCK) k_prol_apply_end(const CaseDev *__restrict__ cs, CaseState *st, int mode)
 {
+    pdl_enter();
     const int ig = 0;
     CASE_PROLOGUE(mode);
     const Dom d = dom_interior(L);
@@ -1313,6 +1346,7 @@ __device__ void tail_cycle(const X &cx, CaseState &ST, const Sched &S, double *s
 __global__ void __launch_bounds__(TAIL_BLOCK, 1) k_tail(const CaseDev *__restrict__ cs, CaseState *st, Sched S,
                                                         int smem_doubles)
 {
+    pdl_enter();
     extern __shared__ double tsm[];
     const CaseDev &C = cs[blockIdx.x];
     CaseState &ST = st[blockIdx.x];
@@ -1326,6 +1360,7 @@ __global__ void __launch_bounds__(TAIL_BLOCK, 1) k_tail(const CaseDev *__restric
 __global__ void __launch_bounds__(TAIL_BLOCK, 1) k_tail_tan(const CaseDev *__restrict__ cs, CaseState *st,
                                                             const CaseTan *__restrict__ ts, Sched S)
 {
+    pdl_enter();
     const CaseDev &C = cs[blockIdx.x];
     CaseState &ST = st[blockIdx.x];
     if (ST.done || C.tail >= C.ngrid) return;
@@ -1354,31 +1389,51 @@ cudaError_t configure_kernels()
     return e;
 }
 
-template <int ISOLVE>
-static void launch_smooth_tma(const Launch &X, dim3 g, int b, const CaseDev *dc, CaseState *ds, int polls,
-                              cudaStream_t st)
+// Launch `k` on `st`, with programmatic stream serialization when `pdl` (the kernel
+// may then be scheduled while its predecessor runs; it waits in pdl_enter()).
+template <typename... KP, typename... A>
+static cudaError_t launch_k(bool pdl, void (*k)(KP...), dim3 g, int b, int smem, cudaStream_t st, A... args)
 {
-    const SmoothMap *m = (const SmoothMap *)X.ptr;
-    if (b <= SMOOTH_BLOCK / 4)
-        k_smooth_tma<ISOLVE, SMOOTH_BLOCK / 4><<<g, b, X.smem, st>>>(dc, ds, m, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3,
-                                                                     X.a4, X.bw, X.bh, polls);
-    else if (b <= SMOOTH_BLOCK / 2)
-        k_smooth_tma<ISOLVE, SMOOTH_BLOCK / 2><<<g, b, X.smem, st>>>(dc, ds, m, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3,
-                                                                     X.a4, X.bw, X.bh, polls);
-    else
-        k_smooth_tma<ISOLVE, SMOOTH_BLOCK><<<g, b, X.smem, st>>>(dc, ds, m, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3,
-                                                                 X.a4, X.bw, X.bh, polls);
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t c = {};
+    c.gridDim = g;
+    c.blockDim = dim3((unsigned)b, 1, 1);
+    c.dynamicSmemBytes = (size_t)smem;
+    c.stream = st;
+    c.attrs = at;
+    c.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&c, k, static_cast<KP>(args)...);
 }
 
 template <int ISOLVE>
-static void launch_smooth(const Launch &X, dim3 g, int b, const CaseDev *dc, CaseState *ds, cudaStream_t st)
+static cudaError_t launch_smooth_tma(bool pdl, const Launch &X, dim3 g, int b, const CaseDev *dc, CaseState *ds,
+                                     int polls, cudaStream_t st)
 {
+    cudaError_t le;
+    const SmoothMap *m = (const SmoothMap *)X.ptr;
     if (b <= SMOOTH_BLOCK / 4)
-        k_smooth<ISOLVE, SMOOTH_BLOCK / 4><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+        le = launch_k(pdl, k_smooth_tma<ISOLVE, SMOOTH_BLOCK / 4>, g, b, X.smem, st, dc, ds, m, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4, X.bw, X.bh, polls);
     else if (b <= SMOOTH_BLOCK / 2)
-        k_smooth<ISOLVE, SMOOTH_BLOCK / 2><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+        le = launch_k(pdl, k_smooth_tma<ISOLVE, SMOOTH_BLOCK / 2>, g, b, X.smem, st, dc, ds, m, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4, X.bw, X.bh, polls);
     else
-        k_smooth<ISOLVE, SMOOTH_BLOCK><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+        le = launch_k(pdl, k_smooth_tma<ISOLVE, SMOOTH_BLOCK>, g, b, X.smem, st, dc, ds, m, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4, X.bw, X.bh, polls);
+    return le;
+}
+
+template <int ISOLVE>
+static cudaError_t launch_smooth(bool pdl, const Launch &X, dim3 g, int b, const CaseDev *dc, CaseState *ds,
+                                 cudaStream_t st)
+{
+    cudaError_t le;
+    if (b <= SMOOTH_BLOCK / 4)
+        le = launch_k(pdl, k_smooth<ISOLVE, SMOOTH_BLOCK / 4>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+    else if (b <= SMOOTH_BLOCK / 2)
+        le = launch_k(pdl, k_smooth<ISOLVE, SMOOTH_BLOCK / 2>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+    else
+        le = launch_k(pdl, k_smooth<ISOLVE, SMOOTH_BLOCK>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+    return le;
 }
 
 cudaError_t launch_one(const Launch &X, const CaseDev *dc, CaseState *ds, const CaseTan *dt, const Sched &S,
@@ -1386,83 +1441,84 @@ cudaError_t launch_one(const Launch &X, const CaseDev *dc, CaseState *ds, const 
 {
     const dim3 g = X.grid;
     const int b = X.block;
+    const bool pdl = S.pdl;
+    cudaError_t le = cudaSuccess;
     switch (X.kernel) {
-    case K_FLUXES: k_fluxes<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode); break;
+    case K_FLUXES: le = launch_k(pdl, k_fluxes, g, b, 0, st, dc, ds, X.ig, X.mode); break;
     case K_ASM:
-        if (X.a1) k_asm<1><<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, (unsigned)X.a0);
-        else k_asm<0><<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, (unsigned)X.a0);
+        if (X.a1) le = launch_k(pdl, k_asm<1>, g, b, 0, st, dc, ds, X.ig, X.mode, (unsigned)X.a0);
+        else le = launch_k(pdl, k_asm<0>, g, b, 0, st, dc, ds, X.ig, X.mode, (unsigned)X.a0);
         break;
-    case K_MASS_COEFP: k_mass_coefp<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1); break;
-    case K_UPDATE: k_update<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, X.a0); break;
-    case K_PFIX: k_pfix<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, X.a0); break;
-    case K_BOUND: k_bound<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, X.a0); break;
+    case K_MASS_COEFP: le = launch_k(pdl, k_mass_coefp, g, b, 0, st, dc, ds, X.ig, X.mode, X.a0, X.a1); break;
+    case K_UPDATE: le = launch_k(pdl, k_update, g, b, 0, st, dc, ds, X.ig, X.mode, X.a0); break;
+    case K_PFIX: le = launch_k(pdl, k_pfix, g, b, 0, st, dc, ds, X.ig, X.mode, X.a0); break;
+    case K_BOUND: le = launch_k(pdl, k_bound, g, b, 0, st, dc, ds, X.ig, X.mode, X.a0); break;
     case K_SMOOTH:
         if (b > SMOOTH_BLOCK) return cudaErrorInvalidValue;
         if (S.isolve == MGFVM_JACOBI)
-            launch_smooth<MGFVM_JACOBI>(X, g, b, dc, ds, st);
+            le = launch_smooth<MGFVM_JACOBI>(pdl, X, g, b, dc, ds, st);
         else
-            launch_smooth<MGFVM_GAUSS_SEIDEL>(X, g, b, dc, ds, st);
+            le = launch_smooth<MGFVM_GAUSS_SEIDEL>(pdl, X, g, b, dc, ds, st);
         break;
     case K_SMOOTH_MIXED:
         if (b > SMOOTH_BLOCK) return cudaErrorInvalidValue;
         if (S.isolve == MGFVM_JACOBI) {
             if (b <= SMOOTH_BLOCK / 4)
-                k_smooth_mixed<MGFVM_JACOBI, SMOOTH_BLOCK / 4><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+                le = launch_k(pdl, k_smooth_mixed<MGFVM_JACOBI, SMOOTH_BLOCK / 4>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
             else if (b <= SMOOTH_BLOCK / 2)
-                k_smooth_mixed<MGFVM_JACOBI, SMOOTH_BLOCK / 2><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+                le = launch_k(pdl, k_smooth_mixed<MGFVM_JACOBI, SMOOTH_BLOCK / 2>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
             else
-                k_smooth_mixed<MGFVM_JACOBI, SMOOTH_BLOCK><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+                le = launch_k(pdl, k_smooth_mixed<MGFVM_JACOBI, SMOOTH_BLOCK>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
         } else {
             if (b <= SMOOTH_BLOCK / 4)
-                k_smooth_mixed<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK / 4><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+                le = launch_k(pdl, k_smooth_mixed<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK / 4>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
             else if (b <= SMOOTH_BLOCK / 2)
-                k_smooth_mixed<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK / 2><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+                le = launch_k(pdl, k_smooth_mixed<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK / 2>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
             else
-                k_smooth_mixed<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+                le = launch_k(pdl, k_smooth_mixed<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
         }
         break;
-    case K_COPY: k_copy<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, X.a0); break;
+    case K_COPY: le = launch_k(pdl, k_copy, g, b, 0, st, dc, ds, X.ig, X.mode, X.a0); break;
     case K_SMOOTH_TMA:
         if (b > SMOOTH_BLOCK || !X.ptr || X.smem > SMOOTH_TMA_SMEM_MAX || (X.bw & 1)) return cudaErrorInvalidValue;
-        if (S.isolve == MGFVM_JACOBI) launch_smooth_tma<MGFVM_JACOBI>(X, g, b, dc, ds, S.tma_wait_polls, st);
-        else launch_smooth_tma<MGFVM_GAUSS_SEIDEL>(X, g, b, dc, ds, S.tma_wait_polls, st);
+        if (S.isolve == MGFVM_JACOBI) le = launch_smooth_tma<MGFVM_JACOBI>(pdl, X, g, b, dc, ds, S.tma_wait_polls, st);
+        else le = launch_smooth_tma<MGFVM_GAUSS_SEIDEL>(pdl, X, g, b, dc, ds, S.tma_wait_polls, st);
         break;
     case K_PP_LEVEL:
         if (b > SMOOTH_BLOCK) return cudaErrorInvalidValue;
         if (S.isolve == MGFVM_JACOBI)
-            k_pp_level<MGFVM_JACOBI><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2);
+            le = launch_k(pdl, k_pp_level<MGFVM_JACOBI>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2);
         else
-            k_pp_level<MGFVM_GAUSS_SEIDEL><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2);
+            le = launch_k(pdl, k_pp_level<MGFVM_GAUSS_SEIDEL>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2);
         break;
     case K_LEVEL_VISIT:
         if (b > SMOOTH_BLOCK || g.x != 3) return cudaErrorInvalidValue;
         if (S.isolve == MGFVM_JACOBI)
-            k_level_visit<MGFVM_JACOBI><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+            le = launch_k(pdl, k_level_visit<MGFVM_JACOBI>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
         else
-            k_level_visit<MGFVM_GAUSS_SEIDEL><<<g, b, X.smem, st>>>(dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3,
-                                                                     X.a4);
+            le = launch_k(pdl, k_level_visit<MGFVM_GAUSS_SEIDEL>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
         break;
-    case K_PFIX_BOUND: k_pfix_bound<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, X.a0); break;
-    case K_RESTV_FLUXES: k_restv_fluxes<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode); break;
-    case K_RESTRICT: k_restrict<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode, (unsigned)X.a0); break;
-    case K_PROL_CORR: k_prol_corr<<<g, b, 0, st>>>(dc, ds, X.ig, X.mode); break;
+    case K_PFIX_BOUND: le = launch_k(pdl, k_pfix_bound, g, b, 0, st, dc, ds, X.ig, X.mode, X.a0); break;
+    case K_RESTV_FLUXES: le = launch_k(pdl, k_restv_fluxes, g, b, 0, st, dc, ds, X.ig, X.mode); break;
+    case K_RESTRICT: le = launch_k(pdl, k_restrict, g, b, 0, st, dc, ds, X.ig, X.mode, (unsigned)X.a0); break;
+    case K_PROL_CORR: le = launch_k(pdl, k_prol_corr, g, b, 0, st, dc, ds, X.ig, X.mode); break;
     case K_PROL_APPLY:
-        if (X.a0) k_prol_apply<true><<<g, b, 0, st>>>(dc, ds, X.ig, X.mode);
-        else k_prol_apply<false><<<g, b, 0, st>>>(dc, ds, X.ig, X.mode);
+        if (X.a0) le = launch_k(pdl, k_prol_apply<true>, g, b, 0, st, dc, ds, X.ig, X.mode);
+        else le = launch_k(pdl, k_prol_apply<false>, g, b, 0, st, dc, ds, X.ig, X.mode);
         break;
-    case K_TAIL: k_tail<<<g, b, X.smem, st>>>(dc, ds, S, X.smem / (int)sizeof(double)); break;
+    case K_TAIL: le = launch_k(pdl, k_tail, g, b, X.smem, st, dc, ds, S, X.smem / (int)sizeof(double)); break;
     case K_TAIL_TAN:
         if (!dt) return cudaErrorInvalidValue;
-        k_tail_tan<<<g, b, 0, st>>>(dc, ds, dt, S);
+        le = launch_k(pdl, k_tail_tan, g, b, 0, st, dc, ds, dt, S);
         break;
-    case K_ENDCYCLE: k_endcycle<<<g, b, 0, st>>>(dc, ds); break;
+    case K_ENDCYCLE: le = launch_k(pdl, k_endcycle, g, b, 0, st, dc, ds); break;
     case K_PROL_APPLY_END:
-        if (X.a0) k_prol_apply_end<true><<<g, b, 0, st>>>(dc, ds, X.mode);
-        else k_prol_apply_end<false><<<g, b, 0, st>>>(dc, ds, X.mode);
+        if (X.a0) le = launch_k(pdl, k_prol_apply_end<true>, g, b, 0, st, dc, ds, X.mode);
+        else le = launch_k(pdl, k_prol_apply_end<false>, g, b, 0, st, dc, ds, X.mode);
         break;
     default: return cudaErrorInvalidValue;
     }
-    return cudaGetLastError();
+    return le != cudaSuccess ? le : cudaGetLastError();
 }
 
 // ----------------------------------------------- raw-pointer entry points

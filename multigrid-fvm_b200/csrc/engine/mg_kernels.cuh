@@ -58,6 +58,7 @@ constexpr int TMA_WAIT_POLLS = 1 << 22;
 struct Sched {
     int isolve, nswpm, nswpp;
     int tma_wait_polls;   // first wait of a TMA-staged smoother CTA (mgfvm_tuning.tma_first_wait)
+    bool pdl;             // launch with programmatic stream serialization (mgfvm_tuning.pdl)
 };
 
 // Tile smoother geometry: a CTA of SMOOTH_BLOCK (one per SM) or SMOOTH_BLOCK/2 (two per

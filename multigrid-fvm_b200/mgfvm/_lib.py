@@ -87,6 +87,8 @@ def lib() -> C.CDLL:
         "mgfvm_get_tangent": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _dp]),
         "mgfvm_objective": (C.c_int, [_vp, C.c_int, _dp, _dp]),
         "mgfvm_gradient": (C.c_int, [C.POINTER(_abi.Config), _dp, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _dp]),
+        "mgfvm_adjoint": (C.c_int, [_vp, C.c_int]),
+        "mgfvm_adjoint_gradient": (C.c_int, [_vp, C.c_int, _dp, _dp, _dp, _dp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

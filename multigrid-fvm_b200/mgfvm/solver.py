@@ -279,6 +279,20 @@ class Solver:
         check(self._lib.mgfvm_objective(self._h, case, C.byref(j), C.byref(d) if tan else None))
         return j.value, (d.value if tan else None)
 
+    def adjoint(self, cycles: int) -> None:
+        """Reverse mode (mgfvm_adjoint): every case restarts from its initial state, runs
+        `cycles` V-cycles, and the transposed cycles carry the adjoint of J back to the
+        inputs.  Read the result with adjoint_gradient(case)."""
+        check(self._lib.mgfvm_adjoint(self._h, int(cycles)))
+
+    def adjoint_gradient(self, case: int = 0) -> Tuple[float, np.ndarray, float, float]:
+        """(J, dJ/dinlet (nfy values), dJ/damuf, dJ/dprsc) of the last adjoint run."""
+        g_in = np.zeros(int(self.cases[case].nfy))
+        j, ga, gp = C.c_double(), C.c_double(), C.c_double()
+        check(self._lib.mgfvm_adjoint_gradient(self._h, case, C.byref(j), g_in.ctypes.data_as(_dp), C.byref(ga),
+                                               C.byref(gp)))
+        return j.value, g_in, ga.value, gp.value
+
     @property
     def transfer_bytes(self) -> Tuple[int, int]:
         """(host->device, device->host) bytes copied by this context so far."""

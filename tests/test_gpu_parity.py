@@ -192,6 +192,8 @@ TUNINGS = [
     {"smooth_tma": [2, 2, 2], "smooth_units": [7, 1, 4], "smooth_threads": [256, 512, 512], "odd_chunks": [1, 1, 1]},
     {"coarse_kernel": [0, 0, 2]},
     {"coarse_kernel": [0, 2, 2], "smooth_units": [4, 0, 0]},
+    {"pdl": 1},
+    {"pdl": 1, "smooth_tma": [2, 2, 2], "coarse_kernel": [0, 0, 2]},
 ]
 
 
@@ -226,7 +228,7 @@ def test_autotune_keeps_state(oracle_built):
     before, after, chosen = s.autotune(2)
     assert before > 0 and 0 < after <= before
     assert set(chosen) == {"smooth_units", "smooth_threads", "asm_slices", "restrict_slices", "update_pfix", "odd_chunks", "pp_level",
-                           "smooth_tma", "coarse_kernel", "prol_fused", "tma_first_wait"}
+                           "smooth_tma", "coarse_kernel", "prol_fused", "tma_first_wait", "pdl"}
     _compare(s, o, STATE, what="after autotune")
     s.cycle(3)
     o.cycle(3)
