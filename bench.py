@@ -297,14 +297,15 @@ def mixed_solve(cases, device, ref_solver, tune, profiles=None):
         ms = s.last_elapsed_ms
         bad = set(s.diverged()) | set(ref_solver.diverged())
         fields = [{f: s.field(k, 0, f) for f in ("u", "v", "p", "sc")} for k in range(len(cases))]
-        err = 0.0
-        for k in range(len(cases)):
-            if k in bad:
-                continue
-            err = max(err, field_errors(fields[k], {f: ref_solver.field(k, 0, f) for f in ("u", "v", "p", "sc")}))
+        per_case = [None if k in bad else
+                    field_errors(fields[k], {f: ref_solver.field(k, 0, f) for f in ("u", "v", "p", "sc")})
+                    for k in range(len(cases))]
+        err = max([e for e in per_case if e is not None], default=0.0)
     return {"value": round((len(cases) - len(bad)) / (ms / 1e3), 4), "unit": "solves/s", "ms_per_step": round(ms, 3),
             "rel_l2_vs_fp64_solve": err, "diverged": len(bad),
-            "form": "smoothers iterate an FP32 correction against FP64 residuals; the rest FP64"}, fields, bad
+            "form": "levels smoothed in tiles keep FP32 smoother operands (aw, ae, as, an, 1/ap and the FP64 "
+                    "residual, stored by the FP64 assembly) and iterate an FP32 correction; p' in FP32; "
+                    "transfers, defects, norms and the one-CTA levels FP64"}, fields, bad, per_case
 
 
 # --------------------------------------------------------------- clocks
@@ -482,6 +483,10 @@ def main():
     ap.add_argument("--batch", type=int, default=64,
                     help="cases of the batched obstacle-flow measurement (0: skip it)")
     ap.add_argument("--no-gradient", action="store_true", help="skip the gradient measurements")
+    ap.add_argument("--parity-dump", default=None,
+                    help="write per-case hashes of the timed solve's final level-0 fields, the cycles each case "
+                         "ran and the mixed form's distance to them to this JSON file (oracle/config_parity.py "
+                         "compares them with the oracle)")
     ap.add_argument("--profile-cycles", type=int, default=0,
                     help="only run 3 warm-up V-cycles then this many V-cycles of the workload "
                          "(for ncu launch lists) and exit")
@@ -615,6 +620,11 @@ def main():
     # the timed solve's final level-0 fields (later measurements change the state)
     gpu_fields = [{f: solver.field(k, 0, f) for f in ("u", "v", "p", "sc")} for k in range(n_cases)] \
         if parity_jobs is not None else None
+    gpu_hashes = None
+    if a.parity_dump:
+        import hashlib
+        gpu_hashes = [hashlib.sha256(b"".join(np.ascontiguousarray(solver.field(k, 0, f)).tobytes()
+                                              for f in ("u", "v", "p", "sc"))).hexdigest() for k in range(n_cases)]
     if world > 1:
         t = torch.tensor([ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -676,7 +686,8 @@ def main():
     mixed = mixed_fields = None
     mixed_bad = set()
     if world == 1:
-        mixed, mixed_fields, mixed_bad = mixed_solve(cases, local, solver, tuned is not None, profiles)
+        mixed, mixed_fields, mixed_bad, mixed_per_case = mixed_solve(cases, local, solver, tuned is not None,
+                                                                      profiles)
 
     # ---- batched throughput: many obstacle-flow cases in one context
     batched = None
@@ -688,6 +699,15 @@ def main():
     if world == 1 and not a.no_gradient:
         grad = gradient_rate(local, check=not a.no_cpu_baseline)
         adj = adjoint_rate(local, check=not a.no_cpu_baseline)
+
+    if a.parity_dump and rank == 0:
+        dump = {"workload": a.workload, "cases": []}
+        for k in range(n_cases):
+            dump["cases"].append({"cycles": int(cycles_per_solve[k]), "diverged": k in diverged,
+                                  "sha256": gpu_hashes[k],
+                                  "mixed_rel_l2_vs_fp64": None if mixed_fields is None else mixed_per_case[k]})
+        with open(a.parity_dump, "w") as f:
+            json.dump(dump, f)
 
     # ---- parity of the timed solve against the CPU oracle's run of the same cycles
     parity = None

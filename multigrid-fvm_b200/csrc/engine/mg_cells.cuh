@@ -246,7 +246,9 @@ __device__ __forceinline__ void cell_sc(const IO &io, const CaseDev &C, const F 
 
 // The three assemblies that depend only on the fluxes at the start of a level
 // visit, plus those fluxes, at cell (i, j) of the full padded array.
-enum AsmBits { A_FLUX = 1, A_U = 2, A_V = 4, A_SC = 8, A_SC_OUTFLOW = 16 };
+enum AsmBits { A_FLUX = 1, A_U = 2, A_V = 4, A_SC = 8, A_SC_OUTFLOW = 16,
+               A_F32 = 32,    // mixed precision: store the equations' FP32 smoother operands (mg_kernels.cu)
+               A_JAC = 64 };  // with A_F32: the smoother is Jacobi (divisor ap + 1e-30)
 
 // The part of `what` thread slice z of 3 does when a launch spreads the assemblies
 // over blockIdx.z (slice 0: fluxes and u, 1: v, 2: scalar and its outflow ghost).
@@ -254,7 +256,7 @@ __host__ __device__ __forceinline__ unsigned asm_slice(unsigned what, int z, int
 {
     if (nz <= 1) return what;
     const unsigned part[3] = {A_FLUX | A_U, A_V, A_SC | A_SC_OUTFLOW};
-    return what & part[z];
+    return (what & part[z]) | (what & (unsigned)(A_F32 | A_JAC));
 }
 template <class IO, class F>
 __device__ __forceinline__ void cell_asm_io(const IO &io, const CaseDev &C, const F &fl, int i, int j, unsigned what)

@@ -229,6 +229,16 @@ struct Builder {
     // cap each, alternating field -> buffer -> field (a single launch copies back).
     // `tmp_ok`: the next kernel can take the result from the ping-pong buffers, so an
     // odd number of tile launches needs no copy back.  Returns whether it is left there.
+    // Mixed precision runs on the V-cycle's levels smoothed in tiles, every level but
+    // the coarsest (a whole level one CTA holds stays FP64: its visits are latency-bound
+    // single launches): FP32 operands and corrections (k_smooth_f32).
+    bool f32_level(int ig, int mode) const
+    {
+        int mx, my;
+        return x->opt.precision == MGFVM_PREC_MIXED && mode != M_OP && ig < min_ngrid() - 1 &&
+               !whole_level(ig, mx, my);
+    }
+    int f32_buf = 0;   // the FP32 correction buffer the last F32 smoothing call ended in
     bool smooth(int ig, int mode, int mask, int nsw, bool tmp_ok = false)
     {
         const int isolve = x->sched.isolve;
@@ -236,13 +246,33 @@ struct Builder {
         if (units <= 0 || (isolve != MGFVM_JACOBI && isolve != MGFVM_GAUSS_SEIDEL)) return false;
         const int neq = __builtin_popcount((unsigned)mask);
         const int bufs = isolve == MGFVM_JACOBI ? 2 : 1;
-        // mixed precision: FP32 correction smoothing on every level but the coarsest
-        const bool mixed = x->opt.precision == MGFVM_PREC_MIXED && ig < min_ngrid() - 1;
-        const int kern = mixed ? K_SMOOTH_MIXED : K_SMOOTH;
-        auto smem_for = [&](int cells) {
-            return mixed ? cells * (int)sizeof(double) + bufs * cells * (int)sizeof(float)
-                         : bufs * cells * (int)sizeof(double);
-        };
+        const int kern = K_SMOOTH;
+        auto smem_for = [&](int cells) { return bufs * cells * (int)sizeof(double); };
+        if (f32_level(ig, mode)) {
+            // launches of at most the level's cap of units; the correction passes between
+            // them in FP32 and the last adds it to the field, so any count works
+            const int tt = x->tune.smooth_threads[ig];
+            const int nt = tt == SMOOTH_BLOCK / 2 || tt == SMOOTH_BLOCK / 4 ? tt : SMOOTH_BLOCK;
+            const int most = (smooth_pairs_side(0, nt) - MIN_TILE) / 2;
+            const int cap = std::min(most, x->tune.smooth_units[ig] > 0 ? x->tune.smooth_units[ig] : MAX_UNITS);
+            const int chunks = (units + cap - 1) / cap;
+            const int hmax = (units + chunks - 1) / chunks;
+            const int tile = smooth_pairs_side(hmax, nt);
+            const int side = tile + 2 * hmax;
+            int u0 = 0;
+            for (int c = 0; c < chunks; ++c) {
+                const int nu = units / chunks + (c < units % chunks ? 1 : 0);
+                const int flags = (c == 0 ? 1 : 0) | (c == chunks - 1 ? 2 : 0) | ((c & 1) ? 4 : 0);
+                Launch &L = add(K_SMOOTH_F32, ig, mode, 0, mask, u0, nu, flags);
+                L.a4 = tile;
+                L.grid = dim3((unsigned)tiles(ig, tile), x->ncases, neq);
+                L.block = std::min(nt, round32(side * ((side + 1) / 2)));
+                L.smem = bufs * side * side * (int)sizeof(float);
+                u0 += nu;
+            }
+            f32_buf = chunks & 1;
+            return false;
+        }
         int mx, my;
         if (whole_level(ig, mx, my)) {
             Launch &L = add(kern, ig, mode, 0, mask, 0, units, 2);
@@ -336,9 +366,13 @@ struct Builder {
     // `uvsc_in_tmp`: the preceding u, v, sc smoothing left its results in the buffers
     int solve_pp(int ig, int mode, bool reduce, int fuse, int bound_bits = 0, bool uvsc_in_tmp = false)
     {
-        add(K_MASS_COEFP, ig, mode, cells(ig), reduce ? 1 : 0, uvsc_in_tmp ? 1 : 0);
+        // mixed precision: p' operands and p' itself in FP32 (p' needs a smoothing to be set)
+        const bool f32 = f32_level(ig, mode) && x->sched.nswpp > 0;
+        const int jac = x->sched.isolve == MGFVM_JACOBI ? 4 : 0;
+        add(K_MASS_COEFP, ig, mode, cells(ig), reduce ? 1 : 0, (uvsc_in_tmp ? 1 : 0) | (f32 ? 2 | jac : 0));
         const bool chain = mode != M_OP && x->tune.odd_chunks[ig] != 1;
         if (smooth(ig, mode, 1 << EQ_PP, x->sched.nswpp, chain)) fuse |= 8;
+        if (f32) fuse |= 16 | (f32_buf ? 32 : 0);
         add(K_UPDATE, ig, mode, cells(ig) + 2, fuse);
         return after_update(ig, mode, fuse, bound_bits);
     }
@@ -379,14 +413,20 @@ struct Builder {
     // Assembly and restriction run one thread per (cell, equation) — 3 slices, each
     // with a third of the dependent loads — unless tuned to one thread per cell.
     static int slices(int, int knob) { return knob == 1 ? 1 : 3; }
+    // the assembly bits of a down-leg (or up-leg) step on level ig, with the FP32
+    // operands of a mixed-precision level
+    int asm_what(int ig, int mode, bool down) const
+    {
+        if (!f32_level(ig, mode)) return asm_bits(down);
+        return asm_bits(down) | A_F32 | (x->sched.isolve == MGFVM_JACOBI ? A_JAC : 0);
+    }
     void step(int ig, int mode, bool down, bool reduce, bool asm_done = false)
     {
         int mx, my;
-        const bool mixed = x->opt.precision == MGFVM_PREC_MIXED && ig < min_ngrid() - 1;
         const int isolve = x->sched.isolve;
         const int ppu = isolve == MGFVM_GAUSS_SEIDEL ? 2 * x->sched.nswpp : x->sched.nswpp;
         const int mu = isolve == MGFVM_GAUSS_SEIDEL ? 2 * x->sched.nswpm : x->sched.nswpm;
-        if (mode != M_OP && !mixed && ppu > 0 && x->tune.pp_level[ig] != 1 &&
+        if (mode != M_OP && ppu > 0 && x->tune.pp_level[ig] != 1 &&
             (isolve == MGFVM_JACOBI || isolve == MGFVM_GAUSS_SEIDEL) && whole_level(ig, mx, my)) {
             // the whole visit (assembly, u/v/sc smoothing, p' and update) in one launch
             const bool pfx = pfix_fusable(ig, mode);
@@ -403,7 +443,7 @@ struct Builder {
             return;
         }
         if (!asm_done) {
-            Launch &L = add(K_ASM, ig, mode, cells(ig), asm_bits(down), 1);
+            Launch &L = add(K_ASM, ig, mode, cells(ig), asm_what(ig, mode, down), 1);
             L.grid.z = slices(ig, x->tune.asm_slices[ig]);
         }
         const bool in_tmp = smooth(ig, mode, (1 << EQ_U) | (1 << EQ_V) | (1 << EQ_SC), x->sched.nswpm,
@@ -418,7 +458,7 @@ struct Builder {
     {
         const int z = slices(ig, x->tune.restrict_slices[ig]);
         add(K_RESTV_FLUXES, ig, mode_f, cells(ig)).grid.z = z;
-        Launch &L = add(K_RESTRICT, ig, mode_f, cells(ig + 1), coarse_asm ? asm_bits(true) : 0);
+        Launch &L = add(K_RESTRICT, ig, mode_f, cells(ig + 1), coarse_asm ? asm_what(ig + 1, M_DOWN, true) : 0);
         L.grid.z = z;
     }
     // :230-233

@@ -138,6 +138,93 @@ __global__ void __launch_bounds__(BLOCK) k_fluxes(const CaseDev *__restrict__ cs
     if (cell_at(dom_flux(L), t, i, j)) cell_fluxes(L, j * L.npx + i);
 }
 
+// ------------------------------------------------ mixed precision: FP32 operands
+// In a mixed-precision context the levels smoothed in tiles keep their smoother
+// operands in FP32.  The assembly forms each equation's coefficients in FP64 with the
+// same routines, then the FP64 residual of the current field, r = su + sum a_nb phi_nb
+// - ap phi (the outer defect), and stores aw, ae, as, an, 1/ap and r as floats in the
+// first halves of the equation's six coefficient arrays.  The smoother iterates the
+// correction delta of A (phi + delta) = b in FP32 from zero, keeping delta between
+// launches in two FP32 ping-pong buffers (the halves of the equation's buffer array),
+// and its last launch adds delta to the FP64 field.  p' starts at zero, so its
+// correction is p' itself: masserror + coefp store its operands (r = su) and update
+// reads the FP32 p'.  The restriction, prolongation, norms and the coarse levels one
+// CTA holds stay FP64.
+__device__ __forceinline__ float *op32(const LevelDev &L, int e, int k)
+{
+    return reinterpret_cast<float *>(L.f[co_slot(e, k)]);
+}
+__device__ __forceinline__ float *del32(const LevelDev &L, int e, int buf)
+{
+    return reinterpret_cast<float *>(L.f[eq_tmp(e)]) + (size_t)buf * L.npx * L.npy;
+}
+
+// Prim whose stores of equation e's coefficient set (aw .. su) land in `k` instead of
+// the arrays; every other store goes to the arrays.
+struct Capture {
+    using T = double;
+    const LevelDev &L;
+    int e;
+    double *k;
+    __device__ __forceinline__ double ld(int s, int q) const { return L.f[s][q]; }
+    __device__ __forceinline__ void st(int s, int q, double v) const
+    {
+        const int c = s - co_slot(e, 0);
+        if (c >= 0 && c < NCOEF) k[c] = v;
+        else L.f[s][q] = v;
+    }
+    __device__ __forceinline__ double g(int s, int q) const { return L.f[s][q]; }
+    __device__ __forceinline__ double amu() const { return L.amu; }
+    __device__ __forceinline__ double amusc() const { return L.amusc; }
+    __device__ __forceinline__ double pb(int i) const { return L.pbuf[i]; }
+    __device__ __forceinline__ void set_pb(int i, double v) const { L.pbuf[i] = v; }
+};
+
+// The FP32 operands of equation e at cell q from its FP64 coefficients k (aw .. su)
+// and field values phi (centre), pe (east; the caller knows when outflow moves it).
+__device__ __forceinline__ void store_ops32(const LevelDev &L, int e, int q, const double *k, bool jac, double pe)
+{
+    const double *phi = L.f[eq_field(e)];
+    const int nx = L.npx;
+    const double ap = jac ? k[CK_AP] + 1.0e-30 : k[CK_AP];
+    const double nb = k[CK_AW] * phi[q - 1] + k[CK_AE] * pe + k[CK_AS] * phi[q - nx] + k[CK_AN] * phi[q + nx];
+    const double r = (nb + k[CK_SU]) - ap * phi[q];
+    op32(L, e, CK_AW)[q] = (float)k[CK_AW];
+    op32(L, e, CK_AE)[q] = (float)k[CK_AE];
+    op32(L, e, CK_AS)[q] = (float)k[CK_AS];
+    op32(L, e, CK_AN)[q] = (float)k[CK_AN];
+    op32(L, e, CK_AP)[q] = (float)(1.0 / ap);
+    op32(L, e, CK_SU)[q] = (float)r;
+}
+
+// cell_asm with A_F32: the same assemblies, FP32 operands stored instead of the FP64
+// coefficient sets (APU, APV, the fluxes and the scalar ghost as before).  `sc_out`:
+// the scalar's outflow ghost is (being) set from the cell west of it in this launch,
+// so that cell's east value is its own.
+__device__ __forceinline__ void cell_asm_f32(const LevelDev &L, const CaseDev &C, int i, int j, unsigned what,
+                                             bool sc_out)
+{
+    const int nx = L.npx, ny = L.npy, q = j * nx + i;
+    const FluxLive fl(L);
+    const bool jac = (what & A_JAC) != 0;
+    if ((what & A_FLUX) && i <= nx - 2 && j <= ny - 2) cell_fluxes(L, q);
+    const bool in = i >= 1 && j >= 1 && i <= nx - 2 && j <= ny - 2;
+    double k[NCOEF];
+    if ((what & A_U) && in && i <= nx - 3) {
+        cell_mom_u(Capture{L, EQ_U, k}, C, fl, i, j);
+        store_ops32(L, EQ_U, q, k, jac, L.f[S_U][q + 1]);
+    }
+    if ((what & A_V) && in && j <= ny - 3) {
+        cell_mom_v(Capture{L, EQ_V, k}, C, fl, i, j);
+        store_ops32(L, EQ_V, q, k, jac, L.f[S_V][q + 1]);
+    }
+    if ((what & A_SC) && in) {
+        cell_sc(Capture{L, EQ_SC, k}, C, fl, i, j);
+        store_ops32(L, EQ_SC, q, k, jac, sc_out && i == nx - 2 ? L.f[S_SC][q] : L.f[S_SC][q + 1]);
+    }
+    if ((what & A_SC_OUTFLOW) && i == nx - 1 && C.ibc_xp == 4) L.f[S_SC][q] = L.f[S_SC][q - 1];
+}
+
 // Fused assembly over the padded array: fluxes, coefu+umom, coefv+vmom,
 // coefsc+scalar, the scalar outflow ghost (AsmBits).  LIVE recomputes the fluxes
 // from u, v (valid at the start of a level visit, before any of them changes).
@@ -149,13 +236,15 @@ __global__ void __launch_bounds__(BLOCK) k_asm(const CaseDev *__restrict__ cs, C
     int i, j;
     if (!cell_at(dom_all(L), t, i, j)) return;
     const unsigned w = asm_slice(what, blockIdx.z, gridDim.z);
-    if (LIVE) cell_asm(L, C, FluxLive(L), i, j, w);
+    if (w & A_F32) cell_asm_f32(L, C, i, j, w, (w & A_SC_OUTFLOW) && C.ibc_xp == 4);
+    else if (LIVE) cell_asm(L, C, FluxLive(L), i, j, w);
     else cell_asm(L, C, FluxArrays(L), i, j, w);
 }
 
 // update :1127-1152; with `fuse` bit 1 also outflow :1211-1228 of u, v, p (bit 2: and
 // sc), with bit 4 also update's obstacle pressure copy (:1153-1177); bit 8: p' is in its
-// ping-pong buffer (an odd number of smoother launches), read from there and copied back.  The copy gives
+// ping-pong buffer (an odd number of smoother launches), read from there and copied back;
+// bit 16: mixed precision, p' is the FP32 correction in buffer (bit 32 ? 1 : 0).  The copy gives
 // every destination the post-update pressure of its source; each is written by one
 // thread, the one updating the source (or, for a source on the boundary ring, the
 // nearest interior cell, which reads it before writing anything), and destinations
@@ -209,6 +298,11 @@ __global__ void __launch_bounds__(BLOCK) k_update(const CaseDev *__restrict__ cs
     int i, j;
     if (cell_at(d, t, i, j)) {
         const int q = j * nx + i;
+        if (fuse & 16) {   // mixed precision: p' is FP32, in buffer (fuse & 32 ? 1 : 0) of its correction
+            const float *pf = del32(L, EQ_PP, (fuse & 32) ? 1 : 0);
+            update_cell(L, C, i, j, (double)pf[q], (double)pf[q + 1], (double)pf[q + nx], out, fuse);
+            return;
+        }
         const double *pp = MGF(L, (fuse & 8) ? S_TMP0 : S_PP);
         const double ppq = pp[q];
         if (fuse & 8) MGF(L, S_PP)[q] = ppq;
@@ -220,10 +314,12 @@ __global__ void __launch_bounds__(BLOCK) k_update(const CaseDev *__restrict__ cs
 }
 
 // masserror + coefp; with `reduce`, sum|div| of this level lands in C.last_err.
-// `from_tmp`: u, v, sc are in their ping-pong buffers (an odd number of smoother
-// launches); read from there and copied back.
+// `flags` bit 1: u, v, sc are in their ping-pong buffers (an odd number of smoother
+// launches); read from there and copied back.  Bit 2: mixed precision, p' operands
+// stored in FP32 (r = su, as p' starts from zero; p' itself is not written); bit 4:
+// with bit 2, the smoother is Jacobi.
 __global__ void __launch_bounds__(BLOCK) k_mass_coefp(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode, int reduce,
-                                                      int from_tmp)
+                                                      int flags)
 {
     pdl_enter();
     CASE_PROLOGUE(mode);
@@ -232,7 +328,23 @@ __global__ void __launch_bounds__(BLOCK) k_mass_coefp(const CaseDev *__restrict_
     if ((int)blockIdx.x >= nb) return;
     double a[1] = {0.0};
     int i, j;
-    if (cell_at(d, t, i, j)) a[0] = cell_mass_coefp(L, C, i, j, from_tmp != 0);
+    if (cell_at(d, t, i, j)) {
+        if (flags & 2) {
+            Coef k;
+            double su;
+            a[0] = mass_coefp_values(L, C, i, j, k, su, S_U, S_V);
+            const int q = j * L.npx + i;
+            const double ap = (flags & 4) ? k.ap + 1.0e-30 : k.ap;
+            op32(L, EQ_PP, CK_AW)[q] = (float)k.aw;
+            op32(L, EQ_PP, CK_AE)[q] = (float)k.ae;
+            op32(L, EQ_PP, CK_AS)[q] = (float)k.as;
+            op32(L, EQ_PP, CK_AN)[q] = (float)k.an;
+            op32(L, EQ_PP, CK_AP)[q] = (float)(1.0 / ap);
+            op32(L, EQ_PP, CK_SU)[q] = (float)su;
+        } else {
+            a[0] = cell_mass_coefp(L, C, i, j, (flags & 1) != 0);
+        }
+    }
     if (!reduce) return;
     block_sum<1>(a);
     if (publish_partials<1>(C.partials, &C.counters[0], a, nb)) {
@@ -793,20 +905,19 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(SMOOTH_BLOCK, 1)
     if (active && r == 0) pp_level_body<ISOLVE>(C, ST, L, nu, reduce, fuse, sm);
 }
 
-// Mixed-precision variant (MGFVM_PREC_MIXED): the same tiles, units and windows, run
-// on the correction delta of A (phi + delta) = b in FP32.  The residual r = su +
-// sum a_nb phi_nb - ap phi_P is taken in FP64 from the staged field at the start of
-// every launch (so a smoothing call of several launches refreshes it in FP64); the
-// units then update delta_P = (sum a_nb delta_nb + r) / ap in FP32, dividing by a
-// reciprocal taken once, and the tile is written back as phi + delta.  A fixed point
-// of the V-cycle is therefore one of the FP64 equations: delta vanishes only where the
-// FP64 residual does.
+// Mixed precision (MGFVM_PREC_MIXED): the tiles, units and windows of k_smooth on
+// the FP32 operands the assembly stored (aw, ae, as, an, 1/ap, r; see op32), iterating
+// the correction delta_P = (sum a_nb delta_nb + r) / ap in FP32.  `flags` bit 1: the
+// first launch of the call (delta starts at zero), bit 2: the last (the field gets
+// phi + delta in FP64; p' keeps delta, which is p' itself), bit 4: delta is read from
+// buffer 1 and written to buffer 0 (else the reverse).  Every launch writes the tile's
+// delta, and zero on the boundary ring where the tile touches it, to its output buffer.
 template <int ISOLVE, int NT>
-__global__ void __launch_bounds__(NT, SMOOTH_BLOCK / NT) k_smooth_mixed(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode, int mask,
-                                                               int u0, int nu, int dir, int tile)
+__global__ void __launch_bounds__(NT, SMOOTH_BLOCK / NT) k_smooth_f32(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode, int mask,
+                                                             int u0, int nu, int flags, int tile)
 {
     pdl_enter();
-    extern __shared__ double sm[];
+    extern __shared__ float smf[];
     const CaseDev &C = cs[blockIdx.y];
     if (!case_active(C, st[blockIdx.y], ig, mode)) return;
     const int e = nth_eq(mask, blockIdx.z);
@@ -818,71 +929,64 @@ __global__ void __launch_bounds__(NT, SMOOTH_BLOCK / NT) k_smooth_mixed(const Ca
         if (threadIdx.x == 0) atomicOr(&st[blockIdx.y].status, (int)CASE_BAD_LAUNCH);
         return;
     }
+    const bool first = (flags & 1) != 0, last = (flags & 2) != 0;
+    const int rb = (flags & 4) ? 1 : 0;
     const int W = P.W, R = P.W * P.Hh, kA = P.kA, kB = P.kB, limA = P.limA, limB = P.limB;
-    const int fs = eq_field(e), ts = eq_tmp(e);
-    const double *src = L.f[dir == 1 ? ts : fs];
-    double *dst = L.f[dir == 0 ? ts : fs];
-    double *phi = sm;
-    float *del = reinterpret_cast<float *>(sm + R), *del2 = del + R;
-    const double *__restrict__ gaw = L.f[co_slot(e, CK_AW)];
-    const double *__restrict__ gae = L.f[co_slot(e, CK_AE)];
-    const double *__restrict__ gas = L.f[co_slot(e, CK_AS)];
-    const double *__restrict__ gan = L.f[co_slot(e, CK_AN)];
-    const double *__restrict__ gap = L.f[co_slot(e, CK_AP)];
-    const double *__restrict__ gsu = L.f[co_slot(e, CK_SU)];
-    double A[6] = {0, 0, 0, 0, 0, 0}, B[6] = {0, 0, 0, 0, 0, 0}, pA = 0.0, pB = 0.0;
-    if (P.okA) {
-        const int g0 = P.gA;
-        pA = src[g0];
-        A[0] = gaw[g0]; A[1] = gae[g0]; A[2] = gas[g0]; A[3] = gan[g0]; A[4] = gap[g0]; A[5] = gsu[g0];
-    }
-    if (P.okB) {
-        const int g0 = P.gB;
-        pB = src[g0];
-        B[0] = gaw[g0]; B[1] = gae[g0]; B[2] = gas[g0]; B[3] = gan[g0]; B[4] = gap[g0]; B[5] = gsu[g0];
-    }
-    const double eps = ISOLVE == MGFVM_JACOBI ? 1.0e-30 : 0.0;
-    if (P.okA) { phi[kA] = pA; del[kA] = 0.0f; if (ISOLVE == MGFVM_JACOBI) del2[kA] = 0.0f; }
-    if (P.okB) { phi[kB] = pB; del[kB] = 0.0f; if (ISOLVE == MGFVM_JACOBI) del2[kB] = 0.0f; }
-    __syncthreads();
-    // FP64 residuals of the cells this launch updates, then the FP32 operator
-    float fA[5] = {0, 0, 0, 0, 0}, fB[5] = {0, 0, 0, 0, 0}, rA = 0.0f, rB = 0.0f;
+    const float *src = del32(L, e, rb);
+    float *dst = del32(L, e, rb ^ 1);
+    float *del = smf, *del2 = smf + R;
+    const float *__restrict__ o0 = op32(L, e, CK_AW);
+    const float *__restrict__ o1 = op32(L, e, CK_AE);
+    const float *__restrict__ o2 = op32(L, e, CK_AS);
+    const float *__restrict__ o3 = op32(L, e, CK_AN);
+    const float *__restrict__ o4 = op32(L, e, CK_AP);
+    const float *__restrict__ o5 = op32(L, e, CK_SU);
+    // operands of the cells this launch updates (the domain cells of its windows)
+    float A[6] = {0, 0, 0, 0, 0, 0}, B[6] = {0, 0, 0, 0, 0, 0}, dA = 0.0f, dB = 0.0f;
     if (limA >= 1) {
-        const double apA = A[4] + eps;
-        const double nb = A[0] * phi[kA - 1] + A[1] * phi[kA + 1] + A[2] * phi[kA - W] + A[3] * phi[kA + W];
-        rA = (float)((nb + A[5]) - apA * pA);
-        fA[0] = (float)A[0]; fA[1] = (float)A[1]; fA[2] = (float)A[2]; fA[3] = (float)A[3];
-        fA[4] = (float)(1.0 / apA);
+        const int g0 = P.gA;
+        A[0] = o0[g0]; A[1] = o1[g0]; A[2] = o2[g0]; A[3] = o3[g0]; A[4] = o4[g0]; A[5] = o5[g0];
     }
     if (limB >= 1) {
-        const double apB = B[4] + eps;
-        const double nb = B[0] * phi[kB - 1] + B[1] * phi[kB + 1] + B[2] * phi[kB - W] + B[3] * phi[kB + W];
-        rB = (float)((nb + B[5]) - apB * pB);
-        fB[0] = (float)B[0]; fB[1] = (float)B[1]; fB[2] = (float)B[2]; fB[3] = (float)B[3];
-        fB[4] = (float)(1.0 / apB);
+        const int g0 = P.gB;
+        B[0] = o0[g0]; B[1] = o1[g0]; B[2] = o2[g0]; B[3] = o3[g0]; B[4] = o4[g0]; B[5] = o5[g0];
     }
+    if (!first) {
+        if (P.okA) dA = src[P.gA];
+        if (P.okB) dB = src[P.gB];
+    }
+    if (P.okA) { del[kA] = dA; if (ISOLVE == MGFVM_JACOBI) del2[kA] = dA; }
+    if (P.okB) { del[kB] = dB; if (ISOLVE == MGFVM_JACOBI) del2[kB] = dB; }
+    __syncthreads();
     for (int h = 1; h <= nu; ++h) {
         if (ISOLVE == MGFVM_GAUSS_SEIDEL) {
             if (((u0 + h - 1) & 1) == 0) {
                 if (h <= limA)
-                    del[kA] = (fA[0] * del[kA - 1] + fA[1] * del[kA + 1] + fA[2] * del[kA - W] + fA[3] * del[kA + W] + rA) * fA[4];
+                    del[kA] = (A[0] * del[kA - 1] + A[1] * del[kA + 1] + A[2] * del[kA - W] + A[3] * del[kA + W] + A[5]) * A[4];
             } else {
                 if (h <= limB)
-                    del[kB] = (fB[0] * del[kB - 1] + fB[1] * del[kB + 1] + fB[2] * del[kB - W] + fB[3] * del[kB + W] + rB) * fB[4];
+                    del[kB] = (B[0] * del[kB - 1] + B[1] * del[kB + 1] + B[2] * del[kB - W] + B[3] * del[kB + W] + B[5]) * B[4];
             }
         } else {
             const float *cur = ((h - 1) & 1) ? del2 : del;
             float *nxt = ((h - 1) & 1) ? del : del2;
             if (h <= limA)
-                nxt[kA] = (fA[0] * cur[kA - 1] + fA[1] * cur[kA + 1] + fA[2] * cur[kA - W] + fA[3] * cur[kA + W] + rA) * fA[4];
+                nxt[kA] = (A[0] * cur[kA - 1] + A[1] * cur[kA + 1] + A[2] * cur[kA - W] + A[3] * cur[kA + W] + A[5]) * A[4];
             if (h <= limB)
-                nxt[kB] = (fB[0] * cur[kB - 1] + fB[1] * cur[kB + 1] + fB[2] * cur[kB - W] + fB[3] * cur[kB + W] + rB) * fB[4];
+                nxt[kB] = (B[0] * cur[kB - 1] + B[1] * cur[kB + 1] + B[2] * cur[kB - W] + B[3] * cur[kB + W] + B[5]) * B[4];
         }
         __syncthreads();
     }
     const float *res = (ISOLVE == MGFVM_JACOBI && (nu & 1)) ? del2 : del;
-    if (P.outA) dst[P.gA] = limA >= 1 ? pA + (double)res[kA] : pA;
-    if (P.outB) dst[P.gB] = limB >= 1 ? pB + (double)res[kB] : pB;
+    // the tile's cells (lim >= 1) and the ring cells it touches (delta 0 there)
+    const float rA = limA >= 1 ? res[kA] : 0.0f, rB = limB >= 1 ? res[kB] : 0.0f;
+    if (P.outA) dst[P.gA] = rA;
+    if (P.outB) dst[P.gB] = rB;
+    if (last && e != EQ_PP) {
+        double *phi = L.f[eq_field(e)];
+        if (P.outA && limA >= 1) phi[P.gA] = phi[P.gA] + (double)rA;
+        if (P.outB && limB >= 1) phi[P.gB] = phi[P.gB] + (double)rB;
+    }
 }
 
 // After an odd number of smoothing launches the result sits in the ping-pong buffer.
@@ -957,7 +1061,9 @@ __global__ void __launch_bounds__(BLOCK) k_restrict(const CaseDev *__restrict__ 
     cell_restrict_fluxes(L, K, C, i, j, z, nz);
     if (!what || !mode_active(C, ig + 1, M_DOWN)) return;
     // slice z assembles the equation whose defect it just computed
-    cell_asm(K, C, FluxLive(K), i, j, asm_slice(what, z, nz) & ~(unsigned)(A_FLUX | A_SC_OUTFLOW));
+    const unsigned w = asm_slice(what, z, nz) & ~(unsigned)(A_FLUX | A_SC_OUTFLOW);
+    if (w & A_F32) cell_asm_f32(K, C, i, j, w, (what & A_SC_OUTFLOW) && C.ibc_xp == 4);
+    else cell_asm(K, C, FluxLive(K), i, j, w);
     if (nz > 1 && z != 2) return;
     // the scalar outflow ghost of an interior row is read by this kernel only in the
     // defect of the cell west of it, so that cell (this thread, after its defect)
@@ -1460,22 +1566,22 @@ cudaError_t launch_one(const Launch &X, const CaseDev *dc, CaseState *ds, const 
         else
             le = launch_smooth<MGFVM_GAUSS_SEIDEL>(pdl, X, g, b, dc, ds, st);
         break;
-    case K_SMOOTH_MIXED:
+    case K_SMOOTH_F32:
         if (b > SMOOTH_BLOCK) return cudaErrorInvalidValue;
         if (S.isolve == MGFVM_JACOBI) {
             if (b <= SMOOTH_BLOCK / 4)
-                le = launch_k(pdl, k_smooth_mixed<MGFVM_JACOBI, SMOOTH_BLOCK / 4>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+                le = launch_k(pdl, k_smooth_f32<MGFVM_JACOBI, SMOOTH_BLOCK / 4>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
             else if (b <= SMOOTH_BLOCK / 2)
-                le = launch_k(pdl, k_smooth_mixed<MGFVM_JACOBI, SMOOTH_BLOCK / 2>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+                le = launch_k(pdl, k_smooth_f32<MGFVM_JACOBI, SMOOTH_BLOCK / 2>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
             else
-                le = launch_k(pdl, k_smooth_mixed<MGFVM_JACOBI, SMOOTH_BLOCK>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+                le = launch_k(pdl, k_smooth_f32<MGFVM_JACOBI, SMOOTH_BLOCK>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
         } else {
             if (b <= SMOOTH_BLOCK / 4)
-                le = launch_k(pdl, k_smooth_mixed<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK / 4>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+                le = launch_k(pdl, k_smooth_f32<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK / 4>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
             else if (b <= SMOOTH_BLOCK / 2)
-                le = launch_k(pdl, k_smooth_mixed<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK / 2>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+                le = launch_k(pdl, k_smooth_f32<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK / 2>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
             else
-                le = launch_k(pdl, k_smooth_mixed<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+                le = launch_k(pdl, k_smooth_f32<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
         }
         break;
     case K_COPY: le = launch_k(pdl, k_copy, g, b, 0, st, dc, ds, X.ig, X.mode, X.a0); break;
