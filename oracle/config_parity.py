@@ -8,7 +8,11 @@ initial state, in parallel processes, and compares hashes: equal hashes mean the
 engine's fields are the oracle's bit for bit (relative L2 error 0), and then the mixed
 form's distance to the FP64 fields is its distance to the oracle.
 
-    python oracle/config_parity.py F.json [--procs N] [--out summary.json]
+    python oracle/config_parity.py F.json [--procs N] [--out summary.json] [--cache C.json]
+    python oracle/config_parity.py --precompute W --cycles N --cache C.json [--procs N]
+
+The oracle's hashes can be computed ahead of the GPU run (--precompute: every case of
+workload W after N cycles) and kept in a cache file that later comparisons reuse.
 
 Cases whose solve turned non-finite (the reference build diverges on the same inputs)
 are reported and excluded from the distributions.
@@ -49,27 +53,57 @@ def _oracle_hash(args):
     return h.hexdigest(), time.perf_counter() - t
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("dump")
-    ap.add_argument("--procs", type=int, default=os.cpu_count() or 1)
-    ap.add_argument("--out", default=None)
-    a = ap.parse_args()
-    _paths()
+def _oracle_hashes(workload, cycles, procs, cache_path, skip=()):
+    """(sha256, seconds) of every case of `workload` after cycles[k] cycles, from the
+    cache where it holds them; cases in `skip` get (None, 0)."""
     import dataclasses
 
     import bench
+    cases, desc, profiles = bench.workload(workload)
+    cache = {"workload": workload, "hashes": {}}
+    if cache_path and os.path.exists(cache_path):
+        with open(cache_path) as f:
+            cache = json.load(f)
+        assert cache["workload"] == workload
+    key = lambda k: f"{k}:{cycles[k]}"
+    todo = [k for k in range(len(cases)) if key(k) not in cache["hashes"] and k not in skip]
+    jobs = [(dataclasses.asdict(cases[k]), None if profiles is None else list(profiles[k]), cycles[k]) for k in todo]
+    t0 = time.perf_counter()
+    if jobs:
+        with mp.get_context("spawn").Pool(procs) as pool:
+            for k, r in zip(todo, pool.imap(_oracle_hash, jobs, chunksize=1)):
+                cache["hashes"][key(k)] = list(r)
+                if cache_path and len(cache["hashes"]) % 16 == 0:
+                    with open(cache_path, "w") as f:
+                        json.dump(cache, f)
+    if cache_path:
+        with open(cache_path, "w") as f:
+            json.dump(cache, f)
+    return ([(None, 0.0) if k in skip else tuple(cache["hashes"][key(k)]) for k in range(len(cases))], desc,
+            time.perf_counter() - t0)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("dump", nargs="?")
+    ap.add_argument("--procs", type=int, default=os.cpu_count() or 1)
+    ap.add_argument("--out", default=None)
+    ap.add_argument("--cache", default=None)
+    ap.add_argument("--precompute", default=None, help="workload whose oracle hashes to compute into --cache")
+    ap.add_argument("--cycles", type=int, default=2000)
+    a = ap.parse_args()
+    _paths()
+    import bench
+    if a.precompute:
+        n = len(bench.workload(a.precompute)[0])
+        _oracle_hashes(a.precompute, [a.cycles] * n, a.procs, a.cache)
+        return
     with open(a.dump) as f:
         dump = json.load(f)
-    cases, desc, profiles = bench.workload(dump["workload"])
     rows = dump["cases"]
-    assert len(rows) == len(cases), "the dump and the workload disagree on the number of cases"
-    jobs = [(dataclasses.asdict(c), None if profiles is None else list(profiles[k]), rows[k]["cycles"])
-            for k, c in enumerate(cases)]
-    t0 = time.perf_counter()
-    with mp.get_context("spawn").Pool(a.procs) as pool:
-        res = pool.map(_oracle_hash, jobs, chunksize=1)
-    wall = time.perf_counter() - t0
+    res, desc, wall = _oracle_hashes(dump["workload"], [r["cycles"] for r in rows], a.procs, a.cache,
+                                     skip={k for k, r in enumerate(rows) if r["diverged"]})
+    assert len(rows) == len(res), "the dump and the workload disagree on the number of cases"
     ok = [k for k, r in enumerate(rows) if not r["diverged"]]
     same = [k for k in ok if res[k][0] == rows[k]["sha256"]]
     differ = [k for k in ok if res[k][0] != rows[k]["sha256"]]
