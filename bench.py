@@ -240,7 +240,9 @@ def adjoint_rate(device, ncases=64, cycles=10, check=True):
         s.adjoint(2)                                   # warm-up
         s.adjoint(cycles)
         adj_ms = s.last_elapsed_ms
-        res0 = s.adjoint_gradient(0)
+        res = [s.adjoint_gradient(k, allow_nonfinite=True) for k in range(ncases)]
+        res0 = res[0]
+        diverged = [k for k, r in enumerate(res) if not np.isfinite(r[2])]
     out = {"config": f"adjoint configuration: {ncases} cases 256x256, ngrid 5, seeded random obstacles, Re 100, "
                      f"inlet profile 1 + 0.1 N(0,1)",
            "method": "reverse mode: taped V-cycle and its phase-by-phase transpose, checkpoints every ~sqrt(n) "
@@ -249,6 +251,7 @@ def adjoint_rate(device, ncases=64, cycles=10, check=True):
            "ms_total": round(adj_ms, 3), "ms_per_cycle": round(adj_ms / cycles, 3),
            "forward_ms_per_cycle": round(fwd_ms, 3),
            "cost_vs_forward_cycles": round(adj_ms / cycles / fwd_ms, 2),
+           "diverged_cases": diverged,
            "note": "a gradient over n cycles costs cost_vs_forward_cycles x the plain batch's n cycles"}
     if check:
         j, g_in, g_a, g_p = res0

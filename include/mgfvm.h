@@ -354,14 +354,15 @@ int mgfvm_gradient(const mgfvm_config *cfg, const double *inlet_u, int n_inlet, 
  * cycles' states come back from checkpoints of u, v, p, sc taken every ~sqrt(ncycles)
  * cycles and re-runs between them.  Afterwards u, v, p, sc and the histories are
  * those after ncycles cycles (other arrays unspecified).  Periodic boundaries are not
- * covered (MGFVM_EUNSUPPORTED); a case that turns non-finite fails the call
- * (MGFVM_ENONFINITE).  Replaces no routine of the reference: the reference computes
+ * covered (MGFVM_EUNSUPPORTED).  A case that turns non-finite within the cycles (the
+ * reference diverges on such inputs too) has no gradient; the others are unaffected.  Replaces no routine of the reference: the reference computes
  * no derivatives. */
 int mgfvm_adjoint(mgfvm_ctx *ctx, int ncycles);
 
 /* The last mgfvm_adjoint's result for case `icase`: J after the cycles and its
  * gradient (dJ_dinlet: nfy values, the inlet faces of mgfvm_set_inlet_profile).  Any
- * pointer may be NULL. */
+ * pointer may be NULL.  MGFVM_ENONFINITE (gradient set to NaN) for a case that turned
+ * non-finite. */
 int mgfvm_adjoint_gradient(mgfvm_ctx *ctx, int icase, double *J, double *dJ_dinlet, double *dJ_damuf,
                            double *dJ_dprsc);
 

@@ -96,6 +96,7 @@ struct mgfvm_ctx {
     // the last mgfvm_adjoint: per case J and its gradient (nfy inlet faces, amuf, prsc)
     int adj_cycles = -1;
     std::vector<double> adj_J, adj_gamuf, adj_gprsc;
+    std::vector<char> adj_bad;                // the case turned non-finite within the cycles
     std::vector<std::vector<double>> adj_gin;
 };
 
@@ -2006,6 +2007,7 @@ int mgfvm_adjoint(mgfvm_ctx *x, int ncycles)
         hs_final = x->hs;
         // J of every case, and its adjoint seed on level 0 (zero elsewhere)
         x->adj_J.assign(n, 0.0);
+        x->adj_bad.assign(n, 0);
         CK(cudaMemsetAsync(x->tpool, 0, x->tcase_off.empty() ? 0 : x->tcase_off.back() + x->tcase_bytes.back(),
                            x->stream));
         for (int c = 0; c < n && rc == MGFVM_OK; ++c) {
@@ -2014,13 +2016,12 @@ int mgfvm_adjoint(mgfvm_ctx *x, int ncycles)
             std::vector<double> p(cells), sc(cells), bp(cells, 0.0), bsc(cells, 0.0);
             if ((rc = mgfvm_get_field(x, c, 0, MGFVM_F_P, p.data())) != MGFVM_OK) break;
             if ((rc = mgfvm_get_field(x, c, 0, MGFVM_F_SC, sc.data())) != MGFVM_OK) break;
+            // a case whose iteration diverged (the reference's does on the same inputs) has
+            // no derivative; its transpose runs on non-finite values without touching the
+            // other cases, and its gradient is reported as such
             bool finite = true;
             for (size_t k = 0; k < cells; ++k) finite &= std::isfinite(p[k]) && std::isfinite(sc[k]);
-            if (!finite) {
-                rc = mgfvm_fail(MGFVM_ENONFINITE, "mgfvm_adjoint: case %d turned non-finite within %d cycles", c,
-                                ncycles);
-                break;
-            }
+            x->adj_bad[c] = !finite;
             objective_of(p.data(), sc.data(), L.npx, L.npy, &x->adj_J[c]);
             const double ny = (double)(L.npy - 2);
             for (int j = 1; j <= L.npy - 2; ++j) {
@@ -2127,10 +2128,18 @@ int mgfvm_adjoint_gradient(mgfvm_ctx *x, int icase, double *J, double *dJ_dinlet
     if (icase < 0 || icase >= x->ncases) return mgfvm_fail(MGFVM_EINVAL, "case %d out of range", icase);
     if (x->adj_cycles < 0 || (int)x->adj_J.size() != x->ncases)
         return mgfvm_fail(MGFVM_EINVAL, "mgfvm_adjoint_gradient: no mgfvm_adjoint has run on this context");
+    const bool bad = x->adj_bad[icase] != 0;
+    const double nan = std::nan("");
     if (J) *J = x->adj_J[icase];
-    if (dJ_dinlet) std::copy(x->adj_gin[icase].begin(), x->adj_gin[icase].end(), dJ_dinlet);
-    if (dJ_damuf) *dJ_damuf = x->adj_gamuf[icase];
-    if (dJ_dprsc) *dJ_dprsc = x->adj_gprsc[icase];
+    if (dJ_dinlet) {
+        if (bad) std::fill(dJ_dinlet, dJ_dinlet + x->adj_gin[icase].size(), nan);
+        else std::copy(x->adj_gin[icase].begin(), x->adj_gin[icase].end(), dJ_dinlet);
+    }
+    if (dJ_damuf) *dJ_damuf = bad ? nan : x->adj_gamuf[icase];
+    if (dJ_dprsc) *dJ_dprsc = bad ? nan : x->adj_gprsc[icase];
+    if (bad)
+        return mgfvm_fail(MGFVM_ENONFINITE, "case %d turned non-finite within the %d cycles: no gradient", icase,
+                          x->adj_cycles);
     return MGFVM_OK;
 }
 

@@ -285,12 +285,16 @@ class Solver:
         inputs.  Read the result with adjoint_gradient(case)."""
         check(self._lib.mgfvm_adjoint(self._h, int(cycles)))
 
-    def adjoint_gradient(self, case: int = 0) -> Tuple[float, np.ndarray, float, float]:
-        """(J, dJ/dinlet (nfy values), dJ/damuf, dJ/dprsc) of the last adjoint run."""
+    def adjoint_gradient(self, case: int = 0, allow_nonfinite: bool = False) -> Tuple[float, np.ndarray, float, float]:
+        """(J, dJ/dinlet (nfy values), dJ/damuf, dJ/dprsc) of the last adjoint run.  A case
+        that turned non-finite raises ENONFINITE unless `allow_nonfinite` (its gradient is
+        then NaN)."""
         g_in = np.zeros(int(self.cases[case].nfy))
         j, ga, gp = C.c_double(), C.c_double(), C.c_double()
-        check(self._lib.mgfvm_adjoint_gradient(self._h, case, C.byref(j), g_in.ctypes.data_as(_dp), C.byref(ga),
-                                               C.byref(gp)))
+        st = self._lib.mgfvm_adjoint_gradient(self._h, case, C.byref(j), g_in.ctypes.data_as(_dp), C.byref(ga),
+                                              C.byref(gp))
+        if not (allow_nonfinite and st == _abi.ENONFINITE):
+            check(st)
         return j.value, g_in, ga.value, gp.value
 
     @property

@@ -142,3 +142,23 @@ def test_adjoint_cluster_sizes(cluster, monkeypatch, oracle_built):
     cfg = small_cases()["obs_gs_touch"]
     prof = 1.0 + 0.05 * np.sin(np.arange(cfg.nfy))
     _close(_adjoint([cfg], [prof], 3)[0], _forward_mode(cfg, prof, 3), f"cluster {cluster}")
+
+
+def test_adjoint_with_a_diverging_case_in_the_batch(oracle_built):
+    """A case whose iteration turns non-finite (the reference's does on the same input)
+    gets no gradient; the other cases of its batch are unaffected."""
+    from mgfvm import MgfvmError, Solver, configs
+    from mgfvm._abi import ENONFINITE
+    cases, profs = configs.c4(26, seed=4)
+    pair = [cases[0], cases[25]]
+    cycles = 10
+    with Solver(pair) as s:
+        s.set_inlet_profile(0, profs[0])
+        s.set_inlet_profile(1, profs[25])
+        s.adjoint(cycles)
+        with pytest.raises(MgfvmError) as ei:
+            s.adjoint_gradient(1)
+        assert ei.value.status == ENONFINITE
+        assert np.isnan(s.adjoint_gradient(1, allow_nonfinite=True)[2])
+        good = s.adjoint_gradient(0)
+    _close(good, _forward_mode(cases[0], profs[0], cycles), "the finite case beside a diverging one")
