@@ -496,6 +496,9 @@ def main():
     ap.add_argument("--profile-tangent", type=int, default=0,
                     help="only run this many tangent V-cycles of a small gradient batch (64x64 channel, "
                          "all 66 directions) after 2 warm-up cycles, inside the NVTX range 'profile', and exit")
+    ap.add_argument("--profile-adjoint", type=int, default=0,
+                    help="only run the reverse mode over this many V-cycles of one adjoint-configuration case "
+                         "(256x256) after a 1-cycle warm-up, the timed run inside the NVTX range 'profile', and exit")
     ap.add_argument("--profile-batch-smoother", choices=["plain", "tma"], default=None,
                     help="only run one V-cycle of the 64-case obstacle-flow batch (levels 0-2 smoothed by "
                          "512-thread tiles of 6 units, per-thread or TMA-staged loads) after 3 warm-up cycles, "
@@ -517,6 +520,17 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
 
     from mgfvm import Solver
+    if a.profile_adjoint:
+        from mgfvm import configs
+        cases, profs = configs.c4(1, seed=4)
+        with Solver(cases, device=local) as s:
+            s.set_inlet_profile(0, profs[0])
+            s.adjoint(1)
+            torch.cuda.nvtx.range_push("profile")
+            s.adjoint(a.profile_adjoint)
+            torch.cuda.nvtx.range_pop()
+            log(f"adjoint: {s.last_elapsed_ms / a.profile_adjoint:.3f} ms per cycle (one case)")
+        return
     if a.profile_batch_smoother:
         from mgfvm import configs
         cases = [configs.c1(10.0 if k % 2 == 0 else 100.0, seed=k + 1) for k in range(64)]

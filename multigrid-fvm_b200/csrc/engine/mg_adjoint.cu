@@ -42,17 +42,24 @@ __host__ __device__ inline unsigned long long write_mask(const Phase &P)
     case P_JAC_RING: return bit(tmp_of(P.a));
     case P_JAC_SWEEP: return bit(P.b == 0 ? tmp_of(P.a) : field_of(P.a));
     case P_JAC_COPY: return bit(field_of(P.a));
-    case P_MASS_COEFP: return bit(S_PP) | coef_bits(EQ_PP);
-    case P_UPDATE: return bit(S_U) | bit(S_V) | bit(S_P);
+    case P_MASS_COEFP:
+        return (P.a & MC_COEF ? bit(S_PP) | (coef_bits(EQ_PP) & ~bit(co_slot(EQ_PP, CK_SU))) : 0ULL) |
+               (P.a & MC_SU ? bit(co_slot(EQ_PP, CK_SU)) : 0ULL);
+    case P_UPDATE: return (P.a & 1 ? bit(S_U) : 0ULL) | (P.a & 2 ? bit(S_V) : 0ULL) | (P.a & 4 ? bit(S_P) : 0ULL);
     case P_PFIX: case P_PFIX_SCATTER: return bit(S_P);
     case P_PFIX_GATHER: return bit(PB_BIT);
     case P_OUTFLOW: return bit(S_U) | bit(S_V) | bit(S_P) | (P.b ? bit(S_SC) : 0ULL);
     case P_RESTV:
-        return bit(S_U) | bit(S_V) | bit(S_P) | bit(S_SC) | bit(S_RU) | bit(S_RV) | bit(S_RP) | bit(S_RSC);
+        return (P.a & 1 ? bit(S_U) | bit(S_RU) : 0ULL) | (P.a & 2 ? bit(S_V) | bit(S_RV) : 0ULL) |
+               (P.a & 4 ? bit(S_P) | bit(S_RP) : 0ULL) | (P.a & 8 ? bit(S_SC) | bit(S_RSC) : 0ULL);
     case P_FINE_RES: return bit(tmp_of(res_eq(P.a)));
     case P_RESTRICT: return bit(P.a == 0 ? S_RESU : P.a == 1 ? S_RESV : S_RESSC);
-    case P_PROL_CORR: return bit(S_CU) | bit(S_CV) | bit(S_CP) | bit(S_C);
-    case P_PROL_APPLY: return bit(S_U) | bit(S_V) | bit(S_P) | bit(S_SC);
+    case P_PROL_CORR:
+        return (P.a & 1 ? bit(S_CU) : 0ULL) | (P.a & 2 ? bit(S_CV) : 0ULL) | (P.a & 4 ? bit(S_CP) : 0ULL) |
+               (P.a & 8 ? bit(S_C) : 0ULL);
+    case P_PROL_APPLY:
+        return (P.a & 1 ? bit(S_U) : 0ULL) | (P.a & 2 ? bit(S_V) : 0ULL) | (P.a & 4 ? bit(S_P) : 0ULL) |
+               (P.a & 8 ? bit(S_SC) : 0ULL);
     default: return 0;
     }
 }
@@ -103,17 +110,17 @@ __device__ __forceinline__ void phase_cell(const X &x, const Phase &P, int i, in
         break;
     }
     case P_JAC_COPY: F.st(field_of(P.a), q, F.ld(tmp_of(P.a), q)); break;
-    case P_MASS_COEFP: cell_mass_coefp_io(F, C, i, j); break;
-    case P_UPDATE: cell_update_io(F, C, q); break;
+    case P_MASS_COEFP: cell_mass_coefp_io(F, C, i, j, false, P.a); break;
+    case P_UPDATE: cell_update_io(F, C, q, P.a); break;
     case P_PFIX: F.st(S_P, F.L.pdst[i], F.ld(S_P, F.L.psrc[i])); break;
     case P_PFIX_GATHER: F.set_pb(i, F.ld(S_P, F.L.psrc[i])); break;
     case P_PFIX_SCATTER: F.st(S_P, F.L.pdst[i], F.pb(i)); break;
     case P_OUTFLOW: row_outflow_io(F, j, P.b != 0); break;
-    case P_RESTV: cell_restv_io(F, x.io(P.ig + 1), i, j); break;
+    case P_RESTV: cell_restv_io(F, x.io(P.ig + 1), i, j, P.a); break;
     case P_FINE_RES: cell_fine_residuals_io(F, C, i, j, P.a); break;
     case P_RESTRICT: cell_restrict_io(F, x.io(P.ig + 1), C, i, j, P.a); break;
-    case P_PROL_CORR: cell_prol_corr_io(F, x.io(P.ig + 1), i, j); break;
-    case P_PROL_APPLY: cell_prol_apply_io<IO, false>(F, x.io(P.ig + 1), i, j); break;
+    case P_PROL_CORR: cell_prol_corr_io(F, x.io(P.ig + 1), i, j, P.a); break;
+    case P_PROL_APPLY: cell_prol_apply_io<IO, false>(F, x.io(P.ig + 1), i, j, P.a); break;
     default: break;
     }
 }
@@ -201,12 +208,27 @@ struct RecCase {
 };
 
 // Copy the arrays phase P overwrites between the level and the tape (save: to the tape).
+// A half-sweep overwrites the cells of its colour only: those alone are kept, in the
+// order phase_cells visits them.
 __device__ void tape_copy(const CaseDev &C, const CaseAdj &A, const Phase &P, bool save)
 {
     const LevelDev &L = C.lv[write_level(P)];
+    double *t = A.tape + P.off;
+    if (P.kind == P_GS) {
+        const Box d = box_eq(L.npx, L.npy, P.a);
+        double *a = L.f[field_of(P.a)];
+        const int wr = (d.wi + 1) >> 1, n = wr * d.wj;
+        for (int k = wk_id(); k < n; k += wk_n()) {
+            const int j = d.j0 + k / wr;
+            const int i = d.i0 + (((d.i0 + j) & 1) != P.b ? 1 : 0) + 2 * (k % wr);
+            if (i > d.i0 + d.wi - 1) continue;
+            if (save) t[k] = a[j * L.npx + i];
+            else a[j * L.npx + i] = t[k];
+        }
+        return;
+    }
     const long long n = (long long)L.npx * L.npy;
     const unsigned long long m = write_mask(P);
-    double *t = A.tape + P.off;
     for (int s = 0; s < NSLOTS; ++s) {
         if (!((m >> s) & 1ULL)) continue;
         double *a = L.f[s];
@@ -228,12 +250,30 @@ __device__ void tape_copy(const CaseDev &C, const CaseAdj &A, const Phase &P, bo
 constexpr int MAXW = 8;   // most values one cell of a phase writes (restv: 8)
 enum { KS_NONE = INT_MIN, KS_AMU = -1, KS_AMUSC = -2, KS_PB = -3 };
 
-// The state of one cell's evaluation: collect (mode 0) or probe read k (mode 1).
+// The state of one cell's evaluation: collect (mode 0) or probe read k (mode 1).  The
+// adjoints of the outputs sit in named fields, reached only at constant offsets, so
+// that after inlining the whole state lives in registers and the read and write
+// counters fold to constants at every access site.
 struct Probe {
     int mode, k, nr, nw, ks, kq, klev, ovf;
     double acc;
-    double yb[MAXW];
+    double y0, y1, y2, y3, y4, y5, y6, y7;
+    __device__ __forceinline__ double yb(int w) const
+    {
+        switch (w) {
+        case 0: return y0; case 1: return y1; case 2: return y2; case 3: return y3;
+        case 4: return y4; case 5: return y5; case 6: return y6; default: return y7;
+        }
+    }
+    __device__ __forceinline__ void set_yb(int w, double v)
+    {
+        switch (w) {
+        case 0: y0 = v; break; case 1: y1 = v; break; case 2: y2 = v; break; case 3: y3 = v; break;
+        case 4: y4 = v; break; case 5: y5 = v; break; case 6: y6 = v; break; default: y7 = v; break;
+        }
+    }
 };
+static_assert(MAXW == 8, "Probe holds MAXW output adjoints");
 
 // Dual-number access whose reads are numbered: in a probe, read k carries derivative
 // 1 and every other read 0, so each value written carries d(value)/d(read k); the
@@ -263,10 +303,10 @@ struct AdjIO {
             return;
         }
         if (P->mode == 0) {
-            P->yb[w] = *b;
+            P->set_yb(w, *b);
             *b = 0.0;
         } else {
-            P->acc += P->yb[w] * x.d;
+            P->acc += P->yb(w) * x.d;
         }
     }
     __device__ __forceinline__ Dual ld(int s, int q) const { return rd(L.f[s][q], s, q); }
@@ -284,11 +324,17 @@ struct AdjCase {
     __device__ __forceinline__ AdjIO io(int ig) const { return AdjIO{C.lv[ig], B.lv[ig], P, ig}; }
 };
 
+// Adjoints of amu and amusc gathered by one thread during one phase: a phase reads the
+// parameters of its own level (f) and of the level below (k) at most.
+struct ParAcc {
+    double amu_f, amusc_f, amu_k, amusc_k;
+};
+
 // The transpose of one cell of phase P: adjoints of its reads += adjoint(out) *
 // d(out)/d(read); adjoints of its outputs cleared.  amu/amusc go to the thread's
-// per-level accumulators.
+// accumulators of the phase.
 __device__ __forceinline__ void adj_cell(const CaseDev &C, const CaseTan &B, const Phase &P, int i, int j,
-                                         double *pacc, int *bad)
+                                         ParAcc &pa, int *bad)
 {
     Probe S;
     S.mode = 0;
@@ -302,7 +348,7 @@ __device__ __forceinline__ void adj_cell(const CaseDev &C, const CaseTan &B, con
     }
     const int K = S.nr, W = S.nw;
     bool any = false;
-    for (int w = 0; w < W; ++w) any |= S.yb[w] != 0.0;
+    for (int w = 0; w < W; ++w) any |= S.yb(w) != 0.0;
     if (!any) return;
     for (int k = 0; k < K; ++k) {
         S.mode = 1;
@@ -312,19 +358,26 @@ __device__ __forceinline__ void adj_cell(const CaseDev &C, const CaseTan &B, con
         S.ks = KS_NONE;
         phase_cell(X, P, i, j);
         if (S.acc == 0.0) continue;
-        if (S.ks >= 0) atomicAdd(B.lv[S.klev].t[S.ks] + S.kq, S.acc);
-        else if (S.ks == KS_AMU) pacc[2 * S.klev] += S.acc;
-        else if (S.ks == KS_AMUSC) pacc[2 * S.klev + 1] += S.acc;
-        else if (S.ks == KS_PB) atomicAdd(B.lv[S.klev].pbuf_t + S.kq, S.acc);
+        if (S.ks >= 0) {
+            atomicAdd(B.lv[S.klev].t[S.ks] + S.kq, S.acc);
+        } else if (S.ks == KS_AMU) {
+            if (S.klev == P.ig) pa.amu_f += S.acc;
+            else pa.amu_k += S.acc;
+        } else if (S.ks == KS_AMUSC) {
+            if (S.klev == P.ig) pa.amusc_f += S.acc;
+            else pa.amusc_k += S.acc;
+        } else if (S.ks == KS_PB) {
+            atomicAdd(B.lv[S.klev].pbuf_t + S.kq, S.acc);
+        }
     }
 }
 
 // The transpose of one red-black half-sweep cell, phi_c = (sum a_nb phi_nb + su) / ap
-// (gs_value), written out: the partial derivatives are those the dual arithmetic of
-// adj_cell forms (d/da_nb = phi_nb / ap, d/dphi_nb = a_nb / ap, d/dsu = 1 / ap,
-// d/dap = -phi_c / ap), so the result is adj_cell's, at one evaluation instead of
-// eleven.  The cell's coefficients are read by no other cell of the half-sweep, so
-// their adjoints take plain additions; the neighbours' take atomics.
+// (gs_value), written out: d/da_nb = phi_nb / ap, d/dphi_nb = a_nb / ap, d/dsu = 1 / ap,
+// d/dap = -phi_c / ap, the partial derivatives the dual arithmetic of adj_cell forms,
+// here with the adjoint divided by ap once (the same numbers to rounding) at one
+// evaluation instead of eleven.  The cell's coefficients are read by no other cell of
+// the half-sweep, so their adjoints take plain additions; the neighbours' take atomics.
 __device__ __forceinline__ void adj_gs_cell(const LevelDev &L, const LevelTan &B, int e, int i, int j)
 {
     const int nx = L.npx, q = j * nx + i, phi = field_of(e);
@@ -337,31 +390,36 @@ __device__ __forceinline__ void adj_gs_cell(const LevelDev &L, const LevelTan &B
     const double *f = L.f[phi];
     const double pw = f[q - 1], pe = f[q + 1], ps = f[q - nx], pn = f[q + nx];
     const double val = gs_value(aw, ae, as, an, ap, su, pw, pe, ps, pn);
-    B.t[co_slot(e, CK_AW)][q] += yb * (pw / ap);
-    B.t[co_slot(e, CK_AE)][q] += yb * (pe / ap);
-    B.t[co_slot(e, CK_AS)][q] += yb * (ps / ap);
-    B.t[co_slot(e, CK_AN)][q] += yb * (pn / ap);
-    B.t[co_slot(e, CK_AP)][q] += yb * ((0.0 - val * 1.0) / ap);
-    B.t[co_slot(e, CK_SU)][q] += yb * ((1.0 - val * 0.0) / ap);
+    const double ya = yb / ap;
+    B.t[co_slot(e, CK_AW)][q] += ya * pw;
+    B.t[co_slot(e, CK_AE)][q] += ya * pe;
+    B.t[co_slot(e, CK_AS)][q] += ya * ps;
+    B.t[co_slot(e, CK_AN)][q] += ya * pn;
+    B.t[co_slot(e, CK_AP)][q] += -(ya * val);
+    B.t[co_slot(e, CK_SU)][q] += ya;
     double *b = B.t[phi];
-    atomicAdd(b + q - 1, yb * (aw / ap));
-    atomicAdd(b + q + 1, yb * (ae / ap));
-    atomicAdd(b + q - nx, yb * (as / ap));
-    atomicAdd(b + q + nx, yb * (an / ap));
+    atomicAdd(b + q - 1, ya * aw);
+    atomicAdd(b + q + 1, ya * ae);
+    atomicAdd(b + q - nx, ya * as);
+    atomicAdd(b + q + nx, ya * an);
 }
 
 // ----------------------------------------------------------------- kernel
-__device__ __forceinline__ double block_total(double v, double *red)
+// Add a phase's amu/amusc adjoints of every thread to the case's per-level sums: a
+// warp sum, then one atomic per warp and value.
+__device__ __forceinline__ void flush_par(ParAcc &pa, const Phase &P, double *pacc)
 {
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    const int w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-    __syncthreads();
-    if ((threadIdx.x & 31) == 0) red[w] = v;
-    __syncthreads();
-    double s = 0.0;
-    if (threadIdx.x == 0)
-        for (int k = 0; k < nw; ++k) s += red[k];
-    return s;
+    double v[4] = {pa.amu_f, pa.amusc_f, pa.amu_k, pa.amusc_k};
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+    if ((threadIdx.x & 31) == 0) {
+        if (v[0] != 0.0) atomicAdd(pacc + 2 * P.ig, v[0]);
+        if (v[1] != 0.0) atomicAdd(pacc + 2 * P.ig + 1, v[1]);
+        if (v[2] != 0.0) atomicAdd(pacc + 2 * (P.ig + 1), v[2]);
+        if (v[3] != 0.0) atomicAdd(pacc + 2 * (P.ig + 1) + 1, v[3]);
+    }
+    pa = ParAcc{0.0, 0.0, 0.0, 0.0};
 }
 
 // One V-cycle of case blockIdx.y, taped, then its transpose, on a cluster of
@@ -371,7 +429,6 @@ __device__ __forceinline__ double block_total(double v, double *red)
 __global__ void __launch_bounds__(ADJ_BLOCK, 1) k_adj_cycle(const CaseDev *__restrict__ cs, CaseState *st,
                                                             const CaseTan *__restrict__ ts, const CaseAdj *__restrict__ as)
 {
-    __shared__ double red[ADJ_BLOCK / 32];
     __shared__ int bad_s;
     const CaseDev &C = cs[blockIdx.y];
     const CaseAdj &A = as[blockIdx.y];
@@ -390,21 +447,18 @@ __global__ void __launch_bounds__(ADJ_BLOCK, 1) k_adj_cycle(const CaseDev *__res
         case_barrier();
     }
     // reverse
-    double pacc[2 * MAXLEV];
-    for (int k = 0; k < 2 * MAXLEV; ++k) pacc[k] = 0.0;
+    ParAcc pa{0.0, 0.0, 0.0, 0.0};
     for (int p = A.nphase - 1; p >= 0; --p) {
         const Phase P = A.prog[p];
         tape_copy(C, A, P, false);
         case_barrier();
-        if (P.kind == P_GS)
+        if (P.kind == P_GS && !A.generic) {
             phase_cells(C, P, [&](int i, int j) { adj_gs_cell(C.lv[P.ig], B.lv[P.ig], P.a, i, j); });
-        else
-            phase_cells(C, P, [&](int i, int j) { adj_cell(C, B, P, i, j, pacc, &bad); });
+        } else {
+            phase_cells(C, P, [&](int i, int j) { adj_cell(C, B, P, i, j, pa, &bad); });
+            flush_par(pa, P, A.pacc);
+        }
         case_barrier();
-    }
-    for (int k = 0; k < 2 * C.ngrid; ++k) {
-        const double s = block_total(pacc[k], red);
-        if (threadIdx.x == 0 && s != 0.0) atomicAdd(A.pacc + k, s);
     }
     if (bad) atomicOr(&bad_s, 1);
     __syncthreads();
@@ -443,9 +497,14 @@ bool build_adj_program(const CaseDev &hc, const Sched &S, std::vector<Phase> &pr
         const LevelDev &L = hc.lv[write_level(P)];
         const unsigned long long m = write_mask(P);
         long long n = 0;
-        for (int s = 0; s < NSLOTS; ++s)
-            if ((m >> s) & 1ULL) n += (long long)L.npx * L.npy;
-        if ((m >> PB_BIT) & 1ULL) n += L.ncopy;
+        if (kind == P_GS) {
+            const Box d = box_eq(L.npx, L.npy, a);
+            n = (long long)std::max(0, (d.wi + 1) >> 1) * std::max(0, d.wj);
+        } else {
+            for (int s = 0; s < NSLOTS; ++s)
+                if ((m >> s) & 1ULL) n += (long long)L.npx * L.npy;
+            if ((m >> PB_BIT) & 1ULL) n += L.ncopy;
+        }
         tape += n;
         prog.push_back(P);
     };
@@ -470,9 +529,12 @@ bool build_adj_program(const CaseDev &hc, const Sched &S, std::vector<Phase> &pr
         add(P_ASM_SC, ig);
         if (down && hc.ibc_xp == 4) add(P_SC_OUTFLOW, ig);
         smooth(ig, uvsc, 3, S.nswpm);
-        add(P_MASS_COEFP, ig);
+        // multi-output routines run one output group per phase: a transposed phase then
+        // probes only the reads of that group
+        add(P_MASS_COEFP, ig, MC_COEF);
+        add(P_MASS_COEFP, ig, MC_SU);
         smooth(ig, pp, 1, S.nswpp);
-        add(P_UPDATE, ig);
+        for (int part = 1; part <= 4; part <<= 1) add(P_UPDATE, ig, part);
         if (hc.lv[ig].ncopy > 0) {
             if (hc.lv[ig].hazard) {
                 add(P_PFIX_GATHER, ig);
@@ -486,14 +548,14 @@ bool build_adj_program(const CaseDev &hc, const Sched &S, std::vector<Phase> &pr
     for (int ig = 0; ig < ng; ++ig) {
         step(ig, true);
         if (ig != ng - 1) {
-            add(P_RESTV, ig);
+            for (int part = 1; part <= 8; part <<= 1) add(P_RESTV, ig, part);
             for (int w = 0; w < 3; ++w) add(P_FINE_RES, ig, w);
             for (int w = 0; w < 3; ++w) add(P_RESTRICT, ig, w);
         }
     }
     for (int ig = ng - 1; ig > 0; --ig) {
-        add(P_PROL_CORR, ig - 1);
-        add(P_PROL_APPLY, ig - 1);
+        for (int part = 1; part <= 8; part <<= 1) add(P_PROL_CORR, ig - 1, part);
+        for (int part = 1; part <= 8; part <<= 1) add(P_PROL_APPLY, ig - 1, part);
         if (ig != 1) step(ig - 1, false);
     }
     return true;

@@ -39,15 +39,15 @@ enum PhaseKind {
     P_JAC_RING,                        // Jacobi: the ping-pong buffer's ring from the field: a = eq
     P_JAC_SWEEP,                       // one Jacobi sweep: a = eq, b = 0 field -> buffer, 1 buffer -> field
     P_JAC_COPY,                        // Jacobi, odd sweep count: the buffer back to the field: a = eq
-    P_MASS_COEFP,                      // masserror + coefp
-    P_UPDATE,                          // update
+    P_MASS_COEFP,                      // masserror + coefp: a = MC_COEF (p' = 0, coefficients) or MC_SU
+    P_UPDATE,                          // update: a = 1 u, 2 v, 4 p
     P_PFIX,                            // update's obstacle pressure copy (no chained copies)
     P_PFIX_GATHER, P_PFIX_SCATTER,     // the same copy through its buffer (chained copies)
     P_OUTFLOW,                         // outflow of u, v, p (b = 1: and the scalar ghost)
-    P_RESTV,                           // restv: coarse state and R(x_f) (level a coarse of ig)
+    P_RESTV,                           // restv: coarse state and R(x_f) of a = 1 u, 2 v, 4 p, 8 sc
     P_FINE_RES,                        // fine residual of equation a (0 u, 1 v, 2 sc) into its buffer
     P_RESTRICT,                        // FAS defect of equation a on the coarse level
-    P_PROL_CORR, P_PROL_APPLY,         // prolongation: coarse corrections, fine gather
+    P_PROL_CORR, P_PROL_APPLY,         // prolongation: coarse corrections, fine gather (a as restv)
     P_NKINDS
 };
 
@@ -65,6 +65,7 @@ struct CaseAdj {
     int nphase;
     double *tape;
     double *pacc;
+    int generic;   // transpose every phase by dual-number probes (the closed forms' check)
 };
 
 // Bit `s` of the mask: slot s of the written level; PB_BIT: the pressure-copy buffer.

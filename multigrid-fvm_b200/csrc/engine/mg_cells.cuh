@@ -280,29 +280,37 @@ __device__ __forceinline__ void cell_asm(const LevelDev &L, const CaseDev &C, co
 // solve_pprime's assembly: masserror :1096-1125 then coefp :1018-1092 (with the
 // p' Dirichlet rows in the order x-, x+, y-, y+) at one interior cell; returns |div|.
 // us, vs: the slots of the velocities to read (the fields, or the smoother's buffers
-// holding them)
+// holding them).  `parts` (MC_*) selects what is formed: the coefficients, the
+// source su (and |div|), or both; each part reads only its own operands.
+enum MassParts { MC_COEF = 1, MC_SU = 2, MC_ALL = 3 };
 template <class IO>
 __device__ __forceinline__ typename IO::T mass_coefp_io(const IO &io, const CaseDev &C, int i, int j,
                                                         CoefT<typename IO::T> &k, typename IO::T &su_out, int us,
-                                                        int vs)
+                                                        int vs, int parts = MC_ALL)
 {
     using T = typename IO::T;
     const LevelDev &L = io.L;
     const int nx = L.npx, ny = L.npy, q = j * nx + i, s = q - nx;
     const double axq = io.g(S_AREAX, q), ayq = io.g(S_AREAY, q);
-    T div = axq * io.ld(us, q) - axq * io.ld(us, q - 1) + ayq * io.ld(vs, q) - ayq * io.ld(vs, s);
-    T su = -div;
-    const double axw = io.g(S_AREAX, q - 1), ays = io.g(S_AREAY, s);
-    k.aw = axw * axw / io.ld(S_APU, q - 1);
-    k.ae = axq * axq / io.ld(S_APU, q);
-    k.as = ays * ays / io.ld(S_APV, s);
-    k.an = ayq * ayq / io.ld(S_APV, q);
-    k.ap = k.aw + k.ae + k.as + k.an + (double)(1 - L.tag[q]) * 1.0e30;
+    T div = T(0.0), su = T(0.0);
+    if (parts & MC_SU) {
+        div = axq * io.ld(us, q) - axq * io.ld(us, q - 1) + ayq * io.ld(vs, q) - ayq * io.ld(vs, s);
+        su = -div;
+    }
+    if (parts & MC_COEF) {
+        const double axw = io.g(S_AREAX, q - 1), ays = io.g(S_AREAY, s);
+        k.aw = axw * axw / io.ld(S_APU, q - 1);
+        k.ae = axq * axq / io.ld(S_APU, q);
+        k.as = ays * ays / io.ld(S_APV, s);
+        k.an = ayq * ayq / io.ld(S_APV, q);
+        k.ap = k.aw + k.ae + k.as + k.an + (double)(1 - L.tag[q]) * 1.0e30;
+    }
     const double diag = 1.0e30;
-    if (C.ibc_xm == 2 && i == 1) { k.ap = k.ap + diag; su = 0.0; }
-    if (C.ibc_xp == 2 && i == nx - 2) { k.ap = k.ap + diag; su = 0.0; }
-    if (C.ibc_ym == 2 && j == 1) { k.ap = k.ap + diag; su = 0.0; }
-    if (C.ibc_yp == 2 && j == ny - 2) { k.ap = k.ap + diag; su = 0.0; }
+    const bool cf = (parts & MC_COEF) != 0;
+    if (C.ibc_xm == 2 && i == 1) { if (cf) k.ap = k.ap + diag; su = 0.0; }
+    if (C.ibc_xp == 2 && i == nx - 2) { if (cf) k.ap = k.ap + diag; su = 0.0; }
+    if (C.ibc_ym == 2 && j == 1) { if (cf) k.ap = k.ap + diag; su = 0.0; }
+    if (C.ibc_yp == 2 && j == ny - 2) { if (cf) k.ap = k.ap + diag; su = 0.0; }
     su_out = su;
     return gabs(div);
 }
@@ -316,21 +324,30 @@ __device__ __forceinline__ double mass_coefp_values(const LevelDev &L, const Cas
 // are read from there and this cell's values are copied back to the fields.
 template <class IO>
 __device__ __forceinline__ typename IO::T cell_mass_coefp_io(const IO &io, const CaseDev &C, int i, int j,
-                                                             bool from_tmp = false)
+                                                             bool from_tmp = false, int parts = MC_ALL)
 {
     using T = typename IO::T;
     CoefT<T> k;
     T su;
     const int us = from_tmp ? S_TMP0 : S_U, vs = from_tmp ? S_TMP1 : S_V;
-    const T ad = mass_coefp_io(io, C, i, j, k, su, us, vs);
+    const T ad = mass_coefp_io(io, C, i, j, k, su, us, vs, parts);
     const int q = j * io.L.npx + i;
     if (from_tmp) {
         if (i <= io.L.npx - 3) io.st(S_U, q, io.ld(us, q));
         if (j <= io.L.npy - 3) io.st(S_V, q, io.ld(vs, q));
         io.st(S_SC, q, io.ld(S_TMP2, q));
     }
-    io.st(S_PP, q, T(0.0));
-    store_coef(io, EQ_PP, q, k, su);
+    if (parts == MC_ALL) {
+        io.st(S_PP, q, T(0.0));
+        store_coef(io, EQ_PP, q, k, su);
+    } else if (parts == MC_COEF) {
+        io.st(S_PP, q, T(0.0));
+        io.st(co_slot(EQ_PP, CK_AW), q, k.aw); io.st(co_slot(EQ_PP, CK_AE), q, k.ae);
+        io.st(co_slot(EQ_PP, CK_AS), q, k.as); io.st(co_slot(EQ_PP, CK_AN), q, k.an);
+        io.st(co_slot(EQ_PP, CK_AP), q, k.ap);
+    } else if (parts == MC_SU) {
+        io.st(co_slot(EQ_PP, CK_SU), q, su);
+    }
     return ad;
 }
 __device__ __forceinline__ double cell_mass_coefp(const LevelDev &L, const CaseDev &C, int i, int j,
@@ -339,16 +356,18 @@ __device__ __forceinline__ double cell_mass_coefp(const LevelDev &L, const CaseD
     return cell_mass_coefp_io(Prim{L}, C, i, j, from_tmp);
 }
 
-// update :1127-1152 (the obstacle pressure copy :1153-1177 is a separate gather)
+// update :1127-1152 (the obstacle pressure copy :1153-1177 is a separate gather);
+// `parts` bits 1, 2, 4 select the u, v, p updates (each reads only its own operands)
 template <class IO>
-__device__ __forceinline__ void cell_update_io(const IO &io, const CaseDev &C, int q)
+__device__ __forceinline__ void cell_update_io(const IO &io, const CaseDev &C, int q, int parts = 7)
 {
     using T = typename IO::T;
     const double ppref = 0.0;
     const T ppq = io.ld(S_PP, q);
-    io.st(S_U, q, io.ld(S_U, q) + io.g(S_AREAX, q) * (ppq - io.ld(S_PP, q + 1)) / io.ld(S_APU, q));
-    io.st(S_V, q, io.ld(S_V, q) + io.g(S_AREAY, q) * (ppq - io.ld(S_PP, q + io.L.npx)) / io.ld(S_APV, q));
-    io.st(S_P, q, io.ld(S_P, q) + C.relxp * (ppq - ppref));
+    if (parts & 1) io.st(S_U, q, io.ld(S_U, q) + io.g(S_AREAX, q) * (ppq - io.ld(S_PP, q + 1)) / io.ld(S_APU, q));
+    if (parts & 2)
+        io.st(S_V, q, io.ld(S_V, q) + io.g(S_AREAY, q) * (ppq - io.ld(S_PP, q + io.L.npx)) / io.ld(S_APV, q));
+    if (parts & 4) io.st(S_P, q, io.ld(S_P, q) + C.relxp * (ppq - ppref));
 }
 __device__ __forceinline__ void cell_update(const LevelDev &L, const CaseDev &C, int q) { cell_update_io(Prim{L}, C, q); }
 
@@ -456,20 +475,30 @@ __device__ __forceinline__ void cell_jacobi(const LevelDev &L, int e, int cur, i
 __device__ __forceinline__ void cell_gs(const LevelDev &L, int e, int phi, int q) { cell_gs_io(Prim{L}, e, phi, q); }
 
 // ------------------------------------------------------------ restriction
-// restv :1354-1389 at coarse interior cell (ic, jc)
+// restv :1354-1389 at coarse interior cell (ic, jc); `parts` bits 1, 2, 4, 8 select
+// u, v, p, sc (each reads only its own fine values)
 template <class IO>
-__device__ __forceinline__ void cell_restv_io(const IO &F, const IO &K, int ic, int jc)
+__device__ __forceinline__ void cell_restv_io(const IO &F, const IO &K, int ic, int jc, int parts = 15)
 {
     using T = typename IO::T;
     const int nxf = F.L.npx, qc = jc * K.L.npx + ic, q = 2 * jc * nxf + 2 * ic, qw = q - 1, qs = q - nxf;
-    const T u = (F.ld(S_U, q) * F.g(S_AREAX, q) + F.ld(S_U, qs) * F.g(S_AREAX, qs)) / (K.g(S_AREAX, qc) + 1.0e-30);
-    const T v = (F.ld(S_V, q) * F.g(S_AREAY, q) + F.ld(S_V, qw) * F.g(S_AREAY, qw)) / (K.g(S_AREAY, qc) + 1.0e-30);
-    const T p = 0.25 * (F.ld(S_P, q) + F.ld(S_P, qw) + F.ld(S_P, qs) + F.ld(S_P, qs - 1));
-    const T sc = 0.25 * (F.ld(S_SC, q) + F.ld(S_SC, qw) + F.ld(S_SC, qs) + F.ld(S_SC, qs - 1));
-    K.st(S_U, qc, u); K.st(S_V, qc, v); K.st(S_P, qc, p); K.st(S_SC, qc, sc);
+    T u = T(0.0), v = T(0.0), p = T(0.0), sc = T(0.0);
+    if (parts & 1)
+        u = (F.ld(S_U, q) * F.g(S_AREAX, q) + F.ld(S_U, qs) * F.g(S_AREAX, qs)) / (K.g(S_AREAX, qc) + 1.0e-30);
+    if (parts & 2)
+        v = (F.ld(S_V, q) * F.g(S_AREAY, q) + F.ld(S_V, qw) * F.g(S_AREAY, qw)) / (K.g(S_AREAY, qc) + 1.0e-30);
+    if (parts & 4) p = 0.25 * (F.ld(S_P, q) + F.ld(S_P, qw) + F.ld(S_P, qs) + F.ld(S_P, qs - 1));
+    if (parts & 8) sc = 0.25 * (F.ld(S_SC, q) + F.ld(S_SC, qw) + F.ld(S_SC, qs) + F.ld(S_SC, qs - 1));
+    if (parts & 1) K.st(S_U, qc, u);
+    if (parts & 2) K.st(S_V, qc, v);
+    if (parts & 4) K.st(S_P, qc, p);
+    if (parts & 8) K.st(S_SC, qc, sc);
     // the fine level does not change until the prolongation back into it, so these are
     // the R(x_f) the corrections subtract (prol_corr's r, same operations)
-    K.st(S_RU, qc, u); K.st(S_RV, qc, v); K.st(S_RP, qc, p); K.st(S_RSC, qc, sc);
+    if (parts & 1) K.st(S_RU, qc, u);
+    if (parts & 2) K.st(S_RV, qc, v);
+    if (parts & 4) K.st(S_RP, qc, p);
+    if (parts & 8) K.st(S_RSC, qc, sc);
 }
 __device__ __forceinline__ void cell_restv(const LevelDev &F, const LevelDev &K, int ic, int jc)
 {
@@ -588,26 +617,26 @@ __device__ __forceinline__ void cell_restrict(const LevelDev &F, const LevelDev 
 // coarse corrections c = x_c - R(x_f) at coarse interior cell (ic, jc):
 // prolu :1760-1777, prolv :1840-1856, prolp :1914-1928, prolsc :1981-1994
 template <class IO>
-__device__ __forceinline__ void cell_prol_corr_io(const IO &F, const IO &K, int ic, int jc)
+__device__ __forceinline__ void cell_prol_corr_io(const IO &F, const IO &K, int ic, int jc, int parts = 15)
 {
     using T = typename IO::T;
     const int nxf = F.L.npx, nxc = K.L.npx, nyc = K.L.npy, qc = jc * nxc + ic;
     const int q = 2 * jc * nxf + 2 * ic, qs = q - nxf;
-    if (ic <= nxc - 3) {
+    if ((parts & 1) && ic <= nxc - 3) {
         T r = (F.ld(S_U, q) * F.g(S_AREAX, q) + F.ld(S_U, qs) * F.g(S_AREAX, qs)) / (K.g(S_AREAX, qc) + 1.0E-30);
         K.st(S_CU, qc, K.ld(S_U, qc) - r);
     }
-    if (jc <= nyc - 3) {
+    if ((parts & 2) && jc <= nyc - 3) {
         T r = (F.ld(S_V, q) * F.g(S_AREAY, q) + F.ld(S_V, q - 1) * F.g(S_AREAY, q - 1)) / (K.g(S_AREAY, qc) + 1.0E-30);
         K.st(S_CV, qc, K.ld(S_V, qc) - r);
     }
-    {
+    if (parts & 4) {
         T r = 0.25 * (F.ld(S_P, q) + F.ld(S_P, q - 1) + F.ld(S_P, qs) + F.ld(S_P, qs - 1));
         T c = K.ld(S_P, qc) - r;
         if (F.g(S_SPU, q) > 1.0e10) c = 0.0;
         K.st(S_CP, qc, c);
     }
-    {
+    if (parts & 8) {
         T r = 0.25 * (F.ld(S_SC, q) + F.ld(S_SC, q - 1) + F.ld(S_SC, qs) + F.ld(S_SC, qs - 1));
         K.st(S_C, qc, K.ld(S_SC, qc) - r);
     }
@@ -661,7 +690,7 @@ struct ProlCorr {
 // corrections are formed here (ProlCorr), and the fine cell (2 ic, 2 jc) also writes
 // coarse cell (ic, jc)'s corrections to the arrays, as cell_prol_corr would have.
 template <class IO, bool FUSED = false>
-__device__ __forceinline__ void cell_prol_apply_io(const IO &F, const IO &K, int i, int j)
+__device__ __forceinline__ void cell_prol_apply_io(const IO &F, const IO &K, int i, int j, int parts = 15)
 {
     using T = typename IO::T;
     const int nxf = F.L.npx, nyf = F.L.npy, nxc = K.L.npx, nyc = K.L.npy, q = j * nxf + i;
@@ -675,7 +704,7 @@ __device__ __forceinline__ void cell_prol_apply_io(const IO &F, const IO &K, int
         K.st(S_C, qc, cr.sc(ic, jc));
     }
     // u faces, i in [1, nxf-3]: prolu :1782-1814
-    if (i <= nxf - 3) {
+    if ((parts & 1) && i <= nxf - 3) {
         const bool up = (j & 1) == 0;                  // even row: corr1 of jc = j/2
         const int jc = up ? j / 2 : (j + 1) / 2;       // odd row: corr2 of jc = (j+1)/2
         const int jn = up ? jc + 1 : jc - 1;           // the other row of the pair
@@ -701,7 +730,7 @@ __device__ __forceinline__ void cell_prol_apply_io(const IO &F, const IO &K, int
         F.st(S_U, q, u);
     }
     // v faces, j in [1, nyf-3]: prolv :1861-1888
-    if (j <= nyf - 3) {
+    if ((parts & 2) && j <= nyf - 3) {
         const bool right = (i & 1) == 0;               // even column: corr1 of ic = i/2
         const int ic = right ? i / 2 : (i + 1) / 2;
         const int in = right ? ic + 1 : ic - 1;        // the other column of the pair
@@ -732,10 +761,12 @@ __device__ __forceinline__ void cell_prol_apply_io(const IO &F, const IO &K, int
         const int ic = (i + 1) / 2, jc = (j + 1) / 2;
         const int in = (i & 1) == 0 ? ic + 1 : ic - 1;
         const int jn = (j & 1) == 0 ? jc + 1 : jc - 1;
-        F.st(S_P, q, F.ld(S_P, q) + (g1 * cr.p(ic, jc) + g2 * cr.p(in, jc) + g3 * cr.p(ic, jn)
-                                     + g4 * cr.p(in, jn)));
-        F.st(S_SC, q, F.ld(S_SC, q) + (g1 * cr.sc(ic, jc) + g2 * cr.sc(in, jc) + g3 * cr.sc(ic, jn)
-                                       + g4 * cr.sc(in, jn)));
+        if (parts & 4)
+            F.st(S_P, q, F.ld(S_P, q) + (g1 * cr.p(ic, jc) + g2 * cr.p(in, jc) + g3 * cr.p(ic, jn)
+                                         + g4 * cr.p(in, jn)));
+        if (parts & 8)
+            F.st(S_SC, q, F.ld(S_SC, q) + (g1 * cr.sc(ic, jc) + g2 * cr.sc(in, jc) + g3 * cr.sc(ic, jn)
+                                           + g4 * cr.sc(in, jn)));
     }
 }
 template <bool FUSED = false>

@@ -1983,8 +1983,11 @@ int mgfvm_adjoint(mgfvm_ctx *x, int ncycles)
         flat.reserve((size_t)prog_tot);
         for (auto &pg : progs) flat.insert(flat.end(), pg.begin(), pg.end());
         std::vector<CaseAdj> ha(n);
+        const char *gen = std::getenv("MGFVM_ADJOINT_GENERIC");
+        const int generic = gen && std::atoi(gen) == 1 ? 1 : 0;
         for (int c = 0; c < n; ++c)
-            ha[c] = CaseAdj{dprog + prog_off[c], (int)progs[c].size(), tape + tape_off[c], pacc + (size_t)c * 2 * MAXLEV};
+            ha[c] = CaseAdj{dprog + prog_off[c], (int)progs[c].size(), tape + tape_off[c], pacc + (size_t)c * 2 * MAXLEV,
+                            generic};
         if (cudaMemcpy(dprog, flat.data(), sizeof(Phase) * flat.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
             cudaMemcpy(dadj, ha.data(), sizeof(CaseAdj) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
             cudaMemcpy(dlive, live_off.data(), sizeof(long long) * n, cudaMemcpyHostToDevice) != cudaSuccess ||

@@ -162,3 +162,16 @@ def test_adjoint_with_a_diverging_case_in_the_batch(oracle_built):
         assert np.isnan(s.adjoint_gradient(1, allow_nonfinite=True)[2])
         good = s.adjoint_gradient(0)
     _close(good, _forward_mode(cases[0], profs[0], cycles), "the finite case beside a diverging one")
+
+
+def test_closed_form_transposes_equal_the_probed_ones(monkeypatch, oracle_built):
+    """The phases transposed in closed form (the red-black half-sweep) give what
+    transposing them by dual-number probes gives, to rounding."""
+    cfg = small_cases()["obs_gs_touch"]
+    prof = 1.0 + 0.05 * np.cos(np.arange(cfg.nfy))
+    closed = _adjoint([cfg], [prof], 3)[0]
+    monkeypatch.setenv("MGFVM_ADJOINT_GENERIC", "1")
+    probed = _adjoint([cfg], [prof], 3)[0]
+    a = np.concatenate([closed[1], closed[2:]])
+    b = np.concatenate([probed[1], probed[2:]])
+    assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()
