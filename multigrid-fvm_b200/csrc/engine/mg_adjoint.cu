@@ -372,24 +372,52 @@ __device__ __forceinline__ void adj_cell(const CaseDev &C, const CaseTan &B, con
     }
 }
 
+// The cells of a half-sweep phase with their index in its colour-only tape.
+template <class Fn>
+__device__ __forceinline__ void gs_cells(const LevelDev &L, const Phase &P, Fn f)
+{
+    const Box d = box_eq(L.npx, L.npy, P.a);
+    if (d.wi <= 0 || d.wj <= 0) return;
+    const int wr = (d.wi + 1) >> 1, n = wr * d.wj;
+    for (int t = wk_id(); t < n; t += wk_n()) {
+        const int j = d.j0 + t / wr;
+        const int i = d.i0 + (((d.i0 + j) & 1) != P.b ? 1 : 0) + 2 * (t % wr);
+        if (i <= d.i0 + d.wi - 1) f(i, j, t);
+    }
+}
+
+// A half-sweep, taped, in one pass: each cell's old value to the tape, then its update
+// (its neighbours are of the other colour, which the half-sweep does not write).
+__device__ __forceinline__ void fwd_gs_cell(const LevelDev &L, int e, int i, int j, double *tape, int t)
+{
+    const int q = j * L.npx + i;
+    double *f = L.f[field_of(e)];
+    tape[t] = f[q];
+    cell_gs_io(Prim{L}, e, field_of(e), q);
+}
+
 // The transpose of one red-black half-sweep cell, phi_c = (sum a_nb phi_nb + su) / ap
-// (gs_value), written out: d/da_nb = phi_nb / ap, d/dphi_nb = a_nb / ap, d/dsu = 1 / ap,
-// d/dap = -phi_c / ap, the partial derivatives the dual arithmetic of adj_cell forms,
-// here with the adjoint divided by ap once (the same numbers to rounding) at one
-// evaluation instead of eleven.  The cell's coefficients are read by no other cell of
-// the half-sweep, so their adjoints take plain additions; the neighbours' take atomics.
-__device__ __forceinline__ void adj_gs_cell(const LevelDev &L, const LevelTan &B, int e, int i, int j)
+// (gs_value), in closed form: d/da_nb = phi_nb / ap, d/dphi_nb = a_nb / ap, d/dsu =
+// 1 / ap, d/dap = -phi_c / ap, the partial derivatives the dual arithmetic of adj_cell
+// forms, here with the adjoint divided by ap once (the same numbers to rounding).  The
+// cell's new value phi_c is read from the field before the tape restores the old one
+// (its neighbours are unchanged by the half-sweep).  The cell's coefficients are read
+// by no other cell of the half-sweep, so their adjoints take plain additions; the
+// neighbours' take atomics.
+__device__ __forceinline__ void adj_gs_cell(const LevelDev &L, const LevelTan &B, int e, int i, int j,
+                                            const double *tape, int t)
 {
     const int nx = L.npx, q = j * nx + i, phi = field_of(e);
+    double *f = L.f[phi];
+    const double val = f[q];
+    f[q] = tape[t];
     double *yp = B.t[phi] + q;
     const double yb = *yp;
     *yp = 0.0;
     if (yb == 0.0) return;
     const double aw = L.f[co_slot(e, CK_AW)][q], ae = L.f[co_slot(e, CK_AE)][q], as = L.f[co_slot(e, CK_AS)][q],
-                 an = L.f[co_slot(e, CK_AN)][q], ap = L.f[co_slot(e, CK_AP)][q], su = L.f[co_slot(e, CK_SU)][q];
-    const double *f = L.f[phi];
+                 an = L.f[co_slot(e, CK_AN)][q], ap = L.f[co_slot(e, CK_AP)][q];
     const double pw = f[q - 1], pe = f[q + 1], ps = f[q - nx], pn = f[q + nx];
-    const double val = gs_value(aw, ae, as, an, ap, su, pw, pe, ps, pn);
     const double ya = yb / ap;
     B.t[co_slot(e, CK_AW)][q] += ya * pw;
     B.t[co_slot(e, CK_AE)][q] += ya * pe;
@@ -402,6 +430,493 @@ __device__ __forceinline__ void adj_gs_cell(const LevelDev &L, const LevelTan &B
     atomicAdd(b + q + 1, ya * ae);
     atomicAdd(b + q - nx, ya * as);
     atomicAdd(b + q + nx, ya * an);
+}
+
+// ------------------------------- closed-form transposes: the assembly family
+// coef_u, coef_v and coef_sc (the hybrid-scheme coefficients from the live fluxes) and
+// their users — the assemblies (coefu + umom, coefv + vmom, coefsc + scalar), the
+// fine residuals and the FAS defects — transposed by hand with the partial derivatives
+// the dual arithmetic forms (so the same numbers as the probes, to rounding): at a
+// non-smooth point max(|c|, d) takes the mean of both sides, |c| at 0 the derivative 0.
+// The forward values are recomputed with the engine's own routines (Prim).
+
+// adjoints of a level's arrays: take (and clear) an output's, add to an input's
+struct Bars {
+    const LevelTan &B;
+    __device__ __forceinline__ double take(int s, int q) const
+    {
+        double *b = B.t[s] + q;
+        const double y = *b;
+        *b = 0.0;
+        return y;
+    }
+    __device__ __forceinline__ void add(int s, int q, double v) const
+    {
+        if (v != 0.0) atomicAdd(B.t[s] + q, v);
+    }
+};
+
+// d/dc and d/dd of max(|c|, d) + sg c (sg = +1: hyb_p, -1: hyb_m)
+__device__ __forceinline__ void hyb_partials(double c, double d, double sg, double &dc, double &dd)
+{
+    const double ac = fabs(c), sc = c > 0.0 ? 1.0 : c < 0.0 ? -1.0 : 0.0;
+    if (ac > d) { dc = sc; dd = 0.0; }
+    else if (d > ac) { dc = 0.0; dd = 1.0; }
+    else { dc = 0.5 * sc; dd = 0.5; }
+    dc += sg;
+}
+
+// the live fluxes' inputs: cx(q) = 0.5 u(q) Ax(q), cy(q) = 0.5 v(q) Ay(q)
+__device__ __forceinline__ void flux_x_adj(const LevelDev &L, const Bars &b, int q, double bc)
+{
+    b.add(S_U, q, (0.5 * bc) * L.f[S_AREAX][q]);
+}
+__device__ __forceinline__ void flux_y_adj(const LevelDev &L, const Bars &b, int q, double bc)
+{
+    b.add(S_V, q, (0.5 * bc) * L.f[S_AREAY][q]);
+}
+
+// Transpose of coef_u at u face (i, j): output adjoints (aw .. ap) -> u, v adjoints;
+// returns the adjoint of amu.
+__device__ double coef_u_adj(const LevelDev &L, const Bars &b, int i, int j, double baw, double bae, double bas,
+                             double ban, double bap)
+{
+    const int nx = L.npx, q = j * nx + i, s = q - nx, top = L.npy - 2;
+    const FluxLive fl(L);
+    const double cq = fl.x(q);
+    const double cxm = 0.5 * (cq + fl.x(q - 1)), cxp = 0.5 * (cq + fl.x(q + 1));
+    const double cym = 0.5 * (fl.y(s) + fl.y(s + 1)), cyp = 0.5 * (fl.y(q) + fl.y(q + 1));
+    const double gx = L.f[S_AREAX][q] / L.dx, gy = L.f[S_AREAY][q] / L.dy;
+    const double dxm = L.amu * gx, dym = L.amu * gy;
+    double bamu = 0.0;
+    // the wall-shear additions to an / as and ap (rows npy-2 and 1)
+    if (j == 1) bamu += (bas + bap) * (L.f[S_AREAY][top * nx + i] / L.dy);
+    if (j == top) bamu += (ban + bap) * gy;
+    baw += bap; bae += bap; bas += bap; ban += bap;      // ap = aw + ae + as + an
+    double dc, dd, bdx = 0.0, bdy = 0.0;
+    hyb_partials(cxm, dxm, 1.0, dc, dd);  const double bcxm = baw * dc; bdx += baw * dd;
+    hyb_partials(cxp, dxm, -1.0, dc, dd); const double bcxp = bae * dc; bdx += bae * dd;
+    hyb_partials(cym, dym, 1.0, dc, dd);  const double bcym = bas * dc; bdy += bas * dd;
+    hyb_partials(cyp, dym, -1.0, dc, dd); const double bcyp = ban * dc; bdy += ban * dd;
+    bamu += bdx * gx + bdy * gy;
+    flux_x_adj(L, b, q, 0.5 * bcxm + 0.5 * bcxp);
+    flux_x_adj(L, b, q - 1, 0.5 * bcxm);
+    flux_x_adj(L, b, q + 1, 0.5 * bcxp);
+    flux_y_adj(L, b, s, 0.5 * bcym);
+    flux_y_adj(L, b, s + 1, 0.5 * bcym);
+    flux_y_adj(L, b, q, 0.5 * bcyp);
+    flux_y_adj(L, b, q + 1, 0.5 * bcyp);
+    return bamu;
+}
+
+// Transpose of coef_v at v face (i, j); returns the adjoint of amu.
+__device__ double coef_v_adj(const LevelDev &L, const Bars &b, int i, int j, double baw, double bae, double bas,
+                             double ban, double bap)
+{
+    const int nx = L.npx, q = j * nx + i, n = q + nx, s = q - nx, rgt = nx - 2;
+    const FluxLive fl(L);
+    const double cxm = 0.5 * (fl.x(q - 1) + fl.x(n - 1)), cxp = 0.5 * (fl.x(q) + fl.x(n));
+    const double cyq = fl.y(q);
+    const double cym = 0.5 * (cyq + fl.y(s)), cyp = 0.5 * (cyq + fl.y(n));
+    const double gx = L.f[S_AREAX][q] / L.dx, gy = L.f[S_AREAY][q] / L.dy;
+    const double dx_ = L.amu * gx, dy_ = L.amu * gy;
+    double bamu = 0.0;
+    // the side-wall additions to aw / ae and ap (columns 1 and npx-2)
+    if (i == 1) bamu += (baw + bap) * (L.f[S_AREAY][j * nx + rgt] / L.dy);
+    if (i == rgt) bamu += (bae + bap) * gy;
+    baw += bap; bae += bap; bas += bap; ban += bap;
+    double dc, dd, bdx = 0.0, bdy = 0.0;
+    hyb_partials(cxm, dx_, 1.0, dc, dd);  const double bcxm = baw * dc; bdx += baw * dd;
+    hyb_partials(cxp, dx_, -1.0, dc, dd); const double bcxp = bae * dc; bdx += bae * dd;
+    hyb_partials(cym, dy_, 1.0, dc, dd);  const double bcym = bas * dc; bdy += bas * dd;
+    hyb_partials(cyp, dy_, -1.0, dc, dd); const double bcyp = ban * dc; bdy += ban * dd;
+    bamu += bdx * gx + bdy * gy;
+    flux_x_adj(L, b, q - 1, 0.5 * bcxm);
+    flux_x_adj(L, b, n - 1, 0.5 * bcxm);
+    flux_x_adj(L, b, q, 0.5 * bcxp);
+    flux_x_adj(L, b, n, 0.5 * bcxp);
+    flux_y_adj(L, b, q, 0.5 * bcym + 0.5 * bcyp);
+    flux_y_adj(L, b, s, 0.5 * bcym);
+    flux_y_adj(L, b, n, 0.5 * bcyp);
+    return bamu;
+}
+
+// Transpose of coef_sc at cell (i, j), obstacle-face additions included; returns the
+// adjoint of amusc.
+__device__ double coef_sc_adj(const LevelDev &L, const Bars &b, int i, int j, double baw, double bae, double bas,
+                              double ban, double bap)
+{
+    const int nx = L.npx, q = j * nx + i, s = q - nx;
+    const FluxLive fl(L);
+    const double *AX = L.f[S_AREAX], *AY = L.f[S_AREAY];
+    const double gxm = AX[q - 1] / L.dx, gym = AY[s] / L.dy, gxp = AX[q] / L.dx, gyp = AY[q] / L.dy;
+    const double a = L.amusc;
+    const double dxm = a * gxm, dym = a * gym, dxp = a * gxp, dyp = a * gyp;
+    double bamusc = 0.0;
+    if (L.seq) {
+        const unsigned code = L.seq[q];
+        const int cnt = (int)(code >> 28);
+        for (int t = 0; t < cnt; ++t) {
+            const int d = (int)((code >> (2 * t)) & 3u);
+            if (d == 0) bamusc += (bae + bap) * (AX[q + 1] / L.dx);
+            else if (d == 1) bamusc += (baw + bap) * (AX[q - 1] / L.dx);
+            else if (d == 2) bamusc += (ban + bap) * (AY[q + nx] / L.dy);
+            else bamusc += (bas + bap) * (AY[q - nx] / L.dy);
+        }
+    }
+    baw += bap; bae += bap; bas += bap; ban += bap;
+    double dc, dd;
+    hyb_partials(fl.x(q - 1), dxm, 1.0, dc, dd); const double bw = baw * dc; bamusc += baw * dd * gxm;
+    hyb_partials(fl.x(q), dxp, -1.0, dc, dd);    const double be = bae * dc; bamusc += bae * dd * gxp;
+    hyb_partials(fl.y(s), dym, 1.0, dc, dd);     const double bs = bas * dc; bamusc += bas * dd * gym;
+    hyb_partials(fl.y(q), dyp, -1.0, dc, dd);    const double bn = ban * dc; bamusc += ban * dd * gyp;
+    flux_x_adj(L, b, q - 1, bw);
+    flux_x_adj(L, b, q, be);
+    flux_y_adj(L, b, s, bs);
+    flux_y_adj(L, b, q, bn);
+    return bamusc;
+}
+
+// Transposes of the assemblies at one cell (P_ASM_U / V / SC); the parameter adjoint
+// goes to `pa`.
+__device__ void asm_u_adj(const CaseDev &C, const LevelDev &L, const Bars &b, int i, int j, ParAcc &pa)
+{
+    const int q = j * L.npx + i;
+    const double baw = b.take(co_slot(EQ_U, CK_AW), q), bae = b.take(co_slot(EQ_U, CK_AE), q),
+                 bas = b.take(co_slot(EQ_U, CK_AS), q), ban = b.take(co_slot(EQ_U, CK_AN), q);
+    const double bapo = b.take(co_slot(EQ_U, CK_AP), q) + b.take(S_APU, q), bsu = b.take(co_slot(EQ_U, CK_SU), q);
+    if (baw == 0.0 && bae == 0.0 && bas == 0.0 && ban == 0.0 && bapo == 0.0 && bsu == 0.0) return;
+    const Coef k = coef_u(Prim{L}, FluxLive(L), i, j);
+    const double ax = L.f[S_AREAX][q], rm = C.relxm, rm1 = 1.0 - C.relxm;
+    const double apr = k.ap / rm;
+    // su = ax (p_P - p_E) + rm1 (ap / rm) u + resu + ...; ap_out = ap / rm + spu
+    b.add(S_P, q, bsu * ax);
+    b.add(S_P, q + 1, -(bsu * ax));
+    b.add(S_U, q, bsu * (rm1 * apr));
+    b.add(S_RESU, q, bsu);
+    const double bap = (bapo + bsu * (rm1 * L.f[S_U][q])) / rm;
+    pa.amu_f += coef_u_adj(L, b, i, j, baw, bae, bas, ban, bap);
+}
+__device__ void asm_v_adj(const CaseDev &C, const LevelDev &L, const Bars &b, int i, int j, ParAcc &pa)
+{
+    const int q = j * L.npx + i;
+    const double baw = b.take(co_slot(EQ_V, CK_AW), q), bae = b.take(co_slot(EQ_V, CK_AE), q),
+                 bas = b.take(co_slot(EQ_V, CK_AS), q), ban = b.take(co_slot(EQ_V, CK_AN), q);
+    const double bapo = b.take(co_slot(EQ_V, CK_AP), q) + b.take(S_APV, q), bsu = b.take(co_slot(EQ_V, CK_SU), q);
+    if (baw == 0.0 && bae == 0.0 && bas == 0.0 && ban == 0.0 && bapo == 0.0 && bsu == 0.0) return;
+    const Coef k = coef_v(Prim{L}, FluxLive(L), i, j);
+    const double ay = L.f[S_AREAY][q], rm = C.relxm, rm1 = 1.0 - C.relxm;
+    const double apr = k.ap / rm;
+    b.add(S_P, q, bsu * ay);
+    b.add(S_P, q + L.npx, -(bsu * ay));
+    b.add(S_V, q, bsu * (rm1 * apr));
+    b.add(S_RESV, q, bsu);
+    const double bap = (bapo + bsu * (rm1 * L.f[S_V][q])) / rm;
+    pa.amu_f += coef_v_adj(L, b, i, j, baw, bae, bas, ban, bap);
+}
+__device__ void asm_sc_adj(const LevelDev &L, const Bars &b, int i, int j, ParAcc &pa)
+{
+    const int q = j * L.npx + i;
+    const double baw = b.take(co_slot(EQ_SC, CK_AW), q), bae = b.take(co_slot(EQ_SC, CK_AE), q),
+                 bas = b.take(co_slot(EQ_SC, CK_AS), q), ban = b.take(co_slot(EQ_SC, CK_AN), q);
+    const double bap = b.take(co_slot(EQ_SC, CK_AP), q), bsu = b.take(co_slot(EQ_SC, CK_SU), q);
+    if (baw == 0.0 && bae == 0.0 && bas == 0.0 && ban == 0.0 && bap == 0.0 && bsu == 0.0) return;
+    b.add(S_RESSC, q, bsu);                          // su = spsc sc_obs + ressc; ap += spsc
+    pa.amusc_f += coef_sc_adj(L, b, i, j, baw, bae, bas, ban, bap);
+}
+
+// Transposes of the residuals resid_u / resid_v / resid_sc at (i, j) of level L given
+// the adjoint br of the residual; `fine`: the fine-level form (with the defect term
+// and the zero where the face area is 0).  Returns the parameter adjoint (amu, or
+// amusc for the scalar).
+__device__ double resid_u_adj(const LevelDev &L, const Bars &b, int i, int j, bool fine, double br)
+{
+    const int nx = L.npx, q = j * nx + i;
+    const double ax = L.f[S_AREAX][q];
+    if (br == 0.0 || (fine && ax == 0.0)) return 0.0;
+    const Coef k = coef_u(Prim{L}, FluxLive(L), i, j);
+    const double *u = L.f[S_U];
+    b.add(S_U, q - 1, br * k.aw);
+    b.add(S_U, q + 1, br * k.ae);
+    b.add(S_U, q - nx, br * k.as);
+    b.add(S_U, q + nx, br * k.an);
+    b.add(S_U, q, -(br * k.ap));
+    b.add(S_P, q, br * ax);
+    b.add(S_P, q + 1, -(br * ax));
+    if (fine) b.add(S_RESU, q, br);
+    return coef_u_adj(L, b, i, j, br * u[q - 1], br * u[q + 1], br * u[q - nx], br * u[q + nx], -(br * u[q]));
+}
+__device__ double resid_v_adj(const LevelDev &L, const Bars &b, int i, int j, bool fine, double br)
+{
+    const int nx = L.npx, q = j * nx + i;
+    const double ay = L.f[S_AREAY][q];
+    if (br == 0.0 || (fine && ay == 0.0)) return 0.0;
+    const Coef k = coef_v(Prim{L}, FluxLive(L), i, j);
+    const double *v = L.f[S_V];
+    b.add(S_V, q - 1, br * k.aw);
+    b.add(S_V, q + 1, br * k.ae);
+    b.add(S_V, q - nx, br * k.as);
+    b.add(S_V, q + nx, br * k.an);
+    b.add(S_V, q, -(br * k.ap));
+    b.add(S_P, q, br * ay);
+    b.add(S_P, q + nx, -(br * ay));
+    if (fine) b.add(S_RESV, q, br);
+    return coef_v_adj(L, b, i, j, br * v[q - 1], br * v[q + 1], br * v[q - nx], br * v[q + nx], -(br * v[q]));
+}
+__device__ double resid_sc_adj(const LevelDev &L, const Bars &b, int i, int j, bool fine, double br)
+{
+    const int nx = L.npx, q = j * nx + i;
+    if (br == 0.0) return 0.0;
+    const Coef k = coef_sc(Prim{L}, FluxLive(L), i, j);
+    const double *c = L.f[S_SC];
+    b.add(S_SC, q - 1, br * k.aw);
+    b.add(S_SC, q + 1, br * k.ae);
+    b.add(S_SC, q - nx, br * k.as);
+    b.add(S_SC, q + nx, br * k.an);
+    b.add(S_SC, q, -(br * k.ap));
+    if (fine) b.add(S_RESSC, q, br);
+    return coef_sc_adj(L, b, i, j, br * c[q - 1], br * c[q + 1], br * c[q - nx], br * c[q + nx], -(br * c[q]));
+}
+
+// P_FINE_RES at fine cell (i, j): the residual of equation `which` into its buffer.
+__device__ void fine_res_adj(const LevelDev &F, const Bars &b, int i, int j, int which, ParAcc &pa)
+{
+    const int q = j * F.npx + i;
+    if (which == 0) pa.amu_f += resid_u_adj(F, b, i, j, true, b.take(S_TMP0, q));
+    else if (which == 1) pa.amu_f += resid_v_adj(F, b, i, j, true, b.take(S_TMP1, q));
+    else pa.amusc_f += resid_sc_adj(F, b, i, j, true, b.take(S_TMP2, q));
+}
+
+// P_RESTRICT at coarse cell (ic, jc): the FAS defect = restricted fine residuals
+// (cell_restrict_io's weights) - the coarse residual of the restricted state.
+__device__ void restrict_adj(const LevelDev &F, const LevelDev &K, const Bars &bf, const Bars &bk, int ic, int jc,
+                             int which, ParAcc &pa)
+{
+    const int nxf = F.npx, qc = jc * K.npx + ic, q = 2 * jc * nxf + 2 * ic;
+    if (which == 0) {
+        const double y = bk.take(S_RESU, qc);
+        if (y == 0.0) return;
+        bf.add(S_TMP0, q, y); bf.add(S_TMP0, q - nxf, y);
+        bf.add(S_TMP0, q - 1, 0.5 * y); bf.add(S_TMP0, q - 1 - nxf, 0.5 * y);
+        bf.add(S_TMP0, q + 1, 0.5 * y); bf.add(S_TMP0, q + 1 - nxf, 0.5 * y);
+        pa.amu_k += resid_u_adj(K, bk, ic, jc, false, -y);
+    } else if (which == 1) {
+        const double y = bk.take(S_RESV, qc);
+        if (y == 0.0) return;
+        bf.add(S_TMP1, q, y); bf.add(S_TMP1, q - 1, y);
+        bf.add(S_TMP1, q - nxf, 0.5 * y); bf.add(S_TMP1, q - nxf - 1, 0.5 * y);
+        bf.add(S_TMP1, q + nxf, 0.5 * y); bf.add(S_TMP1, q + nxf - 1, 0.5 * y);
+        pa.amu_k += resid_v_adj(K, bk, ic, jc, false, -y);
+    } else {
+        const double y = bk.take(S_RESSC, qc);
+        if (y == 0.0) return;
+        bf.add(S_TMP2, q, y); bf.add(S_TMP2, q - nxf, y);
+        bf.add(S_TMP2, q - 1, y); bf.add(S_TMP2, q - 1 - nxf, y);
+        pa.amusc_k += resid_sc_adj(K, bk, ic, jc, false, -y);
+    }
+}
+
+// P_MASS_COEFP at interior cell (i, j).  MC_COEF: p' = 0 and aw = A_w^2 / apu_W ...,
+// ap = their sum + constants (d(a / x)/dx = -(a / x) / x, the dual division's);
+// MC_SU: su = -div, or 0 on a p' Dirichlet row.
+__device__ void mass_coefp_adj(const CaseDev &C, const LevelDev &L, const Bars &b, int i, int j, int parts)
+{
+    const int nx = L.npx, ny = L.npy, q = j * nx + i, s = q - nx;
+    const double *AX = L.f[S_AREAX], *AY = L.f[S_AREAY];
+    if (parts & MC_COEF) {
+        b.take(S_PP, q);
+        const double bap = b.take(co_slot(EQ_PP, CK_AP), q);
+        const double baw = b.take(co_slot(EQ_PP, CK_AW), q) + bap, bae = b.take(co_slot(EQ_PP, CK_AE), q) + bap,
+                     bas = b.take(co_slot(EQ_PP, CK_AS), q) + bap, ban = b.take(co_slot(EQ_PP, CK_AN), q) + bap;
+        const double axw = AX[q - 1], axq = AX[q], ays = AY[s], ayq = AY[q];
+        const double *apu = L.f[S_APU], *apv = L.f[S_APV];
+        const double qw = axw * axw / apu[q - 1], qe = axq * axq / apu[q];
+        const double qs = ays * ays / apv[s], qn = ayq * ayq / apv[q];
+        b.add(S_APU, q - 1, baw * (-(qw * 1.0) / apu[q - 1]));
+        b.add(S_APU, q, bae * (-(qe * 1.0) / apu[q]));
+        b.add(S_APV, s, bas * (-(qs * 1.0) / apv[s]));
+        b.add(S_APV, q, ban * (-(qn * 1.0) / apv[q]));
+    }
+    if (parts & MC_SU) {
+        const double bsu = b.take(co_slot(EQ_PP, CK_SU), q);
+        const bool pinned = (C.ibc_xm == 2 && i == 1) || (C.ibc_xp == 2 && i == nx - 2) || (C.ibc_ym == 2 && j == 1) ||
+                            (C.ibc_yp == 2 && j == ny - 2);
+        if (bsu == 0.0 || pinned) return;
+        // su = -(Ax u_P - Ax u_W + Ay v_P - Ay v_S)
+        const double axq = AX[q], ayq = AY[q];
+        b.add(S_U, q, -(bsu * axq));
+        b.add(S_U, q - 1, bsu * axq);
+        b.add(S_V, q, -(bsu * ayq));
+        b.add(S_V, s, bsu * ayq);
+    }
+}
+
+// P_UPDATE at interior cell q: u += Ax (p'_P - p'_E) / apu (parts & 1), v likewise with
+// p'_N and apv (2), p += relxp p'_P (4).  Each field's own adjoint passes through
+// unchanged (d new / d old = 1).
+__device__ void update_adj(const CaseDev &C, const LevelDev &L, const Bars &b, int q, int parts)
+{
+    const double *pp = L.f[S_PP];
+    if (parts & 1) {
+        const double y = b.B.t[S_U][q];
+        if (y != 0.0) {
+            const double a = L.f[S_AREAX][q], apu = L.f[S_APU][q];
+            const double r = a * (pp[q] - pp[q + 1]) / apu;
+            b.add(S_PP, q, y * (a / apu));
+            b.add(S_PP, q + 1, -(y * (a / apu)));
+            b.add(S_APU, q, y * (-(r * 1.0) / apu));
+        }
+    }
+    if (parts & 2) {
+        const double y = b.B.t[S_V][q];
+        if (y != 0.0) {
+            const int n = q + L.npx;
+            const double a = L.f[S_AREAY][q], apv = L.f[S_APV][q];
+            const double r = a * (pp[q] - pp[n]) / apv;
+            b.add(S_PP, q, y * (a / apv));
+            b.add(S_PP, n, -(y * (a / apv)));
+            b.add(S_APV, q, y * (-(r * 1.0) / apv));
+        }
+    }
+    if (parts & 4) {
+        const double y = b.B.t[S_P][q];
+        if (y != 0.0) b.add(S_PP, q, y * C.relxp);
+    }
+}
+
+// The transfers (linear maps of the fine and coarse states).
+// P_RESTV at coarse cell (ic, jc): coarse x and R(x_f) of part `parts` (1 u, 2 v, 4 p, 8 sc).
+__device__ void restv_adj(const LevelDev &F, const LevelDev &K, const Bars &bf, const Bars &bk, int ic, int jc,
+                          int parts)
+{
+    const int nxf = F.npx, qc = jc * K.npx + ic, q = 2 * jc * nxf + 2 * ic, qw = q - 1, qs = q - nxf;
+    if (parts & 1) {
+        const double y = bk.take(S_U, qc) + bk.take(S_RU, qc);
+        const double den = K.f[S_AREAX][qc] + 1.0e-30;
+        bf.add(S_U, q, y * (F.f[S_AREAX][q] / den));
+        bf.add(S_U, qs, y * (F.f[S_AREAX][qs] / den));
+    }
+    if (parts & 2) {
+        const double y = bk.take(S_V, qc) + bk.take(S_RV, qc);
+        const double den = K.f[S_AREAY][qc] + 1.0e-30;
+        bf.add(S_V, q, y * (F.f[S_AREAY][q] / den));
+        bf.add(S_V, qw, y * (F.f[S_AREAY][qw] / den));
+    }
+    for (int k = 2; k < 4; ++k) {
+        if (!(parts & (1 << k))) continue;
+        const int x = k == 2 ? S_P : S_SC, rx = k == 2 ? S_RP : S_RSC;
+        const double y = 0.25 * (bk.take(x, qc) + bk.take(rx, qc));
+        bf.add(x, q, y); bf.add(x, qw, y); bf.add(x, qs, y); bf.add(x, qs - 1, y);
+    }
+}
+
+// P_PROL_CORR at coarse interior cell (ic, jc): c = x_c - R(x_f) (p's zeroed under solids).
+__device__ void prol_corr_adj(const LevelDev &F, const LevelDev &K, const Bars &bf, const Bars &bk, int ic, int jc,
+                              int parts)
+{
+    const int nxf = F.npx, nxc = K.npx, nyc = K.npy, qc = jc * nxc + ic, q = 2 * jc * nxf + 2 * ic, qs = q - nxf;
+    if ((parts & 1) && ic <= nxc - 3) {
+        const double y = bk.take(S_CU, qc);
+        const double den = K.f[S_AREAX][qc] + 1.0E-30;
+        bk.add(S_U, qc, y);
+        bf.add(S_U, q, -(y * (F.f[S_AREAX][q] / den)));
+        bf.add(S_U, qs, -(y * (F.f[S_AREAX][qs] / den)));
+    }
+    if ((parts & 2) && jc <= nyc - 3) {
+        const double y = bk.take(S_CV, qc);
+        const double den = K.f[S_AREAY][qc] + 1.0E-30;
+        bk.add(S_V, qc, y);
+        bf.add(S_V, q, -(y * (F.f[S_AREAY][q] / den)));
+        bf.add(S_V, q - 1, -(y * (F.f[S_AREAY][q - 1] / den)));
+    }
+    for (int k = 2; k < 4; ++k) {
+        if (!(parts & (1 << k))) continue;
+        const int x = k == 2 ? S_P : S_SC;
+        const double y = bk.take(k == 2 ? S_CP : S_C, qc);
+        if (k == 2 && F.f[S_SPU][q] > 1.0e10) continue;
+        bk.add(x, qc, y);
+        const double r = -(0.25 * y);
+        bf.add(x, q, r); bf.add(x, q - 1, r); bf.add(x, qs, r); bf.add(x, qs - 1, r);
+    }
+}
+
+// P_PROL_APPLY at fine interior cell (i, j): the gather of cell_prol_apply_io (the
+// corrections read from the arrays); the fine field's own adjoint passes through.
+__device__ void prol_apply_adj(const LevelDev &F, const LevelDev &K, const Bars &bf, const Bars &bk, int i, int j,
+                               int parts)
+{
+    const int nxf = F.npx, nyf = F.npy, nxc = K.npx, nyc = K.npy, q = j * nxf + i;
+    const double f1 = 3. / 4., f2 = 1. / 4.;
+    const double *spu = F.f[S_SPU], *spv = F.f[S_SPV];
+    auto corr = [&](int slot, int ia, int ja, int ib, int jb, double w) {
+        bk.add(slot, ja * nxc + ia, w * f1);
+        bk.add(slot, jb * nxc + ib, w * f2);
+    };
+    if ((parts & 1) && i <= nxf - 3) {
+        const double y = bf.B.t[S_U][q];
+        if (y != 0.0) {
+            const bool up = (j & 1) == 0;
+            const int jc = up ? j / 2 : (j + 1) / 2, jn = up ? jc + 1 : jc - 1;
+            if ((i & 1) == 0) {
+                const int ic = i / 2;
+                if (!(spu[2 * jc * nxf + 2 * ic] > 1.0e10)) corr(S_CU, ic, jc, ic, jn, y);
+            } else {
+                const int ia = (i - 1) / 2, ib = (i + 1) / 2;
+                if (ia >= 1 && !(spu[2 * jc * nxf + 2 * ia] > 1.0e10)) corr(S_CU, ia, jc, ia, jn, 0.5 * y);
+                if (ib <= nxc - 3 && !(spu[2 * jc * nxf + 2 * ib] > 1.0e10)) corr(S_CU, ib, jc, ib, jn, 0.5 * y);
+            }
+        }
+    }
+    if ((parts & 2) && j <= nyf - 3) {
+        const double y = bf.B.t[S_V][q];
+        if (y != 0.0) {
+            const bool right = (i & 1) == 0;
+            const int ic = right ? i / 2 : (i + 1) / 2, in = right ? ic + 1 : ic - 1;
+            if ((j & 1) == 0) {
+                const int jc = j / 2;
+                if (!(spv[2 * jc * nxf + 2 * ic] > 1.0e10)) corr(S_CV, ic, jc, in, jc, y);
+            } else {
+                const int ja = (j - 1) / 2, jb = (j + 1) / 2;
+                if (ja >= 1 && !(spv[2 * ja * nxf + 2 * ic] > 1.0e10)) corr(S_CV, ic, ja, in, ja, 0.5 * y);
+                if (jb <= nyc - 3 && !(spv[2 * jb * nxf + 2 * ic] > 1.0e10)) corr(S_CV, ic, jb, in, jb, 0.5 * y);
+            }
+        }
+    }
+    const double g1 = 9. / 16., g2 = 3. / 16., g3 = 3. / 16., g4 = 1. / 16.;
+    const int ic = (i + 1) / 2, jc = (j + 1) / 2;
+    const int in = (i & 1) == 0 ? ic + 1 : ic - 1, jn = (j & 1) == 0 ? jc + 1 : jc - 1;
+    for (int k = 2; k < 4; ++k) {
+        if (!(parts & (1 << k))) continue;
+        const double y = bf.B.t[k == 2 ? S_P : S_SC][q];
+        if (y == 0.0) continue;
+        const int c = k == 2 ? S_CP : S_C;
+        bk.add(c, jc * nxc + ic, y * g1);
+        bk.add(c, jc * nxc + in, y * g2);
+        bk.add(c, jn * nxc + ic, y * g3);
+        bk.add(c, jn * nxc + in, y * g4);
+    }
+}
+
+// The closed-form transpose of one cell of phase P, for the kinds that have one;
+// false: transpose it by probes.
+__device__ __forceinline__ bool adj_closed(const CaseDev &C, const CaseTan &B, const Phase &P, int i, int j,
+                                           ParAcc &pa)
+{
+    const LevelDev &F = C.lv[P.ig];
+    const Bars bf{B.lv[P.ig]};
+    switch (P.kind) {
+    case P_ASM_U: asm_u_adj(C, F, bf, i, j, pa); return true;
+    case P_ASM_V: asm_v_adj(C, F, bf, i, j, pa); return true;
+    case P_ASM_SC: asm_sc_adj(F, bf, i, j, pa); return true;
+    case P_FINE_RES: fine_res_adj(F, bf, i, j, P.a, pa); return true;
+    case P_RESTRICT: restrict_adj(F, C.lv[P.ig + 1], bf, Bars{B.lv[P.ig + 1]}, i, j, P.a, pa); return true;
+    case P_MASS_COEFP: mass_coefp_adj(C, F, bf, i, j, P.a); return true;
+    case P_RESTV: restv_adj(F, C.lv[P.ig + 1], bf, Bars{B.lv[P.ig + 1]}, i, j, P.a); return true;
+    case P_PROL_CORR: prol_corr_adj(F, C.lv[P.ig + 1], bf, Bars{B.lv[P.ig + 1]}, i, j, P.a); return true;
+    case P_PROL_APPLY: prol_apply_adj(F, C.lv[P.ig + 1], bf, Bars{B.lv[P.ig + 1]}, i, j, P.a); return true;
+    case P_UPDATE: update_adj(C, F, bf, j * F.npx + i, P.a); return true;
+    default: return false;
+    }
 }
 
 // ----------------------------------------------------------------- kernel
@@ -437,9 +952,15 @@ __global__ void __launch_bounds__(ADJ_BLOCK, 1) k_adj_cycle(const CaseDev *__res
     if (threadIdx.x == 0) bad_s = 0;
     __syncthreads();
     int bad = 0;
-    // forward, taped
+    // forward, taped (a half-sweep tapes and updates each cell in one pass)
     for (int p = 0; p < A.nphase; ++p) {
         const Phase P = A.prog[p];
+        if (P.kind == P_GS && !A.generic) {
+            double *tape = A.tape + P.off;
+            gs_cells(C.lv[P.ig], P, [&](int i, int j, int t) { fwd_gs_cell(C.lv[P.ig], P.a, i, j, tape, t); });
+            case_barrier();
+            continue;
+        }
         tape_copy(C, A, P, true);
         case_barrier();
         const RecCase X{C, write_level(P), write_mask(P), &bad};
@@ -450,12 +971,24 @@ __global__ void __launch_bounds__(ADJ_BLOCK, 1) k_adj_cycle(const CaseDev *__res
     ParAcc pa{0.0, 0.0, 0.0, 0.0};
     for (int p = A.nphase - 1; p >= 0; --p) {
         const Phase P = A.prog[p];
+        if (P.kind == P_GS && !A.generic) {
+            const double *tape = A.tape + P.off;
+            gs_cells(C.lv[P.ig], P,
+                     [&](int i, int j, int t) { adj_gs_cell(C.lv[P.ig], B.lv[P.ig], P.a, i, j, tape, t); });
+            case_barrier();
+            continue;
+        }
         tape_copy(C, A, P, false);
         case_barrier();
-        if (P.kind == P_GS && !A.generic) {
-            phase_cells(C, P, [&](int i, int j) { adj_gs_cell(C.lv[P.ig], B.lv[P.ig], P.a, i, j); });
-        } else {
-            phase_cells(C, P, [&](int i, int j) { adj_cell(C, B, P, i, j, pa, &bad); });
+        {
+            const bool closed = !A.generic && (P.kind == P_ASM_U || P.kind == P_ASM_V || P.kind == P_ASM_SC ||
+                                               P.kind == P_FINE_RES || P.kind == P_RESTRICT ||
+                                               P.kind == P_MASS_COEFP || P.kind == P_UPDATE || P.kind == P_RESTV ||
+                                               P.kind == P_PROL_CORR || P.kind == P_PROL_APPLY);
+            if (closed)
+                phase_cells(C, P, [&](int i, int j) { adj_closed(C, B, P, i, j, pa); });
+            else
+                phase_cells(C, P, [&](int i, int j) { adj_cell(C, B, P, i, j, pa, &bad); });
             flush_par(pa, P, A.pacc);
         }
         case_barrier();

@@ -92,6 +92,6 @@ int adj_cluster_size(int ncases, int sms);
 cudaError_t launch_live_copy(const CaseDev *dc, const long long *off, double *buf, int ncases, int maxcells,
                              int maxng, int dir, cudaStream_t st);
 
-constexpr int ADJ_BLOCK = 512;
+constexpr int ADJ_BLOCK = 1024;
 
 }  // namespace mg

@@ -164,10 +164,12 @@ def test_adjoint_with_a_diverging_case_in_the_batch(oracle_built):
     _close(good, _forward_mode(cases[0], profs[0], cycles), "the finite case beside a diverging one")
 
 
-def test_closed_form_transposes_equal_the_probed_ones(monkeypatch, oracle_built):
-    """The phases transposed in closed form (the red-black half-sweep) give what
+@pytest.mark.parametrize("name", ["obs_gs_touch", "obs_below_coarsest", "ports", "odd_sweeps", "rect_grid"])
+def test_closed_form_transposes_equal_the_probed_ones(name, monkeypatch, oracle_built):
+    """The phases transposed in closed form (the red-black half-sweep; the assemblies,
+    fine residuals and FAS defects with their hybrid-scheme coefficients) give what
     transposing them by dual-number probes gives, to rounding."""
-    cfg = small_cases()["obs_gs_touch"]
+    cfg = small_cases()[name]
     prof = 1.0 + 0.05 * np.cos(np.arange(cfg.nfy))
     closed = _adjoint([cfg], [prof], 3)[0]
     monkeypatch.setenv("MGFVM_ADJOINT_GENERIC", "1")
