@@ -183,6 +183,12 @@ typedef struct mgfvm_tuning {
                                               scheduled while its predecessor finishes
                                               and wait for it on the device): 0 or 2
                                               yes, 1 no                                 */
+    int band_visit[MGFVM_MAX_LEVELS];      /* on a level too large for one CTA per case but
+                                              held by a cluster of at most 8 (bands of
+                                              rows, halo rows exchanged in distributed
+                                              shared memory; FP64 in either precision):
+                                              the whole visit in one launch: 2 yes, 1 no,
+                                              0 yes in batches of at least 32 cases     */
 } mgfvm_tuning;
 
 typedef struct mgfvm_ctx mgfvm_ctx;

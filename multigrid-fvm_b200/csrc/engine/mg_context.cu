@@ -217,6 +217,28 @@ struct Builder {
             }
         return mx > 0 && mx * ((my + 1) / 2) <= SMOOTH_BLOCK;
     }
+    // Whether a cluster of G <= BAND_MAX_CTAS CTAs per case holds the level in bands of
+    // rows (k_band_visit): one thread per interior column and vertical cell pair of a
+    // band, the band and its halo rows in shared memory, for the largest case.
+    bool band_level(int ig, int &G, int &block, int &smem) const
+    {
+        int mx = 0, my = 0;
+        for (const mgfvm_config &c : x->cfg)
+            if (ig < c.ngrid) {
+                mx = std::max(mx, npx_of(c, ig));
+                my = std::max(my, npy_of(c, ig));
+            }
+        if (mx < 3 || my < 3) return false;
+        const int wc = mx - 2, rows = my - 2;
+        const int b0 = (2 * SMOOTH_BLOCK / wc) & ~1;   // rows of a band that SMOOTH_BLOCK threads cover
+        if (b0 < 2) return false;
+        G = (rows + b0 - 1) / b0;
+        if (G > BAND_MAX_CTAS) return false;
+        const int b = band_rows(my, G);
+        block = round32(wc * (b / 2));
+        smem = (x->sched.isolve == MGFVM_JACOBI ? 2 : 1) * (b + 2) * mx * (int)sizeof(double);
+        return block <= SMOOTH_BLOCK && smem <= BAND_SMEM_MAX;
+    }
     static int round32(int n) { return std::max(32, (n + 31) / 32 * 32); }
     int min_ngrid() const
     {
@@ -231,13 +253,25 @@ struct Builder {
     // `tmp_ok`: the next kernel can take the result from the ping-pong buffers, so an
     // odd number of tile launches needs no copy back.  Returns whether it is left there.
     // Mixed precision runs on the V-cycle's levels smoothed in tiles, every level but
-    // the coarsest (a whole level one CTA holds stays FP64: its visits are latency-bound
-    // single launches): FP32 operands and corrections (k_smooth_f32).
+    // the coarsest (a whole level one CTA holds, and a level of band visits, stays FP64:
+    // its visits are latency-bound single launches): FP32 operands and corrections
+    // (k_smooth_f32).
     bool f32_level(int ig, int mode) const
     {
-        int mx, my;
+        int mx, my, G, blk, smem;
         return x->opt.precision == MGFVM_PREC_MIXED && mode != M_OP && ig < min_ngrid() - 1 &&
-               !whole_level(ig, mx, my);
+               !whole_level(ig, mx, my) && !band_visits(ig, mode, G, blk, smem);
+    }
+    // Whether the visits to level ig run as band visits (k_band_visit, FP64 in either
+    // precision): the level fits a cluster and the tuning asks for them, or leaves it
+    // to the default, which takes them for batches of at least BAND_MIN_CASES cases.
+    bool band_visits(int ig, int mode, int &G, int &blk, int &smem) const
+    {
+        const int isolve = x->sched.isolve, t = x->tune.band_visit[ig];
+        int mx, my;
+        return mode != M_OP && x->sched.nswpp > 0 && t != 1 &&
+               (isolve == MGFVM_JACOBI || isolve == MGFVM_GAUSS_SEIDEL) && !whole_level(ig, mx, my) &&
+               band_level(ig, G, blk, smem) && (t == 2 || x->ncases >= BAND_MIN_CASES);
     }
     int f32_buf = 0;   // the FP32 correction buffer the last F32 smoothing call ended in
     bool smooth(int ig, int mode, int mask, int nsw, bool tmp_ok = false)
@@ -302,7 +336,9 @@ struct Builder {
         int u0 = 0;
         for (int c = 0; c < chunks; ++c) {
             const int nu = units / chunks + (c < units % chunks ? 1 : 0);
-            Launch &L = add(mi >= 0 ? K_SMOOTH_TMA : kern, ig, mode, 0, mask, u0, nu, c & 1);
+            // a later launch reads its coefficients before waiting for the one before it
+            const int early = mi < 0 && c > 0 && x->sched.pdl ? 4 : 0;
+            Launch &L = add(mi >= 0 ? K_SMOOTH_TMA : kern, ig, mode, 0, mask, u0, nu, (c & 1) | early);
             L.a4 = tile;
             L.grid = dim3((unsigned)tiles(ig, tile), x->ncases, neq);
             L.block = std::min(nt, round32(side * ((side + 1) / 2)));
@@ -440,6 +476,20 @@ struct Builder {
             L.grid = dim3(visit ? 3 : 1, x->ncases);
             L.block = round32(mx * ((my + 1) / 2));
             L.smem = (isolve == MGFVM_JACOBI ? 2 : 1) * mx * my * (int)sizeof(double);
+            after_update(ig, mode, fuse | (pfx ? 4 : 0), fuse ? 0 : (down ? 3 : 7));
+            return;
+        }
+        int G, blk, smem;
+        if (band_visits(ig, mode, G, blk, smem)) {
+            // the whole visit in one launch of a cluster of G CTAs per case
+            const bool pfx = pfix_fusable(ig, mode);
+            const int fuse = outflow_fusable(ig, mode, pfx) ? (down ? 1 : 3) : 0;
+            Launch &L = add(K_BAND_VISIT, ig, mode, 0, ppu, reduce ? 1 : 0, fuse | (pfx ? 4 : 0),
+                            asm_done ? 0 : (int)asm_bits(down));
+            L.a4 = std::max(mu, 0);
+            L.grid = dim3(G, x->ncases);
+            L.block = blk;
+            L.smem = smem;
             after_update(ig, mode, fuse | (pfx ? 4 : 0), fuse ? 0 : (down ? 3 : 7));
             return;
         }
@@ -1523,6 +1573,7 @@ static bool tuning_valid(const mgfvm_tuning &t)
         if (t.smooth_tma[ig] < 0 || t.smooth_tma[ig] > 2) return false;
         if (t.coarse_kernel[ig] < 0 || t.coarse_kernel[ig] > 2) return false;
         if (t.prol_fused[ig] < 0 || t.prol_fused[ig] > 2) return false;
+        if (t.band_visit[ig] < 0 || t.band_visit[ig] > 2) return false;
     }
     return t.tma_first_wait >= -1 && t.pdl >= 0 && t.pdl <= 2;
 }
@@ -1634,6 +1685,11 @@ int mgfvm_autotune(mgfvm_ctx *x, int cycles, mgfvm_tuning *chosen, double *ms_be
                 for (auto &o : opts) knobs.push_back({0, o[0], o[1]});
             }
             if (!probe.whole_level(ig, mx, my)) knobs.push_back({3, 2, 0});
+            int bg, bb, bs;
+            if (!probe.whole_level(ig, mx, my) && probe.band_level(ig, bg, bb, bs)) {
+                knobs.push_back({6, 1, 0});
+                knobs.push_back({6, 2, 0});
+            }
             if (ig >= 1 && ig >= x->maxng - 3) knobs.push_back({4, 2, 0});   // one-CTA kernel from here down
             if (ig + 1 < x->maxng) knobs.push_back({5, 1, 0});                 // separate correction kernel
             knobs.push_back({1, 1, 0});
@@ -1650,6 +1706,7 @@ int mgfvm_autotune(mgfvm_ctx *x, int cycles, mgfvm_tuning *chosen, double *ms_be
                 if (k[0] == 3) cand.smooth_tma[ig] = k[1];
                 if (k[0] == 4) cand.coarse_kernel[ig] = k[1];
                 if (k[0] == 5) cand.prol_fused[ig] = k[1];
+                if (k[0] == 6) cand.band_visit[ig] = k[1];
                 if (memcmp(&cand, &keep, sizeof cand) == 0) continue;
                 x->tune = cand;
                 rebuild_schedule(x);

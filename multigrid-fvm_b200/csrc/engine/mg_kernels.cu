@@ -501,14 +501,39 @@ template <int ISOLVE, int NT>
 __global__ void __launch_bounds__(NT, SMOOTH_BLOCK / NT) k_smooth(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode, int mask, int u0, int nu,
                                                          int dir, int tile)
 {
-    pdl_enter();
+    // dir bit 4: the coefficients were written before the previous launch (a later
+    // launch of a smoothing split in several), so they are read before waiting for it
+    const bool early = (dir & 4) != 0;
+    dir &= 3;
+    if (!early) pdl_enter();
     extern __shared__ double sm[];
     const CaseDev &C = cs[blockIdx.y];
-    if (!case_active(C, st[blockIdx.y], ig, mode)) return;
     const int e = nth_eq(mask, blockIdx.z);
     const LevelDev &L = C.lv[ig];
     PairTile P;
     const int g = pair_tile(L, e, nu, tile, P, blockIdx.x);
+    const double *__restrict__ gaw = L.f[co_slot(e, CK_AW)];
+    const double *__restrict__ gae = L.f[co_slot(e, CK_AE)];
+    const double *__restrict__ gas = L.f[co_slot(e, CK_AS)];
+    const double *__restrict__ gan = L.f[co_slot(e, CK_AN)];
+    const double *__restrict__ gap = L.f[co_slot(e, CK_AP)];
+    const double *__restrict__ gsu = L.f[co_slot(e, CK_SU)];
+    double A[6] = {0, 0, 0, 0, 0, 0}, B[6] = {0, 0, 0, 0, 0, 0}, pA = 0.0, pB = 0.0;
+    auto load_coef = [&]() {
+        if (P.okA) {
+            const int g0 = P.gA;
+            A[0] = gaw[g0]; A[1] = gae[g0]; A[2] = gas[g0]; A[3] = gan[g0]; A[4] = gap[g0]; A[5] = gsu[g0];
+        }
+        if (P.okB) {
+            const int g0 = P.gB;
+            B[0] = gaw[g0]; B[1] = gae[g0]; B[2] = gas[g0]; B[3] = gan[g0]; B[4] = gap[g0]; B[5] = gsu[g0];
+        }
+    };
+    if (early) {
+        if (g == 0) load_coef();
+        pdl_enter();
+    }
+    if (!case_active(C, st[blockIdx.y], ig, mode)) return;
     if (g == 1) return;
     if (g == 2) {     // the schedule sizes blocks to fit; never taken
         if (threadIdx.x == 0) atomicOr(&st[blockIdx.y].status, (int)CASE_BAD_LAUNCH);
@@ -519,23 +544,9 @@ __global__ void __launch_bounds__(NT, SMOOTH_BLOCK / NT) k_smooth(const CaseDev 
     const double *src = L.f[dir == 1 ? ts : fs];
     double *dst = L.f[dir == 0 ? ts : fs];
     double *phi = sm, *phi2 = sm + W * P.Hh;
-    const double *__restrict__ gaw = L.f[co_slot(e, CK_AW)];
-    const double *__restrict__ gae = L.f[co_slot(e, CK_AE)];
-    const double *__restrict__ gas = L.f[co_slot(e, CK_AS)];
-    const double *__restrict__ gan = L.f[co_slot(e, CK_AN)];
-    const double *__restrict__ gap = L.f[co_slot(e, CK_AP)];
-    const double *__restrict__ gsu = L.f[co_slot(e, CK_SU)];
-    double A[6] = {0, 0, 0, 0, 0, 0}, B[6] = {0, 0, 0, 0, 0, 0}, pA = 0.0, pB = 0.0;
-    if (P.okA) {
-        const int g0 = P.gA;
-        pA = src[g0];
-        A[0] = gaw[g0]; A[1] = gae[g0]; A[2] = gas[g0]; A[3] = gan[g0]; A[4] = gap[g0]; A[5] = gsu[g0];
-    }
-    if (P.okB) {
-        const int g0 = P.gB;
-        pB = src[g0];
-        B[0] = gaw[g0]; B[1] = gae[g0]; B[2] = gas[g0]; B[3] = gan[g0]; B[4] = gap[g0]; B[5] = gsu[g0];
-    }
+    if (!early) load_coef();
+    if (P.okA) pA = src[P.gA];
+    if (P.okB) pB = src[P.gB];
     const double eps = ISOLVE == MGFVM_JACOBI ? 1.0e-30 : 0.0;   // solver's (ap + 1e-30), solvergs' ap
     const Recip RA = make_recip(ISOLVE == MGFVM_JACOBI ? A[4] + eps : A[4]);
     const Recip RB = make_recip(ISOLVE == MGFVM_JACOBI ? B[4] + eps : B[4]);
@@ -903,6 +914,289 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(SMOOTH_BLOCK, 1)
         atomicOr(&ST.status, (int)CASE_BAD_LAUNCH);   // the schedule sizes blocks to fit; never taken
     cluster_barrier();
     if (active && r == 0) pp_level_body<ISOLVE>(C, ST, L, nu, reduce, fuse, sm);
+}
+
+// ------------------------------------------------ band visits (a cluster per case)
+// A whole visit to a level too large for one CTA but small enough for a cluster of G
+// (at most 8) CTAs, in one launch.  CTA r of the cluster owns a band of interior rows
+// [j0, j1) (band_rows(npy, G) rows each, an even number; the last band may be shorter),
+// one thread per interior column and vertical cell pair of its band.  A smoothing
+// stages the band and one row on either side (the neighbouring bands' edge rows, or the
+// boundary ring) in shared memory.  In every unit each thread updates its cell of the
+// unit's colour (both cells, for Jacobi) and, where that cell is on an edge row of the
+// band, stores the new value into the neighbouring band's copy of the row
+// (distributed shared memory); a cluster barrier ends the unit, so every cell update
+// reads the values a whole-level sweep reads: the same bits as the grid kernels.
+// Order: the assembly `what` over the cells of the whole level | cluster barrier |
+// u, v, sc smoothing (mu units each, one after the other) | cluster barrier |
+// masserror + coefp, the p' units, update with k_update's fusions (`fuse`), the level's
+// sum |div| with `reduce`.  Every CTA of a cluster takes the same cluster barriers (the
+// case's activity is the same for all of them; a CTA without rows only joins them).
+__device__ __forceinline__ unsigned cl_rank_k()
+{
+    unsigned v;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(v));
+    return v;
+}
+__device__ __forceinline__ unsigned cl_size_k()
+{
+    unsigned v;
+    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(v));
+    return v;
+}
+// the shared::cluster address `p` (a shared-memory location of this CTA) has in CTA `rank`
+__device__ __forceinline__ unsigned cl_map(const void *p, unsigned rank)
+{
+    unsigned a;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(a) : "r"(smem_u32(p)), "r"(rank));
+    return a;
+}
+// store v at the shared-memory location `p` has in CTA `rank` of the cluster
+__device__ __forceinline__ void st_cluster(double *p, unsigned rank, double v)
+{
+    asm volatile("st.shared::cluster.f64 [%0], %1;" ::"r"(cl_map(p, rank)), "d"(v) : "memory");
+}
+
+// One CTA's band and this thread's pair: cells (i, ja) and (i, ja + 1).
+struct Band {
+    int r, G;
+    int j0, j1, b, nx, base;   // rows [j0, j1), full band height b, shared index = q - base
+    int i, ja, jb;
+    bool ownA, ownB;           // the cell is in the band
+    bool below, above;         // a neighbouring band exists below (r - 1) / above (r + 1)
+};
+__device__ __forceinline__ Band band_of(const LevelDev &L, int r, int G)
+{
+    Band B;
+    B.r = r;
+    B.G = G;
+    B.nx = L.npx;
+    B.b = band_rows(L.npy, G);
+    B.j0 = 1 + r * B.b;
+    B.j1 = min(B.j0 + B.b, L.npy - 1);
+    B.base = (B.j0 - 1) * L.npx;
+    const int wc = L.npx - 2, t = threadIdx.x;
+    B.i = 1 + t % wc;
+    B.ja = B.j0 + 2 * (t / wc);
+    B.jb = B.ja + 1;
+    const bool some = B.j1 > B.j0;
+    const bool own = some && t < wc * (B.b / 2);
+    B.ownA = own && B.ja < B.j1;
+    B.ownB = own && B.jb < B.j1;
+    B.below = some && r > 0;
+    B.above = some && B.j1 < L.npy - 1;   // then the band is full height and r + 1 < G
+    return B;
+}
+
+__device__ __forceinline__ bool in_dom(const Dom &d, int i, int j)
+{
+    return i >= d.i0 && i < d.i0 + d.wi && j >= d.j0 && j < d.j0 + d.wj;
+}
+
+// The two cells of this thread in one equation's smoothing: coefficients, reciprocals,
+// shared indices and whether each is in the equation's domain.
+struct BandCells {
+    double A[6], Bc[6];
+    Recip RA, RB;
+    int sA, sB;
+    bool inA, inB;
+};
+
+// `units` units of a smoothing on the staged band (phi; phi2 = phi + stride for
+// Jacobi), the neighbours' edge rows exchanged after every unit, a cluster barrier
+// after each (a CTA without rows takes them too).  Returns the buffer holding the result.
+template <int ISOLVE>
+__device__ __forceinline__ const double *band_units(const Band &B, const Dom &d, int units, double *sm, size_t stride,
+                                                    const BandCells &K)
+{
+    constexpr bool JAC = ISOLVE == MGFVM_JACOBI;
+    double *phi = sm, *phi2 = sm + stride;
+    const int nx = B.nx;
+    const bool redA = ((B.i + B.ja) & 1) == 0;
+    // after a unit: the cell (i, j) value v just written goes to the neighbouring bands'
+    // copies of the row (`buf`: the buffer's offset; every CTA has the same layout)
+    auto send = [&](int j, size_t buf, double v) {
+        if (j == B.j0 && B.below) st_cluster(sm + buf + (size_t)(B.b + 1) * nx + B.i, B.r - 1, v);
+        if (j == B.j1 - 1 && B.above) st_cluster(sm + buf + B.i, B.r + 1, v);
+    };
+    for (int h = 1; h <= units; ++h) {
+        if (!JAC) {
+            const bool useA = (((h - 1) & 1) == 0) == redA;
+            if (useA ? K.inA : K.inB) {
+                const int s = useA ? K.sA : K.sB;
+                const double *c = useA ? K.A : K.Bc;
+                const double v = gs_value_r(c[0], c[1], c[2], c[3], useA ? K.RA : K.RB, c[5], phi[s - 1], phi[s + 1],
+                                            phi[s - nx], phi[s + nx]);
+                phi[s] = v;
+                send(useA ? B.ja : B.jb, 0, v);
+            }
+        } else {
+            const double *cur = ((h - 1) & 1) ? phi2 : phi;
+            double *nxt = ((h - 1) & 1) ? phi : phi2;
+            const size_t nb = ((h - 1) & 1) ? 0 : stride;
+            if (K.inA) {
+                const double v = jacobi_value_r(K.A[0], K.A[1], K.A[2], K.A[3], K.RA, K.A[5], cur[K.sA - 1],
+                                                cur[K.sA + 1], cur[K.sA - nx], cur[K.sA + nx], cur[K.sA]);
+                nxt[K.sA] = v;
+                send(B.ja, nb, v);
+            }
+            if (K.inB) {
+                const double v = jacobi_value_r(K.Bc[0], K.Bc[1], K.Bc[2], K.Bc[3], K.RB, K.Bc[5], cur[K.sB - 1],
+                                                cur[K.sB + 1], cur[K.sB - nx], cur[K.sB + nx], cur[K.sB]);
+                nxt[K.sB] = v;
+                send(B.jb, nb, v);
+            }
+        }
+        cluster_barrier();
+    }
+    return (JAC && (units & 1)) ? phi2 : phi;
+}
+
+// `units` units of equation e's smoother on the banded level, from and back to its field.
+template <int ISOLVE>
+__device__ void band_smooth_eq(const LevelDev &L, const Band &B, int e, int units, double *sm)
+{
+    constexpr bool JAC = ISOLVE == MGFVM_JACOBI;
+    const Dom d = dom_eq(L, e);
+    const int nx = B.nx;
+    const size_t stride = (size_t)(B.b + 2) * nx;
+    double *fld = L.f[eq_field(e)];
+    __syncthreads();   // the previous smoothing's write-back has read the buffers
+    if (B.j1 > B.j0) {
+        const int n = (B.j1 - B.j0 + 2) * nx;
+        for (int k = threadIdx.x; k < n; k += blockDim.x) {
+            const double v = fld[B.base + k];
+            sm[k] = v;
+            if (JAC) sm[stride + k] = v;
+        }
+    }
+    BandCells K;
+    K.inA = B.ownA && in_dom(d, B.i, B.ja);
+    K.inB = B.ownB && in_dom(d, B.i, B.jb);
+    const int qA = B.ja * nx + B.i, qB = B.jb * nx + B.i;
+    K.sA = qA - B.base;
+    K.sB = qB - B.base;
+    for (int a = 0; a < 6; ++a) {
+        K.A[a] = K.inA ? L.f[co_slot(e, a)][qA] : 0.0;
+        K.Bc[a] = K.inB ? L.f[co_slot(e, a)][qB] : 0.0;
+    }
+    K.RA = make_recip(JAC ? K.A[4] + 1.0e-30 : K.A[4]);
+    K.RB = make_recip(JAC ? K.Bc[4] + 1.0e-30 : K.Bc[4]);
+    cluster_barrier();   // every band staged before any neighbour writes into it
+    const double *res = band_units<ISOLVE>(B, d, units, sm, stride, K);
+    if (K.inA) fld[qA] = res[K.sA];
+    if (K.inB) fld[qB] = res[K.sB];
+}
+
+// masserror + coefp, the p' units and update (+ fusions) on the banded level.
+template <int ISOLVE>
+__device__ void band_pp(const CaseDev &C, CaseState &ST, const LevelDev &L, const Band &B, int nu, int reduce,
+                        int fuse, double *sm, double *red)
+{
+    constexpr bool JAC = ISOLVE == MGFVM_JACOBI;
+    const Dom d = dom_interior(L);
+    const int nx = B.nx;
+    const size_t stride = (size_t)(B.b + 2) * nx;
+    double *pp = MGF(L, S_PP);
+    BandCells K;
+    double divs = 0.0;
+    K.inA = B.ownA;
+    K.inB = B.ownB;
+    {
+        Coef k;
+        double su = 0.0;
+        for (int a = 0; a < 6; ++a) K.A[a] = K.Bc[a] = 0.0;
+        if (B.ownA) {
+            divs += mass_coefp_values(L, C, B.i, B.ja, k, su, S_U, S_V);
+            K.A[0] = k.aw; K.A[1] = k.ae; K.A[2] = k.as; K.A[3] = k.an; K.A[4] = k.ap; K.A[5] = su;
+        }
+        if (B.ownB) {
+            divs += mass_coefp_values(L, C, B.i, B.jb, k, su, S_U, S_V);
+            K.Bc[0] = k.aw; K.Bc[1] = k.ae; K.Bc[2] = k.as; K.Bc[3] = k.an; K.Bc[4] = k.ap; K.Bc[5] = su;
+        }
+    }
+    // p' starts at zero in the interior (masserror), the ring keeps its values
+    __syncthreads();
+    if (B.j1 > B.j0) {
+        const int n = (B.j1 - B.j0 + 2) * nx;
+        for (int k = threadIdx.x; k < n; k += blockDim.x) {
+            const int q = B.base + k, i = q % nx, j = q / nx;
+            const double v = (i >= 1 && i <= nx - 2 && j >= 1 && j <= L.npy - 2) ? 0.0 : pp[q];
+            sm[k] = v;
+            if (JAC) sm[stride + k] = v;
+        }
+    }
+    K.RA = make_recip(JAC ? K.A[4] + 1.0e-30 : K.A[4]);
+    K.RB = make_recip(JAC ? K.Bc[4] + 1.0e-30 : K.Bc[4]);
+    const int qA = B.ja * nx + B.i, qB = B.jb * nx + B.i;
+    K.sA = qA - B.base;
+    K.sB = qB - B.base;
+    cluster_barrier();   // every CTA has read u, v and staged its band
+    const double *res = band_units<ISOLVE>(B, d, nu, sm, stride, K);
+    const bool out = (fuse & 1) && C.ibc_xp == 4;
+    if (B.ownA) {
+        pp[qA] = res[K.sA];
+        update_cell(L, C, B.i, B.ja, res[K.sA], res[K.sA + 1], res[K.sA + nx], out, fuse);
+    }
+    if (B.ownB) {
+        pp[qB] = res[K.sB];
+        update_cell(L, C, B.i, B.jb, res[K.sB], res[K.sB + 1], res[K.sB + nx], out, fuse);
+    }
+    if (out && B.r == 0 && threadIdx.x < 2) row_outflow(L, threadIdx.x == 0 ? 0 : L.npy - 1, (fuse & 2) != 0);
+    if (reduce) {
+        // the level's sum |div| in a fixed order: a block sum per CTA, the CTAs' sums
+        // added in rank order by CTA 0
+        double a[1] = {divs};
+        block_sum<1>(a);
+        if (threadIdx.x == 0) st_cluster(red + B.r, 0, a[0]);
+        cluster_barrier();
+        if (B.r == 0 && threadIdx.x == 0) {
+            double sum = 0.0;
+            for (int k = 0; k < B.G; ++k) sum += red[k];
+            ST.last_err = sum;
+        }
+    }
+}
+
+template <int ISOLVE>
+__global__ void __launch_bounds__(SMOOTH_BLOCK, 1)
+    k_band_visit(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode, int nu, int reduce, int fuse,
+                 int what, int mu)
+{
+    pdl_enter();
+    extern __shared__ double sm[];
+    __shared__ double red[BAND_MAX_CTAS];
+    const CaseDev &C = cs[blockIdx.y];
+    CaseState &ST = st[blockIdx.y];
+    if (!case_active(C, ST, ig, mode)) return;   // the same for every CTA of the cluster
+    const LevelDev &L = C.lv[ig];
+    const int r = (int)cl_rank_k(), G = (int)cl_size_k();
+    {
+        // the schedule sizes the launch for the largest case; never taken (the check
+        // depends on the case and the launch only, so the whole cluster leaves together)
+        unsigned dyn;
+        asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+        const int b = band_rows(L.npy, G);
+        const size_t need = (size_t)(ISOLVE == MGFVM_JACOBI ? 2 : 1) * (b + 2) * L.npx * sizeof(double);
+        if ((L.npx - 2) * (b / 2) > (int)blockDim.x || need > dyn || G > BAND_MAX_CTAS) {
+            if (r == 0 && threadIdx.x == 0) atomicOr(&ST.status, (int)CASE_BAD_LAUNCH);
+            return;
+        }
+    }
+    if (what) {
+        const int n = L.npx * L.npy;
+        for (int q = r * blockDim.x + threadIdx.x; q < n; q += G * blockDim.x)
+            cell_asm(L, C, FluxLive(L), q % L.npx, q / L.npx, (unsigned)what);
+        cluster_barrier();
+    }
+    const Band B = band_of(L, r, G);
+    if (mu > 0) {
+        band_smooth_eq<ISOLVE>(L, B, EQ_U, mu, sm);
+        band_smooth_eq<ISOLVE>(L, B, EQ_V, mu, sm);
+        band_smooth_eq<ISOLVE>(L, B, EQ_SC, mu, sm);
+        cluster_barrier();   // u, v written before masserror reads them across bands
+    }
+    band_pp<ISOLVE>(C, ST, L, B, nu, reduce, fuse, sm, red);
 }
 
 // Mixed precision (MGFVM_PREC_MIXED): the tiles, units and windows of k_smooth on
@@ -1492,6 +1786,9 @@ cudaError_t configure_kernels()
                          (const void *)k_smooth_tma<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK / 4>};
     for (const void *f : tma)
         if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, SMOOTH_TMA_SMEM_MAX);
+    const void *band[] = {(const void *)k_band_visit<MGFVM_JACOBI>, (const void *)k_band_visit<MGFVM_GAUSS_SEIDEL>};
+    for (const void *f : band)
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, BAND_SMEM_MAX);
     return e;
 }
 
@@ -1510,6 +1807,28 @@ static cudaError_t launch_k(bool pdl, void (*k)(KP...), dim3 g, int b, int smem,
     c.stream = st;
     c.attrs = at;
     c.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&c, k, static_cast<KP>(args)...);
+}
+
+// launch_k for a kernel whose CTAs form clusters of `cx` along x
+template <typename... KP, typename... A>
+static cudaError_t launch_cluster(bool pdl, void (*k)(KP...), dim3 g, int b, int smem, cudaStream_t st, int cx,
+                                  A... args)
+{
+    cudaLaunchAttribute at[2];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)cx;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[1].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t c = {};
+    c.gridDim = g;
+    c.blockDim = dim3((unsigned)b, 1, 1);
+    c.dynamicSmemBytes = (size_t)smem;
+    c.stream = st;
+    c.attrs = at;
+    c.numAttrs = pdl ? 2 : 1;
     return cudaLaunchKernelEx(&c, k, static_cast<KP>(args)...);
 }
 
@@ -1603,6 +1922,13 @@ cudaError_t launch_one(const Launch &X, const CaseDev *dc, CaseState *ds, const 
             le = launch_k(pdl, k_level_visit<MGFVM_JACOBI>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
         else
             le = launch_k(pdl, k_level_visit<MGFVM_GAUSS_SEIDEL>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+        break;
+    case K_BAND_VISIT:
+        if (b > SMOOTH_BLOCK || g.x < 1 || g.x > BAND_MAX_CTAS || X.smem > BAND_SMEM_MAX) return cudaErrorInvalidValue;
+        if (S.isolve == MGFVM_JACOBI)
+            le = launch_cluster(pdl, k_band_visit<MGFVM_JACOBI>, g, b, X.smem, st, (int)g.x, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+        else
+            le = launch_cluster(pdl, k_band_visit<MGFVM_GAUSS_SEIDEL>, g, b, X.smem, st, (int)g.x, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
         break;
     case K_PFIX_BOUND: le = launch_k(pdl, k_pfix_bound, g, b, 0, st, dc, ds, X.ig, X.mode, X.a0); break;
     case K_RESTV_FLUXES: le = launch_k(pdl, k_restv_fluxes, g, b, 0, st, dc, ds, X.ig, X.mode); break;

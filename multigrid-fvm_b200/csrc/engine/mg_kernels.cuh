@@ -30,6 +30,8 @@ enum KernelId {
     K_LEVEL_VISIT,   // a whole one-CTA level visit, a cluster of 3 CTAs per case: K_PP_LEVEL's
                      // a0-a2, a3 = assembly bits (0: done), a4 = u/v/sc units
     K_SMOOTH_TMA,    // as K_SMOOTH, the region staged by TMA box loads (bw, bh, ptr)
+    K_BAND_VISIT,    // a whole level visit, a cluster of grid.x CTAs per case (bands of rows):
+                     // K_LEVEL_VISIT's arguments
     K_NKERNELS
 };
 
@@ -66,6 +68,22 @@ struct Sched {
 // SM) threads, one vertical cell pair per thread, covers a tile plus a halo of one cell
 // per unit on every side.
 constexpr int SMOOTH_BLOCK = 1024;
+// band visits: at most 8 CTAs per case (the portable cluster size) and this much
+// dynamic shared memory per CTA (the band and its two halo rows, two buffers for Jacobi)
+constexpr int BAND_MAX_CTAS = 8;
+constexpr int BAND_SMEM_MAX = 80 * 1024;
+// By default a level runs band visits in batches of at least this many cases: a unit
+// costs about a microsecond there (its cluster barrier), which only pays when the tile
+// launches it replaces have enough work to be slow too (256^2 cases, levels 1-2:
+// slower up to 16 cases, faster from 32)
+constexpr int BAND_MIN_CASES = 32;
+// interior rows of each band when G CTAs share a level of npy padded rows (even; the
+// last band may be shorter)
+__host__ __device__ __forceinline__ int band_rows(int npy, int G)
+{
+    const int b = (npy - 2 + G - 1) / G;
+    return (b + 1) & ~1;
+}
 constexpr int MAX_UNITS = 10;   // default cap of half-sweeps (GS) or sweeps (Jacobi) per launch
 constexpr int MIN_TILE = 8;     // smallest tile side a units cap may leave
 int smooth_pairs_side(int units, int threads);   // tile side whose region fits `threads` pairs

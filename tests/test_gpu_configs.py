@@ -24,12 +24,18 @@ def _check(s, k, o, cycles, what, levels=(0, 1)):
     np.testing.assert_allclose(s.history(k)[0], o.history()[0], rtol=1e-12, atol=0)
 
 
-def test_obstacle_flow_pair(oracle_built):
+@pytest.mark.parametrize("band", [2, 1])
+def test_obstacle_flow_pair(band, oracle_built):
+    """Levels 1 and 2 (130^2 and 66^2 padded) by band visits (a cluster of 8 and of 2
+    CTAs per case; band 2) and by the tile smoothers (band 1, the default for two cases)."""
     from mgfvm import Solver, configs
     from oracle import OracleCase
     cases = configs.c1_pair(seed=1)
     s = Solver(cases)
-    s.cycle(3)
+    s.set_tuning(band_visit=[band] * 5)
+    # the first cycle launched kernel by kernel (profile_cycle), two more from the graph
+    assert any(k == "band_visit" for k, _, _ in s.profile_cycle()) == (band == 2)
+    s.cycle(2)
     for k, cfg in enumerate(cases):
         o = OracleCase(cfg)
         o.cycle(3)
@@ -57,12 +63,16 @@ def test_obstacle_flow_pair_long_run(oracle_built):
             o.close()
 
 
-def test_mixed_size_batch(oracle_built):
+@pytest.mark.parametrize("band", [0, 2])
+def test_mixed_size_batch(band, oracle_built):
+    """Cases of three sizes share every launch; band visits (on level 1 by default, on
+    levels 0-2 where they fit with band 2) cover cases smaller than the launch."""
     from mgfvm import Solver, configs
     from oracle import OracleCase
     cases = configs.c2(9, seed=2)
     assert {c.nfx for c in cases} == {64, 128, 256}
     s = Solver(cases)
+    s.set_tuning(band_visit=[band] * 6)
     s.cycle(2)
     for k, cfg in enumerate(cases):
         o = OracleCase(cfg)

@@ -42,14 +42,16 @@ def test_mixed_fixed_point_matches_fp64_oracle(cfg_name, oracle_built):
     s.close()
 
 
+@pytest.mark.parametrize("band", [0, 2])
 @pytest.mark.parametrize("isolve", [1, 2])
-def test_mixed_follows_fp64_on_obstacle_flow(isolve):
-    """128 x 128 obstacle flow (levels 0 and 1 smooth in tiles over several launches):
-    200 cycles of each form."""
+def test_mixed_follows_fp64_on_obstacle_flow(isolve, band):
+    """128 x 128 obstacle flow (levels 0 and 1 smooth in tiles over several launches;
+    with band 2, level 1 runs FP64 band visits): 200 cycles of each form."""
     from mgfvm import Solver, configs
     cfg = configs.small(128, 4, isolve=isolve, ig_obs=4, sc_obs=0.2,
                         obstacles=[(2, 3, 2, 2), (5, 6, 4, 6), (1, 1, 7, 8), (10, 12, 11, 13)])
     a, b = Solver(cfg), Solver(cfg, precision="mixed")
+    b.set_tuning(band_visit=[band] * 4)
     a.cycle(200)
     b.cycle(200)
     _compare(b, lambda f: a.field(0, 0, f), what="after 200 cycles")

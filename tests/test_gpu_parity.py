@@ -194,6 +194,9 @@ TUNINGS = [
     {"coarse_kernel": [0, 2, 2], "smooth_units": [4, 0, 0]},
     {"pdl": 1},
     {"pdl": 1, "smooth_tma": [2, 2, 2], "coarse_kernel": [0, 0, 2]},
+    {"band_visit": [2, 2, 2]},
+    {"band_visit": [2, 2, 2], "pdl": 1},
+    {"band_visit": [2, 2, 2], "update_pfix": [1, 1, 1], "coarse_kernel": [0, 0, 2]},
 ]
 
 
@@ -201,8 +204,9 @@ TUNINGS = [
 @pytest.mark.parametrize("k", range(len(TUNINGS)))
 def test_schedule_choices_bitexact(name, k, oracle_built):
     """Every schedule choice (units per smoother launch, smoother CTA size, assembly and
-    restriction slices) gives the oracle's bits; the 64-cell cases smooth level 0 in
-    tiles."""
+    restriction slices, band visits) gives the oracle's bits.  The 64-cell cases smooth
+    level 0 in tiles unless the tuning asks for band visits (a cluster of two CTAs per
+    case runs the whole level-0 visit, the mass error included)."""
     from mgfvm import configs
     cfg = dict(small_cases(),
                obs64_gs=configs.small(64, 3, isolve=2, ig_obs=3, sc_obs=0.2,
@@ -210,7 +214,7 @@ def test_schedule_choices_bitexact(name, k, oracle_built):
                obs64_odd_jacobi=configs.small(64, 3, isolve=1, nswpm=3, nswpp=9, ig_obs=3,
                                               obstacles=[(3, 4, 3, 5)]))[name]
     s, o = _pair(cfg)
-    s.set_tuning(**TUNINGS[k])
+    s.set_tuning(**{"band_visit": [1, 1, 1], **TUNINGS[k]})
     for n in (1, 3):
         s.cycle(n)
         o.cycle(n)
@@ -228,7 +232,7 @@ def test_autotune_keeps_state(oracle_built):
     before, after, chosen = s.autotune(2)
     assert before > 0 and 0 < after <= before
     assert set(chosen) == {"smooth_units", "smooth_threads", "asm_slices", "restrict_slices", "update_pfix", "odd_chunks", "pp_level",
-                           "smooth_tma", "coarse_kernel", "prol_fused", "tma_first_wait", "pdl"}
+                           "smooth_tma", "coarse_kernel", "prol_fused", "tma_first_wait", "pdl", "band_visit"}
     _compare(s, o, STATE, what="after autotune")
     s.cycle(3)
     o.cycle(3)
