@@ -392,6 +392,12 @@ def _ref_worker(args):
     return kind, (time.perf_counter() - t) / ncyc
 
 
+def _warm_worker(src):
+    """Loads the CPU implementation in a pool process (nothing is timed)."""
+    _cpu_case(src)
+    return 0
+
+
 def _ref_solve_worker(args):
     """One process: `ncyc` V-cycles of one case on the CPU from its initial state (the
     solve a GPU step ran); returns the level-0 u, v, p, sc and the seconds taken."""
@@ -596,25 +602,27 @@ def main():
         solver.reset()
         return solver.solve(max(c.nvcycle for c in cases), FP_TOL, allow_nonfinite=True)
 
+    # Parity of the timed result: the CPU runs every case of the workload for the cycles
+    # its GPU solve runs, from the same initial state, in background processes (one per
+    # case) while the GPU part runs; its final fields are the oracle of the solve.  The
+    # processes start (and finish their imports) before the warm-up steps, so that no
+    # interpreter start-up competes with the host thread that drives the timed steps.
+    parity_jobs = parity_pool = srcs = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline and n_cases <= 8 and not profiles:
+        # (per-face inlet profiles are not expressible as reference input files)
+        import dataclasses
+        import multiprocessing as mp
+        srcs = WORKLOAD_DIRS.get(a.workload) or [dataclasses.asdict(c) for c in cases]
+        parity_pool = mp.get_context("spawn").Pool(n_cases)
+        parity_pool.map(_warm_worker, srcs)
     for _ in range(a.warmup):
         cyc = step()
     # cases on which the reference's own iteration turns NaN/Inf stop at that cycle and
     # are not counted as solves (the reference's stop test never fires on NaN)
     diverged = solver.diverged()
-    # Parity of the timed result: the CPU runs every case of the workload for the cycles
-    # its GPU solve runs, from the same initial state, in background processes (one per
-    # case) while the GPU part runs; its final fields are the oracle of the solve.
-    parity_jobs = None
-    if rank == 0 and world == 1 and not a.no_cpu_baseline and n_cases <= 8:
-        import dataclasses
-        import multiprocessing as mp
-        srcs = WORKLOAD_DIRS.get(a.workload) or [dataclasses.asdict(c) for c in cases]
-        if profiles:
-            srcs = None    # per-face inlet profiles: not expressible as reference input files
-        if srcs:
-            parity_pool = mp.get_context("spawn").Pool(n_cases)
-            parity_t0 = time.perf_counter()
-            parity_jobs = parity_pool.map_async(_ref_solve_worker, [(srcs[k], int(cyc[k])) for k in range(n_cases)])
+    if parity_pool is not None:
+        parity_t0 = time.perf_counter()
+        parity_jobs = parity_pool.map_async(_ref_solve_worker, [(srcs[k], int(cyc[k])) for k in range(n_cases)])
     launches0 = solver.kernel_launches
     cycles = []
     e0 = torch.cuda.Event(enable_timing=True)

@@ -397,6 +397,15 @@ struct Builder {
         }
         return true;
     }
+    // Whether the launch about to be added follows a smoother launch (or the copy back
+    // of its buffers), with programmatic dependent launch on: masserror+coefp and update
+    // then read the operands that smoothers do not write before waiting for it.
+    bool after_smoother(int mode) const
+    {
+        if (!x->sched.pdl || mode == M_OP || out->empty()) return false;
+        const int k = out->back().kernel;
+        return k == K_SMOOTH || k == K_SMOOTH_F32 || k == K_SMOOTH_TMA || k == K_COPY;
+    }
     // returns the update's fuse bits (0: outflow still to do)
     // `bound_bits` != 0: pbound/outflow follow the obstacle pressure copy (k_bound bits);
     // when both have work they run as one kernel, one CTA per case.
@@ -406,11 +415,12 @@ struct Builder {
         // mixed precision: p' operands and p' itself in FP32 (p' needs a smoothing to be set)
         const bool f32 = f32_level(ig, mode) && x->sched.nswpp > 0;
         const int jac = x->sched.isolve == MGFVM_JACOBI ? 4 : 0;
-        add(K_MASS_COEFP, ig, mode, cells(ig), reduce ? 1 : 0, (uvsc_in_tmp ? 1 : 0) | (f32 ? 2 | jac : 0));
+        add(K_MASS_COEFP, ig, mode, cells(ig), reduce ? 1 : 0,
+            (uvsc_in_tmp ? 1 : 0) | (f32 ? 2 | jac : 0) | (after_smoother(mode) ? 8 : 0));
         const bool chain = mode != M_OP && x->tune.odd_chunks[ig] != 1;
         if (smooth(ig, mode, 1 << EQ_PP, x->sched.nswpp, chain)) fuse |= 8;
         if (f32) fuse |= 16 | (f32_buf ? 32 : 0);
-        add(K_UPDATE, ig, mode, cells(ig) + 2, fuse);
+        add(K_UPDATE, ig, mode, cells(ig) + 2, fuse | (after_smoother(mode) ? 64 : 0));
         return after_update(ig, mode, fuse, bound_bits);
     }
     // the obstacle pressure copy (unless update did it: fuse bit 4) and pbound/outflow

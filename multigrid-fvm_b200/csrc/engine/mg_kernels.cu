@@ -256,15 +256,24 @@ __global__ void __launch_bounds__(BLOCK) k_asm(const CaseDev *__restrict__ cs, C
 // threads copy the ghosts of the boundary rows.
 // One interior cell of update (+ the fusions above): ppq, ppe, ppn = p' at the cell and
 // its east and north neighbours.
+// the values of its own cell an update reads besides p'
+struct UpdIn {
+    double u, v, p, ax, ay, apu, apv;
+};
+__device__ __forceinline__ UpdIn update_in(const LevelDev &L, int q)
+{
+    return {MGF(L, S_U)[q], MGF(L, S_V)[q], MGF(L, S_P)[q], MGF(L, S_AREAX)[q], MGF(L, S_AREAY)[q],
+            MGF(L, S_APU)[q], MGF(L, S_APV)[q]};
+}
 __device__ __forceinline__ void update_cell(const LevelDev &L, const CaseDev &C, int i, int j, double ppq, double ppe,
-                                            double ppn, bool out, int fuse)
+                                            double ppn, bool out, int fuse, const UpdIn &in)
 {
     const int nx = L.npx, q = j * nx + i;
     double *u = MGF(L, S_U), *v = MGF(L, S_V), *p = MGF(L, S_P);
     const double ppref = 0.0;
-    const double un = u[q] + MGF(L, S_AREAX)[q] * (ppq - ppe) / MGF(L, S_APU)[q];
-    const double vn = v[q] + MGF(L, S_AREAY)[q] * (ppq - ppn) / MGF(L, S_APV)[q];
-    const double pn = p[q] + C.relxp * (ppq - ppref);
+    const double un = in.u + in.ax * (ppq - ppe) / in.apu;
+    const double vn = in.v + in.ay * (ppq - ppn) / in.apv;
+    const double pn = in.p + C.relxp * (ppq - ppref);
     const int code = ((fuse & 4) && L.pcode) ? L.pcode[q] : 0;
     if (code & ~PCODE_DST) {
         for (int k = (code & ~PCODE_DST) - 1;; ++k) {
@@ -286,27 +295,47 @@ __device__ __forceinline__ void update_cell(const LevelDev &L, const CaseDev &C,
         if (fuse & 2) MGF(L, S_SC)[q + 1] = MGF(L, S_SC)[q];
     }
 }
+__device__ __forceinline__ void update_cell(const LevelDev &L, const CaseDev &C, int i, int j, double ppq, double ppe,
+                                            double ppn, bool out, int fuse)
+{
+    update_cell(L, C, i, j, ppq, ppe, ppn, out, fuse, update_in(L, j * L.npx + i));
+}
 
 __global__ void __launch_bounds__(BLOCK) k_update(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode,
                                                   int fuse)
 {
-    pdl_enter();
-    CASE_PROLOGUE(mode);
+    // fuse bit 64: the previous launch is a p' smoother, which writes none of the cell's
+    // other operands (u, v, p, areas, apu, apv): they are read before waiting for it
+    const bool early = (fuse & 64) != 0;
+    if (!early) pdl_enter();
+    const CaseDev &C = cs[blockIdx.y];
+    const LevelDev &L = C.lv[ig];
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const Dom d = dom_interior(L);
-    const int n = d.wi * d.wj, nx = L.npx;
-    const bool out = (fuse & 1) && C.ibc_xp == 4;
     int i, j;
-    if (cell_at(d, t, i, j)) {
+    const bool cell = mode_active(C, ig, mode) && cell_at(d, t, i, j);
+    const int nx = L.npx;
+    UpdIn in{};
+    if (early) {
+        if (cell) in = update_in(L, j * nx + i);
+        pdl_enter();
+    }
+    CaseState &ST = st[blockIdx.y];
+    if (!case_active(C, ST, ig, mode)) return;
+    const int n = d.wi * d.wj;
+    const bool out = (fuse & 1) && C.ibc_xp == 4;
+    if (cell) {
         const int q = j * nx + i;
+        if (!early) in = update_in(L, q);
         if (fuse & 16) {   // mixed precision: p' is FP32, in buffer (fuse & 32 ? 1 : 0) of its correction
             const float *pf = del32(L, EQ_PP, (fuse & 32) ? 1 : 0);
-            update_cell(L, C, i, j, (double)pf[q], (double)pf[q + 1], (double)pf[q + nx], out, fuse);
+            update_cell(L, C, i, j, (double)pf[q], (double)pf[q + 1], (double)pf[q + nx], out, fuse, in);
             return;
         }
         const double *pp = MGF(L, (fuse & 8) ? S_TMP0 : S_PP);
         const double ppq = pp[q];
         if (fuse & 8) MGF(L, S_PP)[q] = ppq;
-        update_cell(L, C, i, j, ppq, pp[q + 1], pp[q + nx], out, fuse);
+        update_cell(L, C, i, j, ppq, pp[q + 1], pp[q + nx], out, fuse, in);
     } else if (out && t < n + 2) {
         const int jb = t == n ? 0 : L.npy - 1;
         row_outflow(L, jb, (fuse & 2) != 0);
@@ -321,17 +350,52 @@ __global__ void __launch_bounds__(BLOCK) k_update(const CaseDev *__restrict__ cs
 __global__ void __launch_bounds__(BLOCK) k_mass_coefp(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode, int reduce,
                                                       int flags)
 {
-    pdl_enter();
-    CASE_PROLOGUE(mode);
+    // flags bit 8: the previous launch is a smoother, which writes none of the
+    // coefficients' operands (areas, apu, apv, tag): they are formed before waiting for it
+    const bool early = (flags & 8) != 0;
+    if (!early) pdl_enter();
+    const CaseDev &C = cs[blockIdx.y];
+    const LevelDev &L = C.lv[ig];
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const Dom d = dom_interior(L);
+    int i, j;
+    const bool cell = mode_active(C, ig, mode) && cell_at(d, t, i, j);
+    Coef k;
+    double su = 0.0;
+    if (early) {
+        if (cell) mass_coefp_io(Prim{L}, C, i, j, k, su, S_U, S_V, MC_COEF);
+        pdl_enter();
+    }
+    CaseState &ST = st[blockIdx.y];
+    if (!case_active(C, ST, ig, mode)) return;
     const int n = d.wi * d.wj, nb = (n + blockDim.x - 1) / blockDim.x;
     if ((int)blockIdx.x >= nb) return;
     double a[1] = {0.0};
-    int i, j;
-    if (cell_at(d, t, i, j)) {
+    if (cell && early) {
+        const Prim io{L};
+        const int q = j * L.npx + i;
+        const int us = (flags & 1) ? S_TMP0 : S_U, vs = (flags & 1) ? S_TMP1 : S_V;
+        a[0] = mass_coefp_io(io, C, i, j, k, su, us, vs, MC_SU);
         if (flags & 2) {
-            Coef k;
-            double su;
+            const double ap = (flags & 4) ? k.ap + 1.0e-30 : k.ap;
+            op32(L, EQ_PP, CK_AW)[q] = (float)k.aw;
+            op32(L, EQ_PP, CK_AE)[q] = (float)k.ae;
+            op32(L, EQ_PP, CK_AS)[q] = (float)k.as;
+            op32(L, EQ_PP, CK_AN)[q] = (float)k.an;
+            op32(L, EQ_PP, CK_AP)[q] = (float)(1.0 / ap);
+            op32(L, EQ_PP, CK_SU)[q] = (float)su;
+        } else {
+            // cell_mass_coefp's stores
+            if (flags & 1) {
+                if (i <= L.npx - 3) io.st(S_U, q, io.ld(us, q));
+                if (j <= L.npy - 3) io.st(S_V, q, io.ld(vs, q));
+                io.st(S_SC, q, io.ld(S_TMP2, q));
+            }
+            io.st(S_PP, q, 0.0);
+            store_coef(io, EQ_PP, q, k, su);
+        }
+    } else if (cell) {
+        if (flags & 2) {
             a[0] = mass_coefp_values(L, C, i, j, k, su, S_U, S_V);
             const int q = j * L.npx + i;
             const double ap = (flags & 4) ? k.ap + 1.0e-30 : k.ap;
@@ -1756,8 +1820,10 @@ __global__ void __launch_bounds__(TAIL_BLOCK, 1) k_tail(const CaseDev *__restric
 
 // The same levels with every value paired with its derivative along the case's
 // parameter direction (forward mode, mg_tangent.cuh): the value bits are those of
-// k_tail, the derivatives those of the same V-cycle.
-__global__ void __launch_bounds__(TAIL_BLOCK, 1) k_tail_tan(const CaseDev *__restrict__ cs, CaseState *st,
+// k_tail, the derivatives those of the same V-cycle.  Two CTAs per SM (64 registers,
+// some spilled): a gradient's 258 directions of a 256^2 case then run as one wave on
+// 148 SMs instead of 1.7 (27.8 vs 29.5 ms per V-cycle).
+__global__ void __launch_bounds__(TAIL_BLOCK, 2) k_tail_tan(const CaseDev *__restrict__ cs, CaseState *st,
                                                             const CaseTan *__restrict__ ts, Sched S)
 {
     pdl_enter();
