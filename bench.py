@@ -505,10 +505,11 @@ def main():
     ap.add_argument("--profile-adjoint", type=int, default=0,
                     help="only run the reverse mode over this many V-cycles of one adjoint-configuration case "
                          "(256x256) after a 1-cycle warm-up, the timed run inside the NVTX range 'profile', and exit")
-    ap.add_argument("--profile-batch-smoother", choices=["plain", "tma"], default=None,
+    ap.add_argument("--profile-batch-smoother", choices=["plain", "tma", "band"], default=None,
                     help="only run one V-cycle of the 64-case obstacle-flow batch (levels 0-2 smoothed by "
-                         "512-thread tiles of 6 units, per-thread or TMA-staged loads) after 3 warm-up cycles, "
-                         "inside the NVTX range 'profile', and exit")
+                         "512-thread tiles of 6 units, per-thread or TMA-staged loads; 'band': the default "
+                         "schedule, levels 1-2 by band visits) after 3 warm-up cycles, inside the NVTX range "
+                         "'profile', and exit")
     a = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -542,8 +543,9 @@ def main():
         cases = [configs.c1(10.0 if k % 2 == 0 else 100.0, seed=k + 1) for k in range(64)]
         t = 2 if a.profile_batch_smoother == "tma" else 1
         with Solver(cases, device=local) as s:
-            s.set_tuning(smooth_units={0: 6, 1: 6, 2: 6}, smooth_threads={0: 512, 1: 512, 2: 512},
-                         smooth_tma={0: t, 1: t, 2: t})
+            if a.profile_batch_smoother != "band":
+                s.set_tuning(smooth_units={0: 6, 1: 6, 2: 6}, smooth_threads={0: 512, 1: 512, 2: 512},
+                             smooth_tma={0: t, 1: t, 2: t}, band_visit=[1] * 5)
             s.cycle(3)
             torch.cuda.nvtx.range_push("profile")
             s.cycle(1)

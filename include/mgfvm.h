@@ -189,6 +189,12 @@ typedef struct mgfvm_tuning {
                                               shared memory; FP64 in either precision):
                                               the whole visit in one launch: 2 yes, 1 no,
                                               0 yes in batches of at least 32 cases     */
+    int coarse_cluster;                    /* every level from the first one a CTA per case
+                                              holds down to the coarsest, with the
+                                              transfers into and out of it, as one launch
+                                              of a cluster of three CTAs per case: 2 yes,
+                                              0 or 1 no (measured slower: its transfers
+                                              run on three SMs)                         */
 } mgfvm_tuning;
 
 typedef struct mgfvm_ctx mgfvm_ctx;

@@ -531,16 +531,56 @@ struct Builder {
         if (!fused) add(K_PROL_CORR, ig, mode, cells(ig + 1));
         add(K_PROL_APPLY, ig, mode, cells(ig), fused ? 1 : 0);
     }
+    // The first level of the coarse cluster launch (k_coarse_cycle, when the tuning asks
+    // for it): the first level one CTA per case holds, when every level from there down
+    // is run by the V-cycle's
+    // grid kernels (no one-CTA coarse kernel, no tangent), takes whole-level visits
+    // (pp_level), the smoother is GS or Jacobi and p' is smoothed; x->maxng when there
+    // is none.
+    int coarse_from() const
+    {
+        if (x->tune.coarse_cluster != 2 || x->opt.tangent || x->sched.nswpp <= 0 ||
+            (x->sched.isolve != MGFVM_JACOBI && x->sched.isolve != MGFVM_GAUSS_SEIDEL))
+            return x->maxng;
+        for (const CaseDev &C : x->hc)
+            if (C.tail < C.ngrid) return x->maxng;
+        for (int ig = 0; ig < x->maxng; ++ig) {
+            int mx, my;
+            if (!whole_level(ig, mx, my)) continue;
+            for (int k = ig; k < x->maxng; ++k)
+                if (x->tune.pp_level[k] == 1) return x->maxng;   // whole-level visits turned off
+            return ig;
+        }
+        return x->maxng;
+    }
     void cycle()
     {
         bool asm_done = false;
-        for (int ig = 0; ig < x->maxng; ++ig) {
+        const int c0 = coarse_from();
+        for (int ig = 0; ig < c0; ++ig) {
             if (any(ig, M_DOWN)) step(ig, M_DOWN, true, ig == 0, asm_done);
             asm_done = false;
-            if (any(ig, M_RESTRICT)) {
+            if (ig + 1 < c0 && any(ig, M_RESTRICT)) {
                 asm_done = any(ig + 1, M_DOWN);
                 restrict_(ig, M_RESTRICT, asm_done);
             }
+        }
+        if (c0 < x->maxng) {
+            // the rest of the down leg, the coarse levels and the up leg back into c0 - 1
+            int mx, my;
+            whole_level(c0, mx, my);
+            const int isolve = x->sched.isolve;
+            Launch L{};
+            L.kernel = K_COARSE_CYCLE;
+            L.ig = c0;
+            L.a0 = c0;
+            L.a1 = isolve == MGFVM_GAUSS_SEIDEL ? 2 * x->sched.nswpp : x->sched.nswpp;
+            L.a2 = std::max(0, isolve == MGFVM_GAUSS_SEIDEL ? 2 * x->sched.nswpm : x->sched.nswpm);
+            L.grid = dim3(3, x->ncases);
+            L.block = SMOOTH_BLOCK;
+            L.smem = (isolve == MGFVM_JACOBI ? 2 : 1) * mx * my * (int)sizeof(double);
+            out->push_back(L);
+            if (c0 >= 2 && any(c0 - 1, M_PROLONG)) step(c0 - 1, M_UP, false, false);
         }
         bool tail = false;
         for (const CaseDev &C : x->hc) tail |= C.tail < C.ngrid;
@@ -558,7 +598,7 @@ struct Builder {
             L.smem = x->opt.tangent ? 0 : (int)std::min<long long>(need, TAIL_SMEM_MAX);
             out->push_back(L);
         }
-        for (int ig = x->maxng - 1; ig > 0; --ig) {
+        for (int ig = std::min(x->maxng, c0) - 1; ig > 0; --ig) {
             if (!any(ig - 1, M_PROLONG)) continue;
             prolong(ig - 1, M_PROLONG);
             if (ig != 1) step(ig - 1, M_UP, false, false);
@@ -1585,7 +1625,7 @@ static bool tuning_valid(const mgfvm_tuning &t)
         if (t.prol_fused[ig] < 0 || t.prol_fused[ig] > 2) return false;
         if (t.band_visit[ig] < 0 || t.band_visit[ig] > 2) return false;
     }
-    return t.tma_first_wait >= -1 && t.pdl >= 0 && t.pdl <= 2;
+    return t.tma_first_wait >= -1 && t.pdl >= 0 && t.pdl <= 2 && t.coarse_cluster >= 0 && t.coarse_cluster <= 2;
 }
 
 // The first level of the one-CTA coarse kernel from x->tune.coarse_kernel (the first
@@ -1702,6 +1742,7 @@ int mgfvm_autotune(mgfvm_ctx *x, int cycles, mgfvm_tuning *chosen, double *ms_be
             }
             if (ig >= 1 && ig >= x->maxng - 3) knobs.push_back({4, 2, 0});   // one-CTA kernel from here down
             if (ig + 1 < x->maxng) knobs.push_back({5, 1, 0});                 // separate correction kernel
+            if (ig == 0) knobs.push_back({7, x->tune.coarse_cluster == 2 ? 1 : 2, 0});   // coarse cluster launch
             knobs.push_back({1, 1, 0});
             knobs.push_back({1, 3, 0});
             if (ig + 1 < x->maxng) {
@@ -1717,6 +1758,7 @@ int mgfvm_autotune(mgfvm_ctx *x, int cycles, mgfvm_tuning *chosen, double *ms_be
                 if (k[0] == 4) cand.coarse_kernel[ig] = k[1];
                 if (k[0] == 5) cand.prol_fused[ig] = k[1];
                 if (k[0] == 6) cand.band_visit[ig] = k[1];
+                if (k[0] == 7) cand.coarse_cluster = k[1];
                 if (memcmp(&cand, &keep, sizeof cand) == 0) continue;
                 x->tune = cand;
                 rebuild_schedule(x);

@@ -1818,6 +1818,84 @@ __global__ void __launch_bounds__(TAIL_BLOCK, 1) k_tail(const CaseDev *__restric
     tail_cycle(PrimCase{C}, ST, S, tsm, smem_doubles);
 }
 
+// ------------------------------------------------ the coarse levels in one cluster launch
+// Everything a V-cycle does from the restriction into level c0 (the first level one
+// CTA holds) to the prolongation out of it, as one launch of a cluster of three CTAs
+// per case (rank r): restv + fine fluxes and the FAS restriction (:211-220; slice r of
+// three, one cluster barrier after each), each down-leg visit (:201-207), the
+// prolongations back up (:230-233, the gather forming its corrections from the saved
+// R(x_f)) and the up-leg visits (:235-244).  A visit: the assembly (slice r) | barrier |
+// u, v, sc smoothing (equation r, in place) | barrier | CTA 0: masserror + coefp, the p'
+// units and update (pp_level_body), then the obstacle pressure copy and pbound /
+// outflow of the level | barrier.  The kernels it replaces in the same order, so the
+// same bits.  Which levels and transfers a case takes follows its mode flags
+// (mode_active); every CTA of a cluster sees the same flags and takes the same barriers.
+template <int ISOLVE>
+__device__ void cl_visit(const CaseDev &C, CaseState &ST, int ig, bool down, int nu, int mu, int r, double *sm)
+{
+    const LevelDev &L = C.lv[ig];
+    const unsigned what = A_FLUX | A_U | A_V | A_SC | (down ? A_SC_OUTFLOW : 0u);
+    const unsigned w = asm_slice(what, r, 3);
+    const int n = L.npx * L.npy;
+    for (int q = threadIdx.x; q < n; q += blockDim.x) cell_asm(L, C, FluxLive(L), q % L.npx, q / L.npx, w);
+    cluster_barrier();
+    if (mu > 0 && level_smooth_eq<ISOLVE>(L, r == 0 ? EQ_U : r == 1 ? EQ_V : EQ_SC, mu, sm) == 2 &&
+        threadIdx.x == 0)
+        atomicOr(&ST.status, (int)CASE_BAD_LAUNCH);   // the schedule sizes blocks to fit; never taken
+    cluster_barrier();
+    if (r == 0) {
+        pp_level_body<ISOLVE>(C, ST, L, nu, ig == 0 && down, 0, sm);
+        __syncthreads();
+        pfix_block_io(Prim{L});
+        bound_block_io(C, Prim{L}, down ? 3 : 7);
+    }
+    cluster_barrier();
+}
+
+// restriction ig -> ig + 1 by a cluster: slice r of three over every cell
+__device__ void cl_restrict(const CaseDev &C, int ig, int r)
+{
+    const LevelDev &F = C.lv[ig], &K = C.lv[ig + 1];
+    for (int q = threadIdx.x; q < F.npx * F.npy; q += blockDim.x)
+        cell_restv_fluxes(F, K, C, q % F.npx, q / F.npx, r, 3);
+    cluster_barrier();
+    for (int q = threadIdx.x; q < K.npx * K.npy; q += blockDim.x)
+        cell_restrict_fluxes(F, K, C, q % K.npx, q / K.npx, r, 3);
+    cluster_barrier();
+}
+
+// prolongation ig + 1 -> ig by a cluster: the interior cells of level ig split over it
+__device__ void cl_prolong(const CaseDev &C, int ig, int r)
+{
+    const LevelDev &F = C.lv[ig], &K = C.lv[ig + 1];
+    const Dom d = dom_interior(F);
+    for (int t = r * blockDim.x + threadIdx.x; t < d.wi * d.wj; t += 3 * blockDim.x)
+        cell_prol_apply<true>(F, K, d.i0 + t % d.wi, d.j0 + t / d.wi);
+    cluster_barrier();
+}
+
+template <int ISOLVE>
+__global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(SMOOTH_BLOCK, 1)
+    k_coarse_cycle(const CaseDev *__restrict__ cs, CaseState *st, int c0, int nu, int mu)
+{
+    pdl_enter();
+    extern __shared__ double sm[];
+    const CaseDev &C = cs[blockIdx.y];
+    CaseState &ST = st[blockIdx.y];
+    if (ST.done) return;   // the same for the three CTAs
+    const int r = blockIdx.x;
+    if (c0 >= 1 && mode_active(C, c0 - 1, M_RESTRICT)) cl_restrict(C, c0 - 1, r);
+    for (int ig = c0; ig < C.ngrid; ++ig) {
+        if (mode_active(C, ig, M_DOWN)) cl_visit<ISOLVE>(C, ST, ig, true, nu, mu, r, sm);
+        if (mode_active(C, ig, M_RESTRICT)) cl_restrict(C, ig, r);
+    }
+    for (int ig = C.ngrid - 1; ig >= c0 && ig >= 1; --ig) {
+        if (!mode_active(C, ig - 1, M_PROLONG)) continue;
+        cl_prolong(C, ig - 1, r);
+        if (ig - 1 >= c0 && ig != 1) cl_visit<ISOLVE>(C, ST, ig - 1, false, nu, mu, r, sm);
+    }
+}
+
 // The same levels with every value paired with its derivative along the case's
 // parameter direction (forward mode, mg_tangent.cuh): the value bits are those of
 // k_tail, the derivatives those of the same V-cycle.  Two CTAs per SM (64 registers,
@@ -1988,6 +2066,13 @@ cudaError_t launch_one(const Launch &X, const CaseDev *dc, CaseState *ds, const 
             le = launch_k(pdl, k_level_visit<MGFVM_JACOBI>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
         else
             le = launch_k(pdl, k_level_visit<MGFVM_GAUSS_SEIDEL>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+        break;
+    case K_COARSE_CYCLE:
+        if (b > SMOOTH_BLOCK || g.x != 3) return cudaErrorInvalidValue;
+        if (S.isolve == MGFVM_JACOBI)
+            le = launch_k(pdl, k_coarse_cycle<MGFVM_JACOBI>, g, b, X.smem, st, dc, ds, X.a0, X.a1, X.a2);
+        else
+            le = launch_k(pdl, k_coarse_cycle<MGFVM_GAUSS_SEIDEL>, g, b, X.smem, st, dc, ds, X.a0, X.a1, X.a2);
         break;
     case K_BAND_VISIT:
         if (b > SMOOTH_BLOCK || g.x < 1 || g.x > BAND_MAX_CTAS || X.smem > BAND_SMEM_MAX) return cudaErrorInvalidValue;

@@ -32,6 +32,9 @@ enum KernelId {
     K_SMOOTH_TMA,    // as K_SMOOTH, the region staged by TMA box loads (bw, bh, ptr)
     K_BAND_VISIT,    // a whole level visit, a cluster of grid.x CTAs per case (bands of rows):
                      // K_LEVEL_VISIT's arguments
+    K_COARSE_CYCLE,  // the V-cycle from the restriction into level a0 (every level from a0
+                     // one CTA holds) to the prolongation out of it, a cluster of 3 CTAs per
+                     // case: a1 = p' units, a2 = u/v/sc units
     K_NKERNELS
 };
 

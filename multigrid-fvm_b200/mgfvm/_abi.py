@@ -77,7 +77,8 @@ class Tuning(C.Structure):
                 ("update_pfix", C.c_int * MAX_LEVELS), ("odd_chunks", C.c_int * MAX_LEVELS),
                 ("pp_level", C.c_int * MAX_LEVELS), ("smooth_tma", C.c_int * MAX_LEVELS),
                 ("coarse_kernel", C.c_int * MAX_LEVELS), ("prol_fused", C.c_int * MAX_LEVELS),
-                ("tma_first_wait", C.c_int), ("pdl", C.c_int), ("band_visit", C.c_int * MAX_LEVELS)]
+                ("tma_first_wait", C.c_int), ("pdl", C.c_int), ("band_visit", C.c_int * MAX_LEVELS),
+                ("coarse_cluster", C.c_int)]
 
     def as_dict(self):
         return {k: (list(v) if isinstance(v := getattr(self, k), C.Array) else v) for k, _ in self._fields_}

@@ -196,7 +196,7 @@ class Solver:
 
     KERNELS = ["fluxes", "asm", "mass_coefp", "update", "pfix", "bound", "smooth", "copy", "restv_fluxes",
                "restrict", "prol_corr", "prol_apply", "tail", "endcycle", "prol_apply_end", "smooth_mixed", "pfix_bound", "pp_level",
-               "tail_tan", "level_visit", "smooth_tma", "band_visit"]
+               "tail_tan", "level_visit", "smooth_tma", "band_visit", "coarse_cycle"]
 
     def profile_cycle(self):
         """One directly-launched V-cycle with an event after every kernel: a list of

@@ -24,17 +24,21 @@ def _check(s, k, o, cycles, what, levels=(0, 1)):
     np.testing.assert_allclose(s.history(k)[0], o.history()[0], rtol=1e-12, atol=0)
 
 
-@pytest.mark.parametrize("band", [2, 1])
-def test_obstacle_flow_pair(band, oracle_built):
+@pytest.mark.parametrize("band,coarse", [(2, 2), (1, 0)])
+def test_obstacle_flow_pair(band, coarse, oracle_built):
     """Levels 1 and 2 (130^2 and 66^2 padded) by band visits (a cluster of 8 and of 2
-    CTAs per case; band 2) and by the tile smoothers (band 1, the default for two cases)."""
+    CTAs per case; band 2) and by the tile smoothers (band 1, the default for two cases);
+    levels 3 and 4 with the transfers into and out of them in one cluster launch
+    (coarse 2) and by their separate launches (coarse 0, the default)."""
     from mgfvm import Solver, configs
     from oracle import OracleCase
     cases = configs.c1_pair(seed=1)
     s = Solver(cases)
-    s.set_tuning(band_visit=[band] * 5)
+    s.set_tuning(band_visit=[band] * 5, coarse_cluster=coarse)
     # the first cycle launched kernel by kernel (profile_cycle), two more from the graph
-    assert any(k == "band_visit" for k, _, _ in s.profile_cycle()) == (band == 2)
+    kinds = {k for k, _, _ in s.profile_cycle()}
+    assert ("band_visit" in kinds) == (band == 2)
+    assert ("coarse_cycle" in kinds) == (coarse == 2)
     s.cycle(2)
     for k, cfg in enumerate(cases):
         o = OracleCase(cfg)

@@ -197,6 +197,10 @@ TUNINGS = [
     {"band_visit": [2, 2, 2]},
     {"band_visit": [2, 2, 2], "pdl": 1},
     {"band_visit": [2, 2, 2], "update_pfix": [1, 1, 1], "coarse_kernel": [0, 0, 2]},
+    {"coarse_cluster": 2},
+    {"coarse_cluster": 2, "pdl": 1, "smooth_units": [3, 5, 7]},
+    {"coarse_cluster": 2, "update_pfix": [1, 1, 1], "odd_chunks": [1, 1, 1]},
+    {"coarse_cluster": 2, "band_visit": [2, 2, 2], "pdl": 1},
 ]
 
 
@@ -232,7 +236,8 @@ def test_autotune_keeps_state(oracle_built):
     before, after, chosen = s.autotune(2)
     assert before > 0 and 0 < after <= before
     assert set(chosen) == {"smooth_units", "smooth_threads", "asm_slices", "restrict_slices", "update_pfix", "odd_chunks", "pp_level",
-                           "smooth_tma", "coarse_kernel", "prol_fused", "tma_first_wait", "pdl", "band_visit"}
+                           "smooth_tma", "coarse_kernel", "prol_fused", "tma_first_wait", "pdl", "band_visit",
+                           "coarse_cluster"}
     _compare(s, o, STATE, what="after autotune")
     s.cycle(3)
     o.cycle(3)
