@@ -328,6 +328,12 @@ class ClockSampler:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
+            # let nvidia-smi finish its start-up (driver initialisation) before the timed
+            # region opens: its first sample marks it as running
+            for _ in range(100):
+                if os.path.getsize(self.path) > 0 or self.proc.poll() is not None:
+                    break
+                time.sleep(0.05)
         except Exception:
             self.proc = None
         return self
@@ -573,7 +579,7 @@ def main():
         solver.set_inlet_profile(k, pr)
     tuned = None
     if not a.no_autotune:
-        t_before, t_after, tuned = solver.autotune(5)
+        t_before, t_after, tuned = solver.autotune(20)
         log(f"autotune: {t_before * 1e3:.1f} -> {t_after * 1e3:.1f} us per cycle")
     if a.profile_cycles:
         solver.cycle(3)
