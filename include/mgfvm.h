@@ -188,7 +188,8 @@ typedef struct mgfvm_tuning {
                                               rows, halo rows exchanged in distributed
                                               shared memory; FP64 in either precision):
                                               the whole visit in one launch: 2 yes, 1 no,
-                                              0 yes in batches of at least 32 cases     */
+                                              0 yes in batches of at least 32 cases
+                                              that all have the level at one size      */
     int coarse_cluster;                    /* every level from the first one a CTA per case
                                               holds down to the coarsest, with the
                                               transfers into and out of it, as one launch

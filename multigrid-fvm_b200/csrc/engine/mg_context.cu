@@ -264,14 +264,24 @@ struct Builder {
     }
     // Whether the visits to level ig run as band visits (k_band_visit, FP64 in either
     // precision): the level fits a cluster and the tuning asks for them, or leaves it
-    // to the default, which takes them for batches of at least BAND_MIN_CASES cases.
+    // to the default, which takes them for batches of at least BAND_MIN_CASES cases
+    // that all have the level at one size (a launch is shaped for its largest case, so
+    // smaller ones would leave most of their clusters' threads idle).
     bool band_visits(int ig, int mode, int &G, int &blk, int &smem) const
     {
         const int isolve = x->sched.isolve, t = x->tune.band_visit[ig];
         int mx, my;
         return mode != M_OP && x->sched.nswpp > 0 && t != 1 &&
                (isolve == MGFVM_JACOBI || isolve == MGFVM_GAUSS_SEIDEL) && !whole_level(ig, mx, my) &&
-               band_level(ig, G, blk, smem) && (t == 2 || x->ncases >= BAND_MIN_CASES);
+               band_level(ig, G, blk, smem) &&
+               (t == 2 || (x->ncases >= BAND_MIN_CASES && one_size(ig, mx, my)));
+    }
+    // every case that has level ig has it at mx x my
+    bool one_size(int ig, int mx, int my) const
+    {
+        for (const mgfvm_config &c : x->cfg)
+            if (ig < c.ngrid && (npx_of(c, ig) != mx || npy_of(c, ig) != my)) return false;
+        return true;
     }
     int f32_buf = 0;   // the FP32 correction buffer the last F32 smoothing call ended in
     bool smooth(int ig, int mode, int mask, int nsw, bool tmp_ok = false)

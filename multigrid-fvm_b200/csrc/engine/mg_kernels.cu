@@ -301,32 +301,23 @@ __device__ __forceinline__ void update_cell(const LevelDev &L, const CaseDev &C,
     update_cell(L, C, i, j, ppq, ppe, ppn, out, fuse, update_in(L, j * L.npx + i));
 }
 
+// EARLY: the previous launch is a p' smoother, which writes none of the cell's other
+// operands (u, v, p, areas, apu, apv), so they are read before waiting for it (a
+// finished case, ST.done, set at the end of a cycle, loads nothing).
+template <bool EARLY>
 __global__ void __launch_bounds__(BLOCK) k_update(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode,
                                                   int fuse)
 {
-    // fuse bit 64: the previous launch is a p' smoother, which writes none of the cell's
-    // other operands (u, v, p, areas, apu, apv): they are read before waiting for it
-    const bool early = (fuse & 64) != 0;
-    if (!early) pdl_enter();
-    const CaseDev &C = cs[blockIdx.y];
-    const LevelDev &L = C.lv[ig];
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (!EARLY) pdl_enter();
+    CASE_PROLOGUE(mode);
     const Dom d = dom_interior(L);
-    int i, j;
-    const bool cell = mode_active(C, ig, mode) && cell_at(d, t, i, j);
-    const int nx = L.npx;
-    UpdIn in{};
-    if (early) {
-        if (cell) in = update_in(L, j * nx + i);
-        pdl_enter();
-    }
-    CaseState &ST = st[blockIdx.y];
-    if (!case_active(C, ST, ig, mode)) return;
-    const int n = d.wi * d.wj;
+    const int n = d.wi * d.wj, nx = L.npx;
     const bool out = (fuse & 1) && C.ibc_xp == 4;
-    if (cell) {
+    int i, j;
+    if (cell_at(d, t, i, j)) {
         const int q = j * nx + i;
-        if (!early) in = update_in(L, q);
+        const UpdIn in = update_in(L, q);
+        if (EARLY) pdl_enter();
         if (fuse & 16) {   // mixed precision: p' is FP32, in buffer (fuse & 32 ? 1 : 0) of its correction
             const float *pf = del32(L, EQ_PP, (fuse & 32) ? 1 : 0);
             update_cell(L, C, i, j, (double)pf[q], (double)pf[q + 1], (double)pf[q + nx], out, fuse, in);
@@ -336,9 +327,12 @@ __global__ void __launch_bounds__(BLOCK) k_update(const CaseDev *__restrict__ cs
         const double ppq = pp[q];
         if (fuse & 8) MGF(L, S_PP)[q] = ppq;
         update_cell(L, C, i, j, ppq, pp[q + 1], pp[q + nx], out, fuse, in);
-    } else if (out && t < n + 2) {
-        const int jb = t == n ? 0 : L.npy - 1;
-        row_outflow(L, jb, (fuse & 2) != 0);
+    } else {
+        if (EARLY) pdl_enter();
+        if (out && t < n + 2) {
+            const int jb = t == n ? 0 : L.npy - 1;
+            row_outflow(L, jb, (fuse & 2) != 0);
+        }
     }
 }
 
@@ -347,55 +341,54 @@ __global__ void __launch_bounds__(BLOCK) k_update(const CaseDev *__restrict__ cs
 // launches); read from there and copied back.  Bit 2: mixed precision, p' operands
 // stored in FP32 (r = su, as p' starts from zero; p' itself is not written); bit 4:
 // with bit 2, the smoother is Jacobi.
+// EARLY: the previous launch is a smoother, which writes none of the coefficients'
+// operands (areas, apu, apv, tag): the coefficients are formed before waiting for it,
+// u and v read after (a finished case, ST.done, set at the end of a cycle, forms nothing).
+template <bool EARLY>
 __global__ void __launch_bounds__(BLOCK) k_mass_coefp(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode, int reduce,
                                                       int flags)
 {
-    // flags bit 8: the previous launch is a smoother, which writes none of the
-    // coefficients' operands (areas, apu, apv, tag): they are formed before waiting for it
-    const bool early = (flags & 8) != 0;
-    if (!early) pdl_enter();
-    const CaseDev &C = cs[blockIdx.y];
-    const LevelDev &L = C.lv[ig];
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (!EARLY) pdl_enter();
+    CASE_PROLOGUE(mode);
     const Dom d = dom_interior(L);
-    int i, j;
-    const bool cell = mode_active(C, ig, mode) && cell_at(d, t, i, j);
-    Coef k;
-    double su = 0.0;
-    if (early) {
-        if (cell) mass_coefp_io(Prim{L}, C, i, j, k, su, S_U, S_V, MC_COEF);
-        pdl_enter();
-    }
-    CaseState &ST = st[blockIdx.y];
-    if (!case_active(C, ST, ig, mode)) return;
     const int n = d.wi * d.wj, nb = (n + blockDim.x - 1) / blockDim.x;
     if ((int)blockIdx.x >= nb) return;
     double a[1] = {0.0};
-    if (cell && early) {
-        const Prim io{L};
-        const int q = j * L.npx + i;
-        const int us = (flags & 1) ? S_TMP0 : S_U, vs = (flags & 1) ? S_TMP1 : S_V;
-        a[0] = mass_coefp_io(io, C, i, j, k, su, us, vs, MC_SU);
-        if (flags & 2) {
-            const double ap = (flags & 4) ? k.ap + 1.0e-30 : k.ap;
-            op32(L, EQ_PP, CK_AW)[q] = (float)k.aw;
-            op32(L, EQ_PP, CK_AE)[q] = (float)k.ae;
-            op32(L, EQ_PP, CK_AS)[q] = (float)k.as;
-            op32(L, EQ_PP, CK_AN)[q] = (float)k.an;
-            op32(L, EQ_PP, CK_AP)[q] = (float)(1.0 / ap);
-            op32(L, EQ_PP, CK_SU)[q] = (float)su;
-        } else {
-            // cell_mass_coefp's stores
-            if (flags & 1) {
-                if (i <= L.npx - 3) io.st(S_U, q, io.ld(us, q));
-                if (j <= L.npy - 3) io.st(S_V, q, io.ld(vs, q));
-                io.st(S_SC, q, io.ld(S_TMP2, q));
+    int i, j;
+    if (EARLY) {
+        const bool cell = cell_at(d, t, i, j);
+        Coef k;
+        double su = 0.0;
+        if (cell) mass_coefp_io(Prim{L}, C, i, j, k, su, S_U, S_V, MC_COEF);
+        pdl_enter();
+        if (cell) {
+            const Prim io{L};
+            const int q = j * L.npx + i;
+            const int us = (flags & 1) ? S_TMP0 : S_U, vs = (flags & 1) ? S_TMP1 : S_V;
+            a[0] = mass_coefp_io(io, C, i, j, k, su, us, vs, MC_SU);
+            if (flags & 2) {
+                const double ap = (flags & 4) ? k.ap + 1.0e-30 : k.ap;
+                op32(L, EQ_PP, CK_AW)[q] = (float)k.aw;
+                op32(L, EQ_PP, CK_AE)[q] = (float)k.ae;
+                op32(L, EQ_PP, CK_AS)[q] = (float)k.as;
+                op32(L, EQ_PP, CK_AN)[q] = (float)k.an;
+                op32(L, EQ_PP, CK_AP)[q] = (float)(1.0 / ap);
+                op32(L, EQ_PP, CK_SU)[q] = (float)su;
+            } else {
+                // cell_mass_coefp's stores
+                if (flags & 1) {
+                    if (i <= L.npx - 3) io.st(S_U, q, io.ld(us, q));
+                    if (j <= L.npy - 3) io.st(S_V, q, io.ld(vs, q));
+                    io.st(S_SC, q, io.ld(S_TMP2, q));
+                }
+                io.st(S_PP, q, 0.0);
+                store_coef(io, EQ_PP, q, k, su);
             }
-            io.st(S_PP, q, 0.0);
-            store_coef(io, EQ_PP, q, k, su);
         }
-    } else if (cell) {
+    } else if (cell_at(d, t, i, j)) {
         if (flags & 2) {
+            Coef k;
+            double su;
             a[0] = mass_coefp_values(L, C, i, j, k, su, S_U, S_V);
             const int q = j * L.npx + i;
             const double ap = (flags & 4) ? k.ap + 1.0e-30 : k.ap;
@@ -561,43 +554,21 @@ __device__ __forceinline__ int pair_tile(const LevelDev &L, int e, int nu, int t
 // dir 2 in place (a single tile covering the domain: it reads everything before it
 // writes).  Every cell update is the reference's formula on the same neighbour values,
 // so the result is bit-identical to sweeping the whole level unit by unit.
-template <int ISOLVE, int NT>
+// EARLY: the coefficients were written before the previous launch (a later launch of a
+// smoothing split in several), so they are read before waiting for it (a finished
+// case, ST.done, set at the end of a cycle, loads nothing).
+template <int ISOLVE, int NT, bool EARLY>
 __global__ void __launch_bounds__(NT, SMOOTH_BLOCK / NT) k_smooth(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode, int mask, int u0, int nu,
                                                          int dir, int tile)
 {
-    // dir bit 4: the coefficients were written before the previous launch (a later
-    // launch of a smoothing split in several), so they are read before waiting for it
-    const bool early = (dir & 4) != 0;
-    dir &= 3;
-    if (!early) pdl_enter();
+    if (!EARLY) pdl_enter();
     extern __shared__ double sm[];
     const CaseDev &C = cs[blockIdx.y];
+    if (!case_active(C, st[blockIdx.y], ig, mode)) return;
     const int e = nth_eq(mask, blockIdx.z);
     const LevelDev &L = C.lv[ig];
     PairTile P;
     const int g = pair_tile(L, e, nu, tile, P, blockIdx.x);
-    const double *__restrict__ gaw = L.f[co_slot(e, CK_AW)];
-    const double *__restrict__ gae = L.f[co_slot(e, CK_AE)];
-    const double *__restrict__ gas = L.f[co_slot(e, CK_AS)];
-    const double *__restrict__ gan = L.f[co_slot(e, CK_AN)];
-    const double *__restrict__ gap = L.f[co_slot(e, CK_AP)];
-    const double *__restrict__ gsu = L.f[co_slot(e, CK_SU)];
-    double A[6] = {0, 0, 0, 0, 0, 0}, B[6] = {0, 0, 0, 0, 0, 0}, pA = 0.0, pB = 0.0;
-    auto load_coef = [&]() {
-        if (P.okA) {
-            const int g0 = P.gA;
-            A[0] = gaw[g0]; A[1] = gae[g0]; A[2] = gas[g0]; A[3] = gan[g0]; A[4] = gap[g0]; A[5] = gsu[g0];
-        }
-        if (P.okB) {
-            const int g0 = P.gB;
-            B[0] = gaw[g0]; B[1] = gae[g0]; B[2] = gas[g0]; B[3] = gan[g0]; B[4] = gap[g0]; B[5] = gsu[g0];
-        }
-    };
-    if (early) {
-        if (g == 0) load_coef();
-        pdl_enter();
-    }
-    if (!case_active(C, st[blockIdx.y], ig, mode)) return;
     if (g == 1) return;
     if (g == 2) {     // the schedule sizes blocks to fit; never taken
         if (threadIdx.x == 0) atomicOr(&st[blockIdx.y].status, (int)CASE_BAD_LAUNCH);
@@ -608,9 +579,37 @@ __global__ void __launch_bounds__(NT, SMOOTH_BLOCK / NT) k_smooth(const CaseDev 
     const double *src = L.f[dir == 1 ? ts : fs];
     double *dst = L.f[dir == 0 ? ts : fs];
     double *phi = sm, *phi2 = sm + W * P.Hh;
-    if (!early) load_coef();
-    if (P.okA) pA = src[P.gA];
-    if (P.okB) pB = src[P.gB];
+    const double *__restrict__ gaw = L.f[co_slot(e, CK_AW)];
+    const double *__restrict__ gae = L.f[co_slot(e, CK_AE)];
+    const double *__restrict__ gas = L.f[co_slot(e, CK_AS)];
+    const double *__restrict__ gan = L.f[co_slot(e, CK_AN)];
+    const double *__restrict__ gap = L.f[co_slot(e, CK_AP)];
+    const double *__restrict__ gsu = L.f[co_slot(e, CK_SU)];
+    double A[6] = {0, 0, 0, 0, 0, 0}, B[6] = {0, 0, 0, 0, 0, 0}, pA = 0.0, pB = 0.0;
+    if (EARLY) {
+        if (P.okA) {
+            const int g0 = P.gA;
+            A[0] = gaw[g0]; A[1] = gae[g0]; A[2] = gas[g0]; A[3] = gan[g0]; A[4] = gap[g0]; A[5] = gsu[g0];
+        }
+        if (P.okB) {
+            const int g0 = P.gB;
+            B[0] = gaw[g0]; B[1] = gae[g0]; B[2] = gas[g0]; B[3] = gan[g0]; B[4] = gap[g0]; B[5] = gsu[g0];
+        }
+        pdl_enter();
+        if (P.okA) pA = src[P.gA];
+        if (P.okB) pB = src[P.gB];
+    } else {
+        if (P.okA) {
+            const int g0 = P.gA;
+            pA = src[g0];
+            A[0] = gaw[g0]; A[1] = gae[g0]; A[2] = gas[g0]; A[3] = gan[g0]; A[4] = gap[g0]; A[5] = gsu[g0];
+        }
+        if (P.okB) {
+            const int g0 = P.gB;
+            pB = src[g0];
+            B[0] = gaw[g0]; B[1] = gae[g0]; B[2] = gas[g0]; B[3] = gan[g0]; B[4] = gap[g0]; B[5] = gsu[g0];
+        }
+    }
     const double eps = ISOLVE == MGFVM_JACOBI ? 1.0e-30 : 0.0;   // solver's (ap + 1e-30), solvergs' ap
     const Recip RA = make_recip(ISOLVE == MGFVM_JACOBI ? A[4] + eps : A[4]);
     const Recip RB = make_recip(ISOLVE == MGFVM_JACOBI ? B[4] + eps : B[4]);
@@ -1991,18 +1990,26 @@ static cudaError_t launch_smooth_tma(bool pdl, const Launch &X, dim3 g, int b, c
     return le;
 }
 
+template <int ISOLVE, bool EARLY>
+static cudaError_t launch_smooth_e(bool pdl, const Launch &X, dim3 g, int b, const CaseDev *dc, CaseState *ds,
+                                   int dir, cudaStream_t st)
+{
+    cudaError_t le;
+    if (b <= SMOOTH_BLOCK / 4)
+        le = launch_k(pdl, k_smooth<ISOLVE, SMOOTH_BLOCK / 4, EARLY>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, dir, X.a4);
+    else if (b <= SMOOTH_BLOCK / 2)
+        le = launch_k(pdl, k_smooth<ISOLVE, SMOOTH_BLOCK / 2, EARLY>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, dir, X.a4);
+    else
+        le = launch_k(pdl, k_smooth<ISOLVE, SMOOTH_BLOCK, EARLY>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, dir, X.a4);
+    return le;
+}
+// a3 bit 4: the coefficients may be read before the wait for the previous launch
 template <int ISOLVE>
 static cudaError_t launch_smooth(bool pdl, const Launch &X, dim3 g, int b, const CaseDev *dc, CaseState *ds,
                                  cudaStream_t st)
 {
-    cudaError_t le;
-    if (b <= SMOOTH_BLOCK / 4)
-        le = launch_k(pdl, k_smooth<ISOLVE, SMOOTH_BLOCK / 4>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
-    else if (b <= SMOOTH_BLOCK / 2)
-        le = launch_k(pdl, k_smooth<ISOLVE, SMOOTH_BLOCK / 2>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
-    else
-        le = launch_k(pdl, k_smooth<ISOLVE, SMOOTH_BLOCK>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
-    return le;
+    if (X.a3 & 4) return launch_smooth_e<ISOLVE, true>(pdl, X, g, b, dc, ds, X.a3 & 3, st);
+    return launch_smooth_e<ISOLVE, false>(pdl, X, g, b, dc, ds, X.a3, st);
 }
 
 cudaError_t launch_one(const Launch &X, const CaseDev *dc, CaseState *ds, const CaseTan *dt, const Sched &S,
@@ -2018,8 +2025,14 @@ cudaError_t launch_one(const Launch &X, const CaseDev *dc, CaseState *ds, const 
         if (X.a1) le = launch_k(pdl, k_asm<1>, g, b, 0, st, dc, ds, X.ig, X.mode, (unsigned)X.a0);
         else le = launch_k(pdl, k_asm<0>, g, b, 0, st, dc, ds, X.ig, X.mode, (unsigned)X.a0);
         break;
-    case K_MASS_COEFP: le = launch_k(pdl, k_mass_coefp, g, b, 0, st, dc, ds, X.ig, X.mode, X.a0, X.a1); break;
-    case K_UPDATE: le = launch_k(pdl, k_update, g, b, 0, st, dc, ds, X.ig, X.mode, X.a0); break;
+    case K_MASS_COEFP:
+        if (X.a1 & 8) le = launch_k(pdl, k_mass_coefp<true>, g, b, 0, st, dc, ds, X.ig, X.mode, X.a0, X.a1 & ~8);
+        else le = launch_k(pdl, k_mass_coefp<false>, g, b, 0, st, dc, ds, X.ig, X.mode, X.a0, X.a1);
+        break;
+    case K_UPDATE:
+        if (X.a0 & 64) le = launch_k(pdl, k_update<true>, g, b, 0, st, dc, ds, X.ig, X.mode, X.a0 & ~64);
+        else le = launch_k(pdl, k_update<false>, g, b, 0, st, dc, ds, X.ig, X.mode, X.a0);
+        break;
     case K_PFIX: le = launch_k(pdl, k_pfix, g, b, 0, st, dc, ds, X.ig, X.mode, X.a0); break;
     case K_BOUND: le = launch_k(pdl, k_bound, g, b, 0, st, dc, ds, X.ig, X.mode, X.a0); break;
     case K_SMOOTH:

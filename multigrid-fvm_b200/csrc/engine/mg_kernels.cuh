@@ -75,10 +75,10 @@ constexpr int SMOOTH_BLOCK = 1024;
 // dynamic shared memory per CTA (the band and its two halo rows, two buffers for Jacobi)
 constexpr int BAND_MAX_CTAS = 8;
 constexpr int BAND_SMEM_MAX = 80 * 1024;
-// By default a level runs band visits in batches of at least this many cases: a unit
-// costs about a microsecond there (its cluster barrier), which only pays when the tile
-// launches it replaces have enough work to be slow too (256^2 cases, levels 1-2:
-// slower up to 16 cases, faster from 32)
+// By default a level runs band visits in batches of at least this many cases (of one
+// size at that level): a unit costs about a microsecond there (its cluster barrier),
+// which only pays when the tile launches it replaces have enough work to be slow too
+// (256^2 cases, levels 1-2: slower up to 16 cases, faster from 32)
 constexpr int BAND_MIN_CASES = 32;
 // interior rows of each band when G CTAs share a level of npy padded rows (even; the
 // last band may be shorter)

@@ -69,8 +69,9 @@ def test_obstacle_flow_pair_long_run(oracle_built):
 
 @pytest.mark.parametrize("band", [0, 2])
 def test_mixed_size_batch(band, oracle_built):
-    """Cases of three sizes share every launch; band visits (on level 1 by default, on
-    levels 0-2 where they fit with band 2) cover cases smaller than the launch."""
+    """Cases of three sizes share every launch.  With band 2, band visits run levels 0-2
+    where they fit, shaped for the largest case, so smaller cases leave bands empty
+    (the default takes none for this batch: too few cases, and of several sizes)."""
     from mgfvm import Solver, configs
     from oracle import OracleCase
     cases = configs.c2(9, seed=2)
