@@ -307,7 +307,9 @@ struct Builder {
             int u0 = 0;
             for (int c = 0; c < chunks; ++c) {
                 const int nu = units / chunks + (c < units % chunks ? 1 : 0);
-                const int flags = (c == 0 ? 1 : 0) | (c == chunks - 1 ? 2 : 0) | ((c & 1) ? 4 : 0);
+                // bit 8: a later launch reads its operands before waiting for the one before it
+                const int flags = (c == 0 ? 1 : 0) | (c == chunks - 1 ? 2 : 0) | ((c & 1) ? 4 : 0) |
+                                  (c > 0 && x->sched.pdl ? 8 : 0);
                 Launch &L = add(K_SMOOTH_F32, ig, mode, 0, mask, u0, nu, flags);
                 L.a4 = tile;
                 L.grid = dim3((unsigned)tiles(ig, tile), x->ncases, neq);

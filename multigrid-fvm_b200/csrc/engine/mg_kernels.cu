@@ -1269,11 +1269,13 @@ __global__ void __launch_bounds__(SMOOTH_BLOCK, 1)
 // phi + delta in FP64; p' keeps delta, which is p' itself), bit 4: delta is read from
 // buffer 1 and written to buffer 0 (else the reverse).  Every launch writes the tile's
 // delta, and zero on the boundary ring where the tile touches it, to its output buffer.
-template <int ISOLVE, int NT>
+// EARLY: a later launch of the smoothing (not the first): its operands were written
+// before the previous launch and are read before waiting for it; the correction after.
+template <int ISOLVE, int NT, bool EARLY>
 __global__ void __launch_bounds__(NT, SMOOTH_BLOCK / NT) k_smooth_f32(const CaseDev *__restrict__ cs, CaseState *st, int ig, int mode, int mask,
                                                              int u0, int nu, int flags, int tile)
 {
-    pdl_enter();
+    if (!EARLY) pdl_enter();
     extern __shared__ float smf[];
     const CaseDev &C = cs[blockIdx.y];
     if (!case_active(C, st[blockIdx.y], ig, mode)) return;
@@ -1308,6 +1310,7 @@ __global__ void __launch_bounds__(NT, SMOOTH_BLOCK / NT) k_smooth_f32(const Case
         const int g0 = P.gB;
         B[0] = o0[g0]; B[1] = o1[g0]; B[2] = o2[g0]; B[3] = o3[g0]; B[4] = o4[g0]; B[5] = o5[g0];
     }
+    if (EARLY) pdl_enter();
     if (!first) {
         if (P.okA) dA = src[P.gA];
         if (P.okB) dB = src[P.gB];
@@ -1990,6 +1993,19 @@ static cudaError_t launch_smooth_tma(bool pdl, const Launch &X, dim3 g, int b, c
     return le;
 }
 
+// a3 = flags (bit 8: operands before the wait, EARLY)
+template <int ISOLVE, bool EARLY>
+static cudaError_t launch_smooth_f32(bool pdl, const Launch &X, dim3 g, int b, const CaseDev *dc, CaseState *ds,
+                                     cudaStream_t st)
+{
+    const int f = X.a3 & 7;
+    if (b <= SMOOTH_BLOCK / 4)
+        return launch_k(pdl, k_smooth_f32<ISOLVE, SMOOTH_BLOCK / 4, EARLY>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, f, X.a4);
+    if (b <= SMOOTH_BLOCK / 2)
+        return launch_k(pdl, k_smooth_f32<ISOLVE, SMOOTH_BLOCK / 2, EARLY>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, f, X.a4);
+    return launch_k(pdl, k_smooth_f32<ISOLVE, SMOOTH_BLOCK, EARLY>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, f, X.a4);
+}
+
 template <int ISOLVE, bool EARLY>
 static cudaError_t launch_smooth_e(bool pdl, const Launch &X, dim3 g, int b, const CaseDev *dc, CaseState *ds,
                                    int dir, cudaStream_t st)
@@ -2045,19 +2061,11 @@ cudaError_t launch_one(const Launch &X, const CaseDev *dc, CaseState *ds, const 
     case K_SMOOTH_F32:
         if (b > SMOOTH_BLOCK) return cudaErrorInvalidValue;
         if (S.isolve == MGFVM_JACOBI) {
-            if (b <= SMOOTH_BLOCK / 4)
-                le = launch_k(pdl, k_smooth_f32<MGFVM_JACOBI, SMOOTH_BLOCK / 4>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
-            else if (b <= SMOOTH_BLOCK / 2)
-                le = launch_k(pdl, k_smooth_f32<MGFVM_JACOBI, SMOOTH_BLOCK / 2>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
-            else
-                le = launch_k(pdl, k_smooth_f32<MGFVM_JACOBI, SMOOTH_BLOCK>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+            if (X.a3 & 8) le = launch_smooth_f32<MGFVM_JACOBI, true>(pdl, X, g, b, dc, ds, st);
+            else le = launch_smooth_f32<MGFVM_JACOBI, false>(pdl, X, g, b, dc, ds, st);
         } else {
-            if (b <= SMOOTH_BLOCK / 4)
-                le = launch_k(pdl, k_smooth_f32<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK / 4>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
-            else if (b <= SMOOTH_BLOCK / 2)
-                le = launch_k(pdl, k_smooth_f32<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK / 2>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
-            else
-                le = launch_k(pdl, k_smooth_f32<MGFVM_GAUSS_SEIDEL, SMOOTH_BLOCK>, g, b, X.smem, st, dc, ds, X.ig, X.mode, X.a0, X.a1, X.a2, X.a3, X.a4);
+            if (X.a3 & 8) le = launch_smooth_f32<MGFVM_GAUSS_SEIDEL, true>(pdl, X, g, b, dc, ds, st);
+            else le = launch_smooth_f32<MGFVM_GAUSS_SEIDEL, false>(pdl, X, g, b, dc, ds, st);
         }
         break;
     case K_COPY: le = launch_k(pdl, k_copy, g, b, 0, st, dc, ds, X.ig, X.mode, X.a0); break;

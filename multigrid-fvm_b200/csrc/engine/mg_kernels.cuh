@@ -22,7 +22,8 @@ enum KernelId {
     K_PROL_CORR, K_PROL_APPLY,   // prol_apply: a0 = 1 forms the corrections itself (no K_PROL_CORR before it)
     K_TAIL, K_ENDCYCLE, K_PROL_APPLY_END,
     K_SMOOTH_F32,    // mixed precision: the tiles of K_SMOOTH on FP32 operands and corrections
-                     // (a3 = flags: 1 first, 2 last, 4 read buffer 1)
+                     // (a3 = flags: 1 first, 2 last, 4 read buffer 1, 8 operands read
+                     // before the wait for the previous launch)
     K_PFIX_BOUND,    // K_PFIX then K_BOUND (a0 = bits), one CTA per case
     K_PP_LEVEL,      // masserror+coefp, p' smoothing, update on a one-CTA level: a0 = units,
                      // a1 = reduce, a2 = update fuse bits
