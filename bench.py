@@ -640,15 +640,19 @@ def main():
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
         e0.record(stream)
+        solve_ms = []
         for _ in range(a.steps):
             with torch.cuda.stream(stream):
                 flush.fill_(1.0)          # L2 flush between steps (256 MiB write)
             cycles.append(step())
+            solve_ms.append(solver.last_elapsed_ms)
         e1.record(stream)
         torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     ms = e0.elapsed_time(e1)
+    log(f"timed steps: {ms / max(1, a.steps):.1f} ms each; the solves inside them "
+        + ", ".join(f"{t:.1f}" for t in solve_ms) + " ms (device, first to last chunk)")
     launches = solver.kernel_launches - launches0
     # the timed solve's final level-0 fields (later measurements change the state)
     gpu_fields = [{f: solver.field(k, 0, f) for f in ("u", "v", "p", "sc")} for k in range(n_cases)] \
