@@ -492,13 +492,16 @@ struct Builder {
             const int fuse = outflow_fusable(ig, mode, pfx) ? (down ? 1 : 3) : 0;
             const int what = asm_done ? 0 : (int)asm_bits(down);
             const bool visit = what != 0 || mu > 0;
+            // the pressure copy and pbound / outflow left after update run in the same
+            // CTA (pp_level_tail) instead of the launches after_update would add
+            const int bb = fuse ? 0 : (down ? 3 : 7);
+            const int tail = (!pfx && pfix_needed(ig, mode) ? 128 : 0) | (bb && bound_needed(bb) ? bb << 8 : 0);
             Launch &L = add(visit ? K_LEVEL_VISIT : K_PP_LEVEL, ig, mode, 0, ppu, reduce ? 1 : 0,
-                            fuse | (pfx ? 4 : 0), what);
+                            fuse | (pfx ? 4 : 0) | tail, what);
             L.a4 = std::max(mu, 0);
             L.grid = dim3(visit ? 3 : 1, x->ncases);
             L.block = round32(mx * ((my + 1) / 2));
             L.smem = (isolve == MGFVM_JACOBI ? 2 : 1) * mx * my * (int)sizeof(double);
-            after_update(ig, mode, fuse | (pfx ? 4 : 0), fuse ? 0 : (down ? 3 : 7));
             return;
         }
         int G, blk, smem;

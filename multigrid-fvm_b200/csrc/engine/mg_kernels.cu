@@ -430,6 +430,22 @@ __global__ void __launch_bounds__(BLOCK) k_pfix(const CaseDev *__restrict__ cs, 
 
 // pbound :1179-1210 then outflow :1211-1228 (bits: 1 periodic, 2 outflow of u, v, p,
 // 4 the scalar ghost too) — one block per case.
+// update's obstacle pressure copy (:1153-1177) by one CTA
+template <class IO>
+__device__ __forceinline__ void pfix_block_io(const IO &io)
+{
+    const LevelDev &L = io.L;
+    if (L.ncopy <= 0) return;
+    if (L.hazard) {
+        for (int t = threadIdx.x; t < L.ncopy; t += blockDim.x) io.set_pb(t, io.ld(S_P, L.psrc[t]));
+        __syncthreads();
+        for (int t = threadIdx.x; t < L.ncopy; t += blockDim.x) io.st(S_P, L.pdst[t], io.pb(t));
+    } else {
+        for (int t = threadIdx.x; t < L.ncopy; t += blockDim.x) io.st(S_P, L.pdst[t], io.ld(S_P, L.psrc[t]));
+    }
+    __syncthreads();
+}
+
 template <class IO>
 __device__ __forceinline__ void bound_block_io(const CaseDev &C, const IO &io, int bits)
 {
@@ -829,20 +845,35 @@ __device__ __forceinline__ int level_smooth_eq(const LevelDev &L, int e, int mu,
     return 0;
 }
 
+// After the update of a one-CTA level: `fuse` bit 128, the obstacle pressure copy (when
+// update does not do it); bits 8-10, pbound / outflow with these k_bound bits — the
+// launches after_update would add, run by the same CTA.
+__device__ __forceinline__ void pp_level_tail(const CaseDev &C, const LevelDev &L, int fuse)
+{
+    if (!(fuse & (128 | (7 << 8)))) return;
+    __syncthreads();
+    if (fuse & 128) pfix_block_io(Prim{L});
+    if ((fuse >> 8) & 7) bound_block_io(C, Prim{L}, (fuse >> 8) & 7);
+}
+
 // solve_pprime and update on a level that one CTA per case holds (at most SMOOTH_BLOCK
 // vertical cell pairs): masserror + coefp for every interior cell (:1096-1125,
 // :1018-1092), all `nu` p' units in shared memory (as k_smooth with one tile), then
 // update (:1127-1152) with k_update's fusions (`fuse` bits 1, 2, 4) reading p' from
 // shared memory, and the final p' written to the field.  The p' coefficients stay in
 // registers (nothing else reads them).  With `reduce` the level's sum |div| (a block
-// tree) becomes the case's mass error.  Same bits as the separate kernels.
+// tree) becomes the case's mass error; then pp_level_tail (`fuse` bits 128, 8-10).
+// Same bits as the separate kernels.
 template <int ISOLVE>
 __device__ __forceinline__ void pp_level_body(const CaseDev &C, CaseState &ST, const LevelDev &L, int nu, int reduce,
                                               int fuse, double *sm)
 {
     PairTile P;
     const int g = pair_tile(L, EQ_PP, nu, max(L.npx, L.npy), P, 0);
-    if (g == 1) return;
+    if (g == 1) {
+        pp_level_tail(C, L, fuse);
+        return;
+    }
     if (g == 2) {
         if (threadIdx.x == 0) atomicOr(&ST.status, (int)CASE_BAD_LAUNCH);
         return;
@@ -923,6 +954,7 @@ __device__ __forceinline__ void pp_level_body(const CaseDev &C, CaseState &ST, c
         block_sum<1>(a);
         if (threadIdx.x == 0) ST.last_err = a[0];
     }
+    pp_level_tail(C, L, fuse);
 }
 
 template <int ISOLVE>
@@ -1724,21 +1756,6 @@ struct PrimCase {
     __device__ __forceinline__ Prim io(int ig) const { return Prim{C.lv[ig]}; }
 };
 
-// update's obstacle pressure copy (:1153-1177) by one CTA
-template <class IO>
-__device__ __forceinline__ void pfix_block_io(const IO &io)
-{
-    const LevelDev &L = io.L;
-    if (L.ncopy <= 0) return;
-    if (L.hazard) {
-        for (int t = threadIdx.x; t < L.ncopy; t += blockDim.x) io.set_pb(t, io.ld(S_P, L.psrc[t]));
-        __syncthreads();
-        for (int t = threadIdx.x; t < L.ncopy; t += blockDim.x) io.st(S_P, L.pdst[t], io.pb(t));
-    } else {
-        for (int t = threadIdx.x; t < L.ncopy; t += blockDim.x) io.st(S_P, L.pdst[t], io.ld(S_P, L.psrc[t]));
-    }
-    __syncthreads();
-}
 
 // One SIMPLE step on level ig (down leg :201-207, up leg :235-244).  The plain run
 // stages each level's smoothing in shared memory where it fits (tail_smooth); the
