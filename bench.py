@@ -328,7 +328,7 @@ class ClockSampler:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
-            # let nvidia-smi finish its start-up (driver initialisation) before the timed
+            # let nvidia-smi finish its start-up (NVML initialisation) before the timed
             # region opens: its first sample marks it as running
             for _ in range(100):
                 if os.path.getsize(self.path) > 0 or self.proc.poll() is not None:
